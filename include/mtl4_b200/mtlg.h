@@ -1,0 +1,246 @@
+/*
+ * mtl4_b200 C ABI: the drop-in boundary for MTL4's sparse-solve hot path on
+ * one B200 GPU (sm_100a).  Plain pointers and sizes only; every function
+ * returns an int status (MTLG_OK == 0).
+ *
+ * Reference surface each group replaces (paths inside simunova/mtl4):
+ *   mtlg_csr_*     mtl::compressed2D<T> raw-array constructor
+ *                  (boost/numeric/mtl/matrix/compressed2D.hpp:355-364)
+ *   mtlg_vec_*     mtl::dense_vector<T>(n, address)
+ *                  (boost/numeric/mtl/vector/dense_vector.hpp:122)
+ *   mtlg_spmv      w = A*v, w += A*v, w -= A*v
+ *                  (boost/numeric/mtl/vector/crtp_base_vector.hpp:94-101,
+ *                   boost/numeric/mtl/operation/mat_vec_mult.hpp:614-683)
+ *   mtlg_dot / mtlg_two_norm
+ *                  mtl::dot, mtl::two_norm
+ *                  (boost/numeric/mtl/operation/dot.hpp:228,
+ *                   boost/numeric/mtl/operation/two_norm.hpp:54)
+ *   mtlg_pc_*      itl::pc::identity / diagonal / ilu_0 / ic_0 and
+ *                  solve(P, x) / adjoint_solve(P, x)
+ *                  (boost/numeric/itl/pc/identity.hpp:25, diagonal.hpp:29-64,
+ *                   ilu_0.hpp:34-92, ilu.hpp:74-115, ic_0.hpp:40-107)
+ *   mtlg_solve     itl::cg(A,x,b,P,iter) (boost/numeric/itl/krylov/cg.hpp:76),
+ *                  itl::bicgstab (bicgstab.hpp:29),
+ *                  itl::gmres(A,x,b,L,R,iter,restart) (gmres.hpp:124) with
+ *                  itl::basic_iteration<double>
+ *                  (boost/numeric/itl/iteration/basic_iteration.hpp:24-93)
+ *   mtlg_refine_solve, mtlg_batch_*, mtlg_server_*
+ *                  no reference counterpart: FP64 iterative refinement around
+ *                  an FP32 inner solve, batched and served solves.
+ */
+#ifndef MTL4_B200_MTLG_H
+#define MTL4_B200_MTLG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (mapped to the reference's exception types by the C++
+ * front end: utility/exception.hpp:116-204, itl/utility/exception.hpp:22-31) */
+enum {
+    MTLG_OK = 0,
+    MTLG_ERR_INVALID_ARG = 1,       /* null handle, bad enum, negative size     */
+    MTLG_ERR_NOT_SQUARE = 2,        /* mtl::matrix_not_square                   */
+    MTLG_ERR_MISSING_DIAGONAL = 3,  /* mtl::missing_diagonal                    */
+    MTLG_ERR_ZERO_PIVOT = 4,        /* factorization produced a non-finite pivot */
+    MTLG_ERR_BREAKDOWN = 5,         /* itl::unexpected_orthogonality            */
+    MTLG_ERR_OOM = 6,               /* device allocation failed / over budget   */
+    MTLG_ERR_TIMEOUT = 7,           /* a bounded device-side wait expired       */
+    MTLG_ERR_CUDA = 8,              /* CUDA runtime error                       */
+    MTLG_ERR_INCOMPATIBLE_SIZE = 9, /* mtl::incompatible_size                   */
+    MTLG_ERR_UNSORTED = 10,         /* CSR rows must be sorted, in range        */
+    MTLG_ERR_TOO_LARGE = 11,        /* nnz or n beyond int32 device indexing    */
+    MTLG_ERR_NOT_SUPPORTED = 12,
+    MTLG_ERR_ADMISSION = 13,        /* serving: request does not fit the budget */
+    MTLG_ERR_NOT_FOUND = 14,        /* serving: unknown request id              */
+    MTLG_PENDING = 15               /* serving: request not finished yet        */
+};
+
+typedef enum { MTLG_F64 = 0, MTLG_F32 = 1 } mtlg_dtype;
+typedef enum { MTLG_ASSIGN = 0, MTLG_PLUS = 1, MTLG_MINUS = 2 } mtlg_assign;
+typedef enum { MTLG_PC_IDENTITY = 0, MTLG_PC_DIAGONAL = 1, MTLG_PC_ILU0 = 2, MTLG_PC_IC0 = 3 } mtlg_pc_kind;
+typedef enum { MTLG_CG = 0, MTLG_BICGSTAB = 1, MTLG_GMRES = 2 } mtlg_solver;
+
+/* Termination state of one solve; mirrors itl::basic_iteration. */
+enum {
+    MTLG_ST_RUNNING = 0,
+    MTLG_ST_CONVERGED = 1,   /* resid <= rtol*norm_r0 or resid <= atol   error_code 0 */
+    MTLG_ST_MAXIT = 2,       /* "Too many iterations."                    error_code 1 */
+    MTLG_ST_BREAKDOWN = 3,   /* zero rho/gamma/omega (BiCGSTAB) or NaN    */
+    MTLG_ST_NO_DIRECTION = 4 /* GMRES found no direction                  error_code 2 */
+};
+
+typedef struct mtlg_ctx mtlg_ctx;
+typedef struct mtlg_csr mtlg_csr;
+typedef struct mtlg_vec mtlg_vec;
+typedef struct mtlg_pc mtlg_pc;
+typedef struct mtlg_batch mtlg_batch;
+typedef struct mtlg_server mtlg_server;
+
+/* basic_iteration<double>(r0 or norm, max_iter, rtol, atol).  norm_r0 < 0
+ * means "take ||b||" as the reference's constructor from b does
+ * (basic_iteration.hpp:32-34). */
+typedef struct {
+    int max_iter;
+    int restart;        /* GMRES restart length (gmres.hpp:124-137) */
+    double rtol;
+    double atol;
+    double norm_r0;
+} mtlg_iter_params;
+
+typedef struct {
+    int iterations;     /* iter.iterations(); total inner iterations for refinement */
+    int error_code;     /* iter.error_code(): 0 converged, 1 too many iterations, 2 GMRES */
+    int status;         /* MTLG_ST_* */
+    int outer_iterations;
+    double resid;       /* iter.resid() */
+    double relresid;    /* iter.relresid() = resid / norm_r0 */
+    double norm_r0;
+    double seconds;     /* device time of the solve (CUDA events) */
+} mtlg_iter_result;
+
+/* FP64 iterative refinement around an FP32 inner Krylov solve. */
+typedef struct {
+    int max_outer;      /* refinement steps */
+    int max_inner;      /* inner iterations per step */
+    int restart;
+    int pad;
+    double rtol;        /* outer: ||b - A x||_FP64 <= rtol * ||b|| */
+    double inner_rtol;  /* inner: relative to the step's right-hand side */
+} mtlg_refine_params;
+
+/* ---- context -------------------------------------------------------------- */
+int mtlg_ctx_create(int device, size_t hbm_budget, mtlg_ctx** out);
+int mtlg_ctx_destroy(mtlg_ctx* ctx);
+int mtlg_ctx_synchronize(mtlg_ctx* ctx);
+/* Use an external cudaStream_t (e.g. torch's current stream); NULL restores
+ * the context's own stream. */
+int mtlg_ctx_set_stream(mtlg_ctx* ctx, void* cuda_stream);
+void* mtlg_ctx_stream(mtlg_ctx* ctx);
+/* Kernels this library enqueued on the context since creation (graph replays
+ * count every kernel node they run). */
+int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
+/* Bytes of device memory the context's objects hold. */
+size_t mtlg_ctx_bytes_in_use(mtlg_ctx* ctx);
+const char* mtlg_status_string(int status);
+const char* mtlg_last_error_message(void);
+
+/* ---- CSR matrix (compressed2D) --------------------------------------------- */
+/* Host arrays are copied.  Columns must be sorted and in range in every row
+ * (the reference's trisolves require sorted rows, lower_trisolve.hpp:105). */
+int mtlg_csr_create(mtlg_ctx* ctx, int64_t n_rows, int64_t n_cols, int64_t nnz, const int64_t* row_ptr,
+                    const int32_t* col, const void* val, mtlg_dtype val_dtype, mtlg_csr** out);
+int mtlg_csr_destroy(mtlg_csr* A);
+int mtlg_csr_info(const mtlg_csr* A, int64_t* n_rows, int64_t* n_cols, int64_t* nnz);
+/* Replace the values (same pattern), e.g. a new operator with the old graph. */
+int mtlg_csr_update_values(mtlg_csr* A, const void* val, mtlg_dtype val_dtype);
+/* SpMV tiling statistics: tiles by kind (0 stream, 1 vector, 2 long row). */
+int mtlg_csr_plan_info(const mtlg_csr* A, int64_t* tiles_by_kind3, int* max_row_len);
+
+/* ---- dense vectors (dense_vector) ----------------------------------------- */
+int mtlg_vec_create(mtlg_ctx* ctx, int64_t n, mtlg_dtype dtype, mtlg_vec** out);   /* zero-filled */
+/* Borrow caller-owned device memory (not freed by mtlg_vec_destroy). */
+int mtlg_vec_wrap(mtlg_ctx* ctx, int64_t n, mtlg_dtype dtype, void* device_ptr, mtlg_vec** out);
+int mtlg_vec_destroy(mtlg_vec* v);
+int mtlg_vec_upload(mtlg_vec* v, const void* host, int64_t n);     /* host dtype == vector dtype */
+int mtlg_vec_download(const mtlg_vec* v, void* host, int64_t n);
+int mtlg_vec_fill(mtlg_vec* v, double value);
+void* mtlg_vec_device_ptr(const mtlg_vec* v);
+int64_t mtlg_vec_size(const mtlg_vec* v);
+
+/* ---- level-1 / SpMV --------------------------------------------------------- */
+/* y (=|+=|-=) A x.  FP64 vectors use the FP64 values, FP32 vectors the FP32
+ * copy of the values (made once, on first use).  Rows of up to 32 entries are
+ * summed sequentially in storage order, as the reference does. */
+int mtlg_spmv(mtlg_ctx* ctx, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, int assign);
+/* Fused q = A p and the dot p.q (cg.hpp:103 lazy pair) in one pass. */
+int mtlg_spmv_dot(mtlg_ctx* ctx, mtlg_csr* A, const mtlg_vec* p, mtlg_vec* q, double* pq);
+int mtlg_dot(mtlg_ctx* ctx, const mtlg_vec* x, const mtlg_vec* y, double* out);
+int mtlg_two_norm(mtlg_ctx* ctx, const mtlg_vec* x, double* out);
+/* y += a x */
+int mtlg_axpy(mtlg_ctx* ctx, double a, const mtlg_vec* x, mtlg_vec* y);
+
+/* ---- preconditioners -------------------------------------------------------- */
+/* storage = value type of the stored factors / inverse diagonal (the `Value`
+ * template argument).  ILU(0)/IC(0) always factorize in FP64 on the GPU. */
+int mtlg_pc_create(mtlg_ctx* ctx, mtlg_csr* A, int kind, mtlg_dtype storage, mtlg_pc** out);
+int mtlg_pc_destroy(mtlg_pc* P);
+/* y = solve(P, x); y = adjoint_solve(P, x).  x and y have the same dtype. */
+int mtlg_pc_apply(mtlg_ctx* ctx, mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y);
+int mtlg_pc_adjoint_apply(mtlg_ctx* ctx, mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y);
+/* Stored factors as CSR on the host (which: 0 = L, 1 = U).  ILU(0): L strict
+ * lower with implied unit diagonal, U upper with inverted diagonal first in
+ * each row.  IC(0): U with diagonal 1/sqrt(pivot) first, L = trans(U) with
+ * the diagonal last.  Call with null arrays to query nnz. */
+int mtlg_pc_factor(const mtlg_pc* P, int which, int64_t* nnz, int64_t* row_ptr, int32_t* col, double* val);
+/* Number of dependency levels of the L and U sweeps. */
+int mtlg_pc_levels(const mtlg_pc* P, int* levels_L, int* levels_U);
+
+/* ---- solvers ---------------------------------------------------------------- */
+/* x is in/out (initial guess on entry).  pc_right may be NULL (identity); CG
+ * and BiCGSTAB ignore it as the reference does.  Returns MTLG_OK when the
+ * solve ran (convergence is reported in `result`), MTLG_ERR_BREAKDOWN when
+ * BiCGSTAB hit a zero rho/gamma/omega (the reference throws). */
+int mtlg_solve(mtlg_ctx* ctx, int solver, mtlg_csr* A, mtlg_pc* pc_left, mtlg_pc* pc_right, mtlg_vec* x,
+               const mtlg_vec* b, const mtlg_iter_params* params, mtlg_iter_result* result);
+/* x, b FP64; the inner solve runs on the FP32 values and FP32 vectors with
+ * `pc` (storage FP32, factorized in FP64). */
+int mtlg_refine_solve(mtlg_ctx* ctx, int solver, mtlg_csr* A, mtlg_pc* pc, mtlg_vec* x, const mtlg_vec* b,
+                      const mtlg_refine_params* params, mtlg_iter_result* result);
+
+/* ---- batched solves ------------------------------------------------------- */
+/* Many independent systems of uneven size solved together: every kernel of an
+ * iteration covers all unfinished systems.  Each system keeps its own
+ * iteration state, so its result does not depend on the others. */
+int mtlg_batch_create(mtlg_ctx* ctx, mtlg_batch** out);
+int mtlg_batch_destroy(mtlg_batch* B);
+/* Adds a system (host arrays copied); returns its index in *index. */
+int mtlg_batch_add(mtlg_batch* B, int64_t n, int64_t nnz, const int64_t* row_ptr, const int32_t* col,
+                   const double* val, const double* b, int solver, int pc_kind, const mtlg_iter_params* params,
+                   int* index);
+/* precision MTLG_F64: plain FP64 solves; MTLG_F32: FP32 inner with FP64
+ * refinement (refine may be NULL for defaults). */
+int mtlg_batch_solve(mtlg_batch* B, int precision, const mtlg_refine_params* refine);
+int mtlg_batch_result(const mtlg_batch* B, int index, double* x_host, mtlg_iter_result* result);
+int mtlg_batch_size(const mtlg_batch* B);
+
+/* ---- served solves (continuous batching) ----------------------------------- */
+typedef struct {
+    size_t hbm_budget;        /* bytes the server may hold on the device */
+    int max_active;           /* systems advanced together */
+    int iters_per_step;       /* inner iterations per engine step */
+    int precision;            /* MTLG_F64 or MTLG_F32 (FP32 inner + FP64 refinement) */
+    int pad;
+    double rtol;
+    double inner_rtol;
+} mtlg_server_opts;
+
+typedef struct {
+    int64_t submitted, admitted, completed, rejected, cancelled;
+    int64_t active, queued;
+    int64_t steps;
+    size_t bytes_in_use;
+} mtlg_server_stats;
+
+int mtlg_server_create(mtlg_ctx* ctx, const mtlg_server_opts* opts, mtlg_server** out);
+int mtlg_server_destroy(mtlg_server* S);
+/* Queue a request (host arrays copied to pinned staging).  Fails with
+ * MTLG_ERR_ADMISSION only if the request could never fit the budget. */
+int mtlg_server_submit(mtlg_server* S, int64_t n, int64_t nnz, const int64_t* row_ptr, const int32_t* col,
+                       const double* val, const double* b, int solver, int pc_kind, int max_iter,
+                       int64_t* request_id);
+/* One engine step: admit queued requests that fit, advance every active
+ * system by up to iters_per_step iterations, retire finished ones. */
+int mtlg_server_step(mtlg_server* S);
+/* MTLG_OK with the solution once finished, MTLG_PENDING before. */
+int mtlg_server_poll(mtlg_server* S, int64_t request_id, double* x_host, mtlg_iter_result* result);
+int mtlg_server_cancel(mtlg_server* S, int64_t request_id);
+int mtlg_server_stats_get(const mtlg_server* S, mtlg_server_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MTL4_B200_MTLG_H */

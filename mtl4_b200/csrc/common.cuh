@@ -1,0 +1,301 @@
+// Shared definitions of the mtl4_b200 CUDA library (sm_100a).
+//
+// Execution model: every operation runs over a set of independent systems
+// ("systems" = independent linear systems; a single solve is a set of one).
+// Each system is described by a SysDesc (pointers into its own device
+// buffers) and owns a SysState (its Krylov scalars and termination state,
+// the device-side counterpart of itl::basic_iteration).  Work is cut into
+// row tiles that never straddle two systems, so every per-system reduction
+// sums the same partials in the same order whether the system runs alone or
+// in a batch.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mtl4_b200/mtlg.h"
+
+namespace mtlg {
+
+// ----------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+const char* last_error();
+
+#define MTLG_CUDA(call)                                                                     \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            ::mtlg::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return MTLG_ERR_CUDA;                                                           \
+        }                                                                                   \
+    } while (0)
+
+#define MTLG_TRY(expr)                  \
+    do {                                \
+        int s_ = (expr);                \
+        if (s_ != MTLG_OK) return s_;   \
+    } while (0)
+
+#define MTLG_CHECK_ARG(cond, msg)                       \
+    do {                                                \
+        if (!(cond)) {                                  \
+            ::mtlg::set_error("invalid argument: %s", msg); \
+            return MTLG_ERR_INVALID_ARG;                \
+        }                                               \
+    } while (0)
+
+// ----------------------------------------------------------------- constants
+constexpr int kTileRows = 256;        // rows per stream tile == threads per CTA
+constexpr int kTileNnz = 2048;        // entries staged in shared memory per tile
+constexpr int kShortRow = 32;         // rows up to this length: one thread, sequential sum
+constexpr int kBlock = 256;
+constexpr int kSweepRows = 32;        // rows per sweep task (one warp, one row per lane)
+constexpr int kMaxDots = 4;           // dots a fused pass can reduce at once
+constexpr int kNumVec = 16;           // workspace vectors per system
+constexpr long long kSpinLimit = 1LL << 20;  // polls before a device wait gives up (~0.5 s)
+
+// Tile kinds of the SpMV / vector tiling.
+enum TileKind : int { TILE_STREAM = 0, TILE_LONG = 1 };
+
+struct Tile {
+    int sys;        // system index
+    int row_begin;  // first row (system-local)
+    int row_end;    // one past the last row
+    int kind;       // TileKind
+};
+
+// One dependency-ordered sweep task: kSweepRows consecutive rows of a
+// system's level-ordered triangular factor.
+struct SweepTask {
+    int sys;
+    int first;      // first level-ordered row of the task
+};
+
+// Level-ordered triangular factor (device pointers).  Row k of the factor is
+// original row `row_of[k]` (-1 marks padding that aligns levels to warps);
+// its off-diagonal entries keep the reference's storage order and `dia[k]`
+// is the multiplier applied last (inverse diagonal, 1 for a unit diagonal).
+struct TriFactor {
+    const int* rp;
+    const int* ci;
+    const void* val;   // T
+    const void* dia;   // T
+    const int* row_of;
+};
+
+// Workspace vector slots.
+enum Vec : int {
+    V_R = 0, V_P0, V_P1, V_Q, V_Z, V_Z0, V_RT, V_V, V_S, V_T, V_PHAT, V_SHAT, V_D, V_W0, V_W1, V_W2
+};
+
+struct SysDesc {
+    int n;
+    int nnz;
+    const int* rp;
+    const int* ci;
+    const void* val;        // values in the solve precision T
+    const double* val64;    // FP64 values (outer residual of refinement)
+    void* x;                // solution (T)
+    const void* b;          // right-hand side (T)
+    void* ws;               // workspace: vector k at (T*)ws + k * ws_stride
+    long long ws_stride;
+    int pc;                 // mtlg_pc_kind
+    int pad0;
+    const void* inv_diag;   // T, Jacobi
+    TriFactor L, U;
+    double* x64;            // refinement: FP64 solution
+    const double* b64;      // refinement: FP64 right-hand side
+    double* r64;            // refinement: FP64 residual
+};
+
+// Device-side state of one system's solve (basic_iteration + Krylov scalars).
+struct SysState {
+    double rho, rho_1, alpha, beta, omega, gamma;
+    double rr, resid, norm_r0, rtol, atol;
+    double dots[kMaxDots];
+    double scale;           // refinement: ||r|| of the current step
+    double nb;              // refinement: ||b||
+    int iter, max_iter, status, error;
+    int ostatus;            // refinement (outer) status
+    int pad1;
+    int first, flags;
+    int outer, max_outer;
+    int inner_total, inner_max;
+    double inner_rtol, outer_rtol;
+};
+
+// Per-launch view of the system set.
+struct SetView {
+    const Tile* tiles;
+    int n_tiles;
+    int n_sys;
+    const int* sys_tile_begin;   // [n_sys + 1]
+    SysDesc* desc;
+    SysState* st;
+    double* partials;            // [n_tiles * kMaxDots]
+    unsigned* counters;          // [n_sys] last-block counters (self-resetting)
+    int* running;                // systems still running
+    int* err;                    // device error flags (timeouts)
+    unsigned long long cond;     // cudaGraphConditionalHandle (0: not in a graph)
+    int use_cond;
+};
+
+// ----------------------------------------------------------------- device helpers
+template <typename T> struct Sentinel;
+template <> struct Sentinel<double> {
+    static constexpr unsigned long long bits = 0xFFFFFFFFFFFFFFFFull;
+};
+template <> struct Sentinel<float> {
+    static constexpr unsigned bits = 0xFFFFFFFFu;
+};
+
+template <typename T> __device__ __forceinline__ T sentinel_value();
+template <> __device__ __forceinline__ double sentinel_value<double>() { return __longlong_as_double(-1ll); }
+template <> __device__ __forceinline__ float sentinel_value<float>() { return __uint_as_float(0xFFFFFFFFu); }
+
+__device__ __forceinline__ double ld_volatile(const double* p)
+{
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ float ld_volatile(const float* p)
+{
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_volatile(double* p, double v)
+{
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_volatile(float* p, float v)
+{
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ bool is_sentinel(double v)
+{
+    return (unsigned long long)__double_as_longlong(v) == Sentinel<double>::bits;
+}
+__device__ __forceinline__ bool is_sentinel(float v) { return (unsigned)__float_as_uint(v) == Sentinel<float>::bits; }
+// A computed value must never look like "not ready": map the sentinel bit
+// pattern (a NaN) to the canonical NaN.
+__device__ __forceinline__ double unsentinel(double v) { return is_sentinel(v) ? __longlong_as_double(0x7FF8000000000000ll) : v; }
+__device__ __forceinline__ float unsentinel(float v) { return is_sentinel(v) ? __uint_as_float(0x7FC00000u) : v; }
+
+template <typename T>
+__device__ __forceinline__ T* wsvec(const SysDesc& d, int k)
+{
+    return static_cast<T*>(d.ws) + (long long)k * d.ws_stride;
+}
+
+// Deterministic block reduction of kMaxDots doubles (fixed tree, fixed
+// thread->element mapping).  Result valid in thread 0.
+template <int ND>
+__device__ __forceinline__ void block_reduce(double (&v)[ND], double* smem /* [ND * 32] */)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o);
+    }
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < ND; ++j) smem[j * 32 + warp] = v[j];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int j = 0; j < ND; ++j) {
+            double t = lane < nw ? smem[j * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            v[j] = t;
+        }
+    }
+}
+
+// Writes this tile's partial dots and reports whether the calling CTA is the
+// last of its system to do so (then it owns the system's finalize).  The
+// counter resets itself for the next pass.
+template <int ND>
+__device__ __forceinline__ bool publish_partials(const SetView& sv, int tile, int sys, const double (&v)[ND])
+{
+    __shared__ int s_last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < ND; ++j) sv.partials[(long long)tile * kMaxDots + j] = v[j];
+        __threadfence();
+        const unsigned ntiles = unsigned(sv.sys_tile_begin[sys + 1] - sv.sys_tile_begin[sys]);
+        const unsigned prev = atomicAdd(&sv.counters[sys], 1u);
+        s_last = (prev == ntiles - 1);
+        if (s_last) {
+            sv.counters[sys] = 0;
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    return s_last != 0;
+}
+
+// Sum of a system's tile partials in tile order (deterministic); called by
+// the whole last CTA, result valid in thread 0.
+template <int ND>
+__device__ __forceinline__ void gather_partials(const SetView& sv, int sys, double (&out)[ND], double* smem)
+{
+    const int t0 = sv.sys_tile_begin[sys], t1 = sv.sys_tile_begin[sys + 1];
+#pragma unroll
+    for (int j = 0; j < ND; ++j) out[j] = 0.0;
+    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < ND; ++j) out[j] += __ldcg(&sv.partials[(long long)t * kMaxDots + j]);
+    }
+    block_reduce<ND>(out, smem);
+}
+
+__device__ __forceinline__ void set_cond(const SetView& sv, unsigned v)
+{
+    if (sv.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)sv.cond, v);
+}
+
+// basic_iteration::finished(r) for a residual norm (basic_iteration.hpp:60-65,
+// 85-93): converged if resid <= rtol*norm_r0 or resid <= atol (atol only when
+// norm_r0 == 0); otherwise "too many iterations" once iter >= max_iter.
+// Returns true when the system stops; retires it from the running count.
+__device__ __forceinline__ bool check_finished(const SetView& sv, SysState& s, double resid)
+{
+    s.resid = resid;
+    bool conv = (s.norm_r0 == 0.0) ? (resid <= s.atol) : (resid <= s.rtol * s.norm_r0 || resid <= s.atol);
+    if (conv) {
+        s.status = MTLG_ST_CONVERGED;
+        s.error = 0;
+    } else if (isnan(resid) || isinf(resid)) {
+        s.status = MTLG_ST_BREAKDOWN;
+        s.error = 1;
+    } else if (s.iter >= s.max_iter) {
+        s.status = MTLG_ST_MAXIT;
+        s.error = 1;
+    } else {
+        return false;
+    }
+    if (atomicSub(sv.running, 1) == 1) set_cond(sv, 0u);
+    return true;
+}
+
+__device__ __forceinline__ void retire(const SetView& sv, SysState& s, int status, int error)
+{
+    s.status = status;
+    s.error = error;
+    if (atomicSub(sv.running, 1) == 1) set_cond(sv, 0u);
+}
+
+}  // namespace mtlg

@@ -1,0 +1,287 @@
+// Host side: context, device memory accounting, CSR / vector handles, tiling.
+#pragma once
+#include "sweep.cuh"
+
+#include <algorithm>
+#include <memory>
+#include <mutex>
+
+struct mtlg_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0;
+    size_t in_use = 0;
+    int64_t launches = 0;
+    int sm_count = 148;
+    int sweep_grid = 148;       // persistent grid of the sweep / factor kernels
+    int* d_scratch_err = nullptr;
+};
+
+namespace mtlg {
+
+static thread_local std::string g_err;
+void set_error(const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+const char* last_error() { return g_err.c_str(); }
+
+inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Device allocation charged to the context (all buffers 256-byte aligned and
+// padded by 16 bytes so vector loads of a tail never leave the allocation).
+inline int dalloc(mtlg_ctx* c, void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    const size_t b = round_up(bytes + 16, 256);
+    if (c->budget && c->in_use + b > c->budget) {
+        set_error("device budget exceeded: %zu + %zu > %zu bytes", c->in_use, b, c->budget);
+        return MTLG_ERR_OOM;
+    }
+    cudaError_t e = cudaMalloc(p, b);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
+        *p = nullptr;
+        return MTLG_ERR_OOM;
+    }
+    c->in_use += b;
+    return MTLG_OK;
+}
+inline void dfree(mtlg_ctx* c, void* p, size_t bytes)
+{
+    if (!p) return;
+    if (bytes == 0) bytes = 16;
+    cudaFree(p);
+    const size_t b = round_up(bytes + 16, 256);
+    c->in_use = c->in_use >= b ? c->in_use - b : 0;
+}
+
+// Typed owning device buffer.
+template <typename T>
+struct DBuf {
+    mtlg_ctx* ctx = nullptr;
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    int alloc(mtlg_ctx* c, size_t count)
+    {
+        release();
+        ctx = c;
+        n = count;
+        void* q = nullptr;
+        int s = dalloc(c, &q, count * sizeof(T));
+        p = static_cast<T*>(q);
+        return s;
+    }
+    int upload(mtlg_ctx* c, const T* h, size_t count)
+    {
+        MTLG_TRY(alloc(c, count));
+        if (count) MTLG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+        return MTLG_OK;
+    }
+    void release()
+    {
+        if (p && ctx) dfree(ctx, p, n * sizeof(T));
+        p = nullptr;
+        n = 0;
+    }
+};
+
+template <typename T>
+inline void tally(mtlg_ctx* c, int64_t k) { c->launches += k; }
+
+// Tiling of one system's rows (see the Tile comment in common.cuh).
+inline void plan_tiles(const int64_t* rp, int n, int sys, std::vector<Tile>& out)
+{
+    int r = 0;
+    while (r < n) {
+        int64_t len = rp[r + 1] - rp[r];
+        if (len > kTileNnz) {
+            out.push_back({sys, r, r + 1, TILE_LONG});
+            ++r;
+            continue;
+        }
+        const int rb = r;
+        int64_t nnz = 0;
+        while (r < n && r - rb < kTileRows) {
+            len = rp[r + 1] - rp[r];
+            if (len > kTileNnz || nnz + len > kTileNnz) break;
+            nnz += len;
+            ++r;
+        }
+        out.push_back({sys, rb, r, TILE_STREAM});
+    }
+}
+
+}  // namespace mtlg
+
+using namespace mtlg;
+
+struct mtlg_vec {
+    mtlg_ctx* ctx = nullptr;
+    int64_t n = 0;
+    int dtype = MTLG_F64;
+    void* p = nullptr;
+    bool owned = false;
+    size_t bytes() const { return size_t(n) * (dtype == MTLG_F64 ? 8 : 4); }
+};
+
+struct mtlg_csr {
+    mtlg_ctx* ctx = nullptr;
+    int64_t n_rows = 0, n_cols = 0, nnz = 0;
+    DBuf<int> rp, ci;
+    DBuf<double> v64;
+    DBuf<float> v32;
+    std::vector<int64_t> h_rp;
+    std::vector<int> h_ci;
+    std::vector<int> h_dpos;       // diagonal position per row (-1: none)
+    DBuf<int> dpos;
+    std::vector<Tile> tiles;
+    int max_row = 0;
+    int64_t tiles_by_kind[3] = {0, 0, 0};
+    // single-system operation set (standalone SpMV / dot)
+    DBuf<Tile> d_tiles;
+    DBuf<int> d_stb;
+    DBuf<double> partials;
+    DBuf<unsigned> counters;
+    DBuf<SysDesc> desc;
+    DBuf<SysState> st;
+    DBuf<int> misc;                // running, err[3]
+};
+
+namespace mtlg {
+
+inline int ensure_f32_values(mtlg_csr* A)
+{
+    if (A->v32.p) return MTLG_OK;
+    MTLG_TRY(A->v32.alloc(A->ctx, size_t(A->nnz)));
+    if (A->nnz) {
+        const int grid = int(std::min<int64_t>((A->nnz + 255) / 256, 4096));
+        k_cast_f64_f32<<<grid, 256, 0, A->ctx->stream>>>(A->nnz, A->v64.p, A->v32.p);
+        A->ctx->launches++;
+        MTLG_CUDA(cudaGetLastError());
+    }
+    return MTLG_OK;
+}
+
+// Single-system set over a CSR's own tiling (standalone operations).
+inline int csr_op_set(mtlg_csr* A, SetView& sv)
+{
+    mtlg_ctx* c = A->ctx;
+    if (!A->d_tiles.p) {
+        MTLG_TRY(A->d_tiles.upload(c, A->tiles.data(), A->tiles.size()));
+        int stb[2] = {0, int(A->tiles.size())};
+        MTLG_TRY(A->d_stb.upload(c, stb, 2));
+        MTLG_TRY(A->partials.alloc(c, std::max<size_t>(1, A->tiles.size()) * kMaxDots));
+        MTLG_TRY(A->counters.alloc(c, 1));
+        MTLG_CUDA(cudaMemsetAsync(A->counters.p, 0, sizeof(unsigned), c->stream));
+        MTLG_TRY(A->desc.alloc(c, 1));
+        MTLG_TRY(A->st.alloc(c, 1));
+        MTLG_CUDA(cudaMemsetAsync(A->st.p, 0, sizeof(SysState), c->stream));
+        MTLG_TRY(A->misc.alloc(c, 4));
+        MTLG_CUDA(cudaMemsetAsync(A->misc.p, 0, 4 * sizeof(int), c->stream));
+    }
+    sv = SetView{};
+    sv.tiles = A->d_tiles.p;
+    sv.n_tiles = int(A->tiles.size());
+    sv.n_sys = 1;
+    sv.sys_tile_begin = A->d_stb.p;
+    sv.desc = A->desc.p;
+    sv.st = A->st.p;
+    sv.partials = A->partials.p;
+    sv.counters = A->counters.p;
+    sv.running = A->misc.p;
+    sv.err = A->misc.p + 1;
+    sv.cond = 0;
+    sv.use_cond = 0;
+    return MTLG_OK;
+}
+
+inline SpmvOp spmv_op_default()
+{
+    SpmvOp op;
+    memset(&op, 0, sizeof op);
+    op.x = SLOT_X;
+    op.y = SLOT_NONE;
+    op.w = SLOT_NONE;
+    op.y2 = SLOT_NONE;
+    op.p = op.z = op.pnew = SLOT_NONE;
+    op.ndot = 0;
+    for (int j = 0; j < kMaxDots; ++j) op.da[j] = op.db[j] = op.dc[j] = OPND_ONE;
+    op.fin = FIN_NONE;
+    op.skip = SKIP_NONE;
+    op.count_body = 0;
+    return op;
+}
+
+inline VecOp vec_op_default(int kind)
+{
+    VecOp op;
+    memset(&op, 0, sizeof op);
+    op.op = kind;
+    op.a = op.b = op.c = op.e = op.f = op.g = SLOT_NONE;
+    for (int j = 0; j < kMaxDots; ++j) op.da[j] = op.db[j] = op.dc[j] = OPND_ONE;
+    op.fin = FIN_NONE;
+    op.skip = SKIP_NONE;
+    return op;
+}
+
+// Kernel dispatchers ---------------------------------------------------------
+template <typename T>
+inline int launch_spmv(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const SpmvOp& op, int xf, int asg)
+{
+    if (sv.n_tiles == 0) return MTLG_OK;
+    dim3 g(sv.n_tiles), b(kBlock);
+#define MTLG_SPMV_CASE(XF, ASG) \
+    if (xf == XF && asg == ASG) { k_spmv<T, XF, ASG><<<g, b, 0, st>>>(sv, op); c->launches++; return MTLG_OK; }
+    MTLG_SPMV_CASE(XF_PLAIN, ASG_SET)
+    MTLG_SPMV_CASE(XF_PLAIN, ASG_ADD)
+    MTLG_SPMV_CASE(XF_PLAIN, ASG_SUB)
+    MTLG_SPMV_CASE(XF_PLAIN, ASG_WMINUS)
+    MTLG_SPMV_CASE(XF_CG_P, ASG_SET)
+    MTLG_SPMV_CASE(XF_CG_P_JAC, ASG_SET)
+#undef MTLG_SPMV_CASE
+    set_error("unsupported SpMV variant %d/%d", xf, asg);
+    return MTLG_ERR_NOT_SUPPORTED;
+}
+
+template <typename T>
+inline int launch_vec(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const VecOp& op)
+{
+    if (sv.n_tiles == 0) return MTLG_OK;
+    dim3 g(sv.n_tiles), b(kBlock);
+    switch (op.op) {
+#define MTLG_VEC_CASE(OP) \
+    case OP: k_vec<T, OP><<<g, b, 0, st>>>(sv, op); break;
+        MTLG_VEC_CASE(VOP_DOT)
+        MTLG_VEC_CASE(VOP_AXPY)
+        MTLG_VEC_CASE(VOP_CG_UPDATE)
+        MTLG_VEC_CASE(VOP_BI_P)
+        MTLG_VEC_CASE(VOP_BI_S)
+        MTLG_VEC_CASE(VOP_BI_XR)
+        MTLG_VEC_CASE(VOP_REF_CAST)
+        MTLG_VEC_CASE(VOP_REF_UPDATE)
+        MTLG_VEC_CASE(VOP_FILL)
+        MTLG_VEC_CASE(VOP_COPY)
+        MTLG_VEC_CASE(VOP_SCALE_COPY)
+#undef MTLG_VEC_CASE
+    default:
+        set_error("unsupported vector op %d", op.op);
+        return MTLG_ERR_NOT_SUPPORTED;
+    }
+    c->launches++;
+    return MTLG_OK;
+}
+
+}  // namespace mtlg

@@ -1,0 +1,521 @@
+// CSR SpMV and fused vector passes with device-side Krylov scalar updates.
+//
+// SpMV follows the reference's row-major CSR product
+// (boost/numeric/mtl/operation/mat_vec_mult.hpp:614-683): every row is an
+// accumulator started at zero and updated entry by entry in storage order,
+// tmp += A.data[j] * v[A.ref_minor()[j]], then assigned/added/subtracted
+// into w (Assign::first_update).  The product is rounded before the addition
+// (the reference build does not fuse this loop).  Rows of up to kShortRow
+// entries keep that exact order (one thread per row), so their results are
+// bitwise the reference's in FP64 and FP32.  Longer rows are split over a
+// warp (or the whole CTA) and summed as a fixed tree.
+#pragma once
+#include "common.cuh"
+
+namespace mtlg {
+
+// ---------------------------------------------------------------- operands
+// Vector operand codes: >= 0 workspace slot, negatives name descriptor
+// vectors; OPND_* are per-row values available in epilogues.
+enum Slot : int { SLOT_X = -1, SLOT_B = -2, SLOT_X64 = -3, SLOT_B64 = -4, SLOT_R64 = -5, SLOT_NONE = -100 };
+enum Opnd : int { OPND_ONE = -1000, OPND_Y = -1001, OPND_XP = -1002, OPND_D = -1003 };
+
+template <typename T>
+__device__ __forceinline__ T* vptr(const SysDesc& d, int slot)
+{
+    if (slot >= 0) return wsvec<T>(d, slot);
+    switch (slot) {
+    case SLOT_X: return static_cast<T*>(d.x);
+    case SLOT_B: return const_cast<T*>(static_cast<const T*>(d.b));
+    default: return nullptr;
+    }
+}
+
+// ---------------------------------------------------------------- finalize
+enum Fin : int {
+    FIN_NONE = 0,
+    FIN_STORE,          // st.dots[j] = sum_j
+    FIN_CG_INIT,        // rr -> finished?  (identity: rho = rr)
+    FIN_CG_INIT_JAC,    // rr, r.Dr -> finished?  rho = r.z
+    FIN_CG_ALPHA,       // p.q -> alpha = rho / p.q, ++iter
+    FIN_CG_UPDATE,      // rr -> finished?  identity: beta = rr / rho
+    FIN_CG_UPDATE_JAC,  // rr, r.z -> finished?  beta = r.z / rho
+    FIN_CG_UPDATE_PC,   // rr -> finished?  (z follows from the sweeps)
+    FIN_CG_RHO,         // r.z after the sweeps -> beta
+    FIN_BI_TOP,         // rt.r, r.r at the loop top (init and after r update)
+    FIN_BI_GAMMA,       // rt.v -> alpha
+    FIN_BI_S,           // s.s -> finished(s)?
+    FIN_BI_OMEGA,       // t.s, t.t -> omega
+    FIN_REF_OUTER,      // FP64 r.r -> refinement stop test, scale
+    FIN_NORM_R0,        // norm_r0 = sqrt(b.b)  (basic_iteration from b)
+    FIN_REF_NB,         // refinement: nb = ||b||_FP64
+    FIN_REF_CG_INIT,    // inner CG init on the scaled residual (norm_r0 = ||r||)
+    FIN_REF_CG_INIT_JAC,
+    FIN_REF_BI_INIT,    // inner BiCGSTAB init (norm_r0 = ||r||)
+};
+
+// Status flags
+enum : int { FLAG_FINISHING = 1 };
+
+__device__ __forceinline__ void bicg_top(const SetView& sv, SysState& s, double rtr, double rr, bool first_pass)
+{
+    if (!first_pass) s.rho_1 = s.rho;  // rho_2 = rho_1 (bicgstab.hpp:75)
+    if (check_finished(sv, s, sqrt(fabs(rr)))) return;
+    s.iter += 1;
+    s.rho = rtr;  // rho_1 = dot(rtilde, r)
+    if (s.rho == 0.0) { retire(sv, s, MTLG_ST_BREAKDOWN, 1); return; }
+    if (s.iter > 1) {
+        if (s.omega == 0.0) { retire(sv, s, MTLG_ST_BREAKDOWN, 1); return; }
+        s.beta = (s.rho / s.rho_1) * (s.alpha / s.omega);
+    }
+}
+
+__device__ void finalize(const SetView& sv, int fin, int sys, const double* dots)
+{
+    SysState& s = sv.st[sys];
+    switch (fin) {
+    case FIN_STORE:
+        for (int j = 0; j < kMaxDots; ++j) s.dots[j] = dots[j];
+        break;
+    case FIN_NORM_R0:
+        s.norm_r0 = sqrt(fabs(dots[0]));
+        break;
+    case FIN_REF_NB:
+        s.nb = sqrt(fabs(dots[0]));
+        break;
+    case FIN_REF_CG_INIT:
+        s.norm_r0 = sqrt(fabs(dots[0]));
+        s.rr = dots[0];
+        s.rho = dots[0];
+        check_finished(sv, s, sqrt(fabs(dots[0])));
+        break;
+    case FIN_REF_CG_INIT_JAC:
+        s.norm_r0 = sqrt(fabs(dots[0]));
+        s.rr = dots[0];
+        s.rho = dots[1];
+        check_finished(sv, s, sqrt(fabs(dots[0])));
+        break;
+    case FIN_REF_BI_INIT:
+        s.norm_r0 = sqrt(fabs(dots[1]));
+        bicg_top(sv, s, dots[0], dots[1], true);
+        break;
+    case FIN_CG_INIT:
+        s.rr = dots[0];
+        s.rho = dots[0];
+        s.iter = 0;
+        check_finished(sv, s, sqrt(fabs(dots[0])));
+        break;
+    case FIN_CG_INIT_JAC:
+        s.rr = dots[0];
+        s.rho = dots[1];
+        s.iter = 0;
+        check_finished(sv, s, sqrt(fabs(dots[0])));
+        break;
+    case FIN_CG_ALPHA:
+        s.dots[0] = dots[0];
+        s.alpha = s.rho / dots[0];
+        s.iter += 1;
+        break;
+    case FIN_CG_UPDATE:
+        s.rr = dots[0];
+        if (!check_finished(sv, s, sqrt(fabs(dots[0])))) {
+            s.rho_1 = s.rho;
+            s.rho = dots[0];
+            s.beta = s.rho / s.rho_1;
+        }
+        break;
+    case FIN_CG_UPDATE_JAC:
+        s.rr = dots[0];
+        if (!check_finished(sv, s, sqrt(fabs(dots[0])))) {
+            s.rho_1 = s.rho;
+            s.rho = dots[1];
+            s.beta = s.rho / s.rho_1;
+        }
+        break;
+    case FIN_CG_UPDATE_PC:
+        s.rr = dots[0];
+        check_finished(sv, s, sqrt(fabs(dots[0])));
+        break;
+    case FIN_CG_RHO:
+        s.rho_1 = s.rho;
+        s.rho = dots[0];
+        s.beta = s.rho / s.rho_1;
+        break;
+    case FIN_BI_TOP:
+        bicg_top(sv, s, dots[0], dots[1], s.iter == 0);
+        break;
+    case FIN_BI_GAMMA:
+        s.gamma = dots[0];
+        if (s.gamma == 0.0) { retire(sv, s, MTLG_ST_BREAKDOWN, 1); break; }
+        s.alpha = s.rho / s.gamma;
+        break;
+    case FIN_BI_S: {
+        // iter.finished(s) (bicgstab.hpp:64): on true, x += alpha*phat is
+        // still due; the x/r pass does it and then retires the system.
+        const double res = sqrt(fabs(dots[0]));
+        s.resid = res;
+        bool conv = (s.norm_r0 == 0.0) ? (res <= s.atol) : (res <= s.rtol * s.norm_r0 || res <= s.atol);
+        if (conv) { s.flags |= FLAG_FINISHING; s.error = 0; s.dots[3] = MTLG_ST_CONVERGED; }
+        else if (isnan(res) || isinf(res)) { retire(sv, s, MTLG_ST_BREAKDOWN, 1); }
+        else if (s.iter >= s.max_iter) { s.flags |= FLAG_FINISHING; s.error = 1; s.dots[3] = MTLG_ST_MAXIT; }
+        break;
+    }
+    case FIN_BI_OMEGA:
+        s.omega = dots[0] / dots[1];
+        break;
+    case FIN_REF_OUTER: {
+        // Refinement stop test on the FP64 residual: ||b - A x|| <= rtol*||b||.
+        const double rn = sqrt(fabs(dots[0]));
+        s.inner_total += s.iter;
+        s.iter = 0;
+        s.scale = rn;
+        s.resid = rn;
+        s.flags = 0;
+        if (rn <= s.outer_rtol * s.nb) {
+            s.ostatus = MTLG_ST_CONVERGED; s.status = MTLG_ST_CONVERGED; s.error = 0;
+        } else if (isnan(rn) || isinf(rn)) {
+            s.ostatus = MTLG_ST_BREAKDOWN; s.status = MTLG_ST_BREAKDOWN; s.error = 1;
+        } else if (s.outer >= s.max_outer) {
+            s.ostatus = MTLG_ST_MAXIT; s.status = MTLG_ST_MAXIT; s.error = 1;
+        } else {
+            s.outer += 1;
+            s.status = MTLG_ST_RUNNING;
+            atomicAdd(sv.running, 1);
+        }
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// ---------------------------------------------------------------- SpMV
+enum XForm : int { XF_PLAIN = 0, XF_CG_P = 1, XF_CG_P_JAC = 2, XF_JAC = 3 };
+enum Assign : int { ASG_SET = 0, ASG_ADD = 1, ASG_SUB = 2, ASG_WMINUS = 3 };
+enum Skip : int { SKIP_NONE = 0, SKIP_INNER = 1, SKIP_OUTER = 2, SKIP_RUNNING = 3 };
+
+struct SpmvOp {
+    int x, y, w;        // input slot, output slot, W for y = W - A x
+    int y2;             // optional second output (copy of y)
+    int p, z, pnew;     // XF_CG_*: old p, z (or r), new p
+    int ndot;
+    int da[kMaxDots], db[kMaxDots], dc[kMaxDots];
+    int fin;
+    int skip;
+    int count_body;     // increments the body counter (first kernel of a loop body)
+};
+
+__device__ __forceinline__ bool skip_system(const SysState& s, int mode)
+{
+    if (mode == SKIP_INNER) return s.status != MTLG_ST_RUNNING || (s.flags & FLAG_FINISHING);
+    if (mode == SKIP_OUTER) return s.ostatus != MTLG_ST_RUNNING;
+    if (mode == SKIP_RUNNING) return s.status != MTLG_ST_RUNNING;
+    return false;
+}
+
+// acc + a*x with the product rounded first (no contraction)
+__device__ __forceinline__ double mac(double acc, double a, double x) { return __dadd_rn(acc, __dmul_rn(a, x)); }
+__device__ __forceinline__ float mac(float acc, float a, float x) { return __fadd_rn(acc, __fmul_rn(a, x)); }
+
+template <typename T, int XF>
+struct XIn {
+    const T* x;
+    const T* p;
+    const T* z;
+    const T* dinv;
+    T beta;
+    bool first;
+    __device__ __forceinline__ T operator()(int j) const
+    {
+        if (XF == XF_PLAIN) return x[j];
+        if (XF == XF_JAC) return dinv[j] * x[j];
+        T zj = (XF == XF_CG_P_JAC) ? dinv[j] * z[j] : z[j];
+        return first ? zj : fma(beta, p[j], zj);
+    }
+};
+
+// Slot codes that name a vector (workspace slot or descriptor vector).
+__device__ __forceinline__ bool names_vector(int code) { return code >= SLOT_B; }
+
+template <typename T, int ASG>
+__device__ __forceinline__ T assign_out(T old_or_w, T acc)
+{
+    if (ASG == ASG_SET) return acc;
+    if (ASG == ASG_ADD) return old_or_w + acc;
+    return old_or_w - acc;  // ASG_SUB and ASG_WMINUS
+}
+
+template <typename T, int ASG, int XF>
+struct RowEpilogue {
+    T* y;
+    T* y2;
+    const T* w;
+    T* pnew;
+    const T* dvec[2 * kMaxDots + kMaxDots];
+    int ndot;
+    const SpmvOp* op;
+    __device__ __forceinline__ void operator()(int i, T acc, T xp, const T* dinv, double (&dot)[kMaxDots]) const
+    {
+        T base = (ASG == ASG_SET) ? T(0) : ((ASG == ASG_WMINUS) ? w[i] : y[i]);
+        T out = assign_out<T, ASG>(base, acc);
+        y[i] = out;
+        if (y2) y2[i] = out;
+        if (XF != XF_PLAIN) pnew[i] = xp;
+        for (int j = 0; j < ndot; ++j) {
+            T a = pick(op->da[j], i, out, xp, dinv, dvec[3 * j + 0]);
+            T b = pick(op->db[j], i, out, xp, dinv, dvec[3 * j + 1]);
+            T c = pick(op->dc[j], i, out, xp, dinv, dvec[3 * j + 2]);
+            dot[j] += double(a * b * c);
+        }
+    }
+    __device__ __forceinline__ static T pick(int code, int i, T y, T xp, const T* dinv, const T* v)
+    {
+        switch (code) {
+        case OPND_ONE: return T(1);
+        case OPND_Y: return y;
+        case OPND_XP: return xp;
+        case OPND_D: return dinv[i];
+        default: return v[i];
+        }
+    }
+};
+
+// One CTA per tile.  Stream tiles stage the tile's values and column
+// indices in shared memory with coalesced loads, then every thread sums one
+// row; rows longer than kShortRow are summed by a warp from shared memory.
+// Long tiles hold one row with more than kTileNnz entries, summed by the CTA
+// straight from global memory.
+template <typename T, int XF, int ASG>
+__global__ void __launch_bounds__(kBlock) k_spmv(SetView sv, SpmvOp op)
+{
+    __shared__ T s_val[kTileNnz];
+    __shared__ int s_col[kTileNnz];
+    __shared__ int s_med[kTileRows];
+    __shared__ int s_nmed;
+    __shared__ double s_red[kMaxDots * 32];
+
+    const int tile_id = blockIdx.x;
+    const Tile tile = sv.tiles[tile_id];
+    const int sys = tile.sys;
+    const SysDesc& d = sv.desc[sys];
+    const SysState& s = sv.st[sys];
+
+    if (op.count_body && tile_id == 0 && threadIdx.x == 0) {
+        // loop-body counter: bounds a graph while-loop independently of
+        // the solver's own termination test
+        int runs = atomicAdd(&sv.err[1], 1) + 1;
+        if (runs > sv.err[2] || *(volatile int*)sv.running <= 0) set_cond(sv, 0u);
+    }
+    if (skip_system(s, op.skip)) return;
+
+    const int* __restrict__ rp = d.rp;
+    const int* __restrict__ ci = d.ci;
+    const T* __restrict__ va = static_cast<const T*>(d.val);
+    XIn<T, XF> xin;
+    xin.x = vptr<T>(d, op.x);
+    xin.p = op.p != SLOT_NONE ? vptr<T>(d, op.p) : nullptr;
+    xin.z = op.z != SLOT_NONE ? vptr<T>(d, op.z) : nullptr;
+    xin.dinv = static_cast<const T*>(d.inv_diag);
+    xin.beta = T(s.beta);
+    xin.first = (s.iter == 0);
+
+    RowEpilogue<T, ASG, XF> epi;
+    epi.y = vptr<T>(d, op.y);
+    epi.y2 = op.y2 != SLOT_NONE ? vptr<T>(d, op.y2) : nullptr;
+    epi.w = op.w != SLOT_NONE ? vptr<T>(d, op.w) : nullptr;
+    epi.pnew = op.pnew != SLOT_NONE ? vptr<T>(d, op.pnew) : nullptr;
+    epi.ndot = op.ndot;
+    epi.op = &op;
+    for (int j = 0; j < kMaxDots; ++j) {
+        epi.dvec[3 * j + 0] = (j < op.ndot && names_vector(op.da[j])) ? vptr<T>(d, op.da[j]) : nullptr;
+        epi.dvec[3 * j + 1] = (j < op.ndot && names_vector(op.db[j])) ? vptr<T>(d, op.db[j]) : nullptr;
+        epi.dvec[3 * j + 2] = (j < op.ndot && names_vector(op.dc[j])) ? vptr<T>(d, op.dc[j]) : nullptr;
+    }
+    double dot[kMaxDots] = {0.0, 0.0, 0.0, 0.0};
+    const T* dinv = xin.dinv;
+
+    if (tile.kind == TILE_STREAM) {
+        const int rb = tile.row_begin, re = tile.row_end;
+        const int k0 = rp[rb], k1 = rp[re];
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+            s_val[k - k0] = va[k];
+            s_col[k - k0] = ci[k];
+        }
+        if (threadIdx.x == 0) s_nmed = 0;
+        __syncthreads();
+        const int i = rb + threadIdx.x;
+        if (i < re) {
+            const int a = rp[i] - k0, e = rp[i + 1] - k0;
+            if (e - a <= kShortRow) {
+                T acc = T(0);
+                for (int k = a; k < e; ++k) acc = mac(acc, s_val[k], xin(s_col[k]));
+                epi(i, acc, xin(i), dinv, dot);
+            } else {
+                s_med[atomicAdd(&s_nmed, 1)] = i;
+            }
+        }
+        __syncthreads();
+        const int nmed = s_nmed;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int m = warp; m < nmed; m += nw) {
+            const int r = s_med[m];
+            const int a = rp[r] - k0, e = rp[r + 1] - k0;
+            T acc = T(0);
+            for (int k = a + lane; k < e; k += 32) acc = mac(acc, s_val[k], xin(s_col[k]));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) epi(r, acc, xin(r), dinv, dot);
+        }
+    } else {
+        const int r = tile.row_begin;
+        const int a = rp[r], e = rp[r + 1];
+        T acc = T(0);
+        for (int k = a + threadIdx.x; k < e; k += blockDim.x) acc = mac(acc, va[k], xin(ci[k]));
+        // fixed-shape CTA tree
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        __shared__ T s_acc[32];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0) s_acc[warp] = acc;
+        __syncthreads();
+        if (warp == 0) {
+            acc = lane < (int)(blockDim.x >> 5) ? s_acc[lane] : T(0);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) epi(r, acc, xin(r), dinv, dot);
+        }
+    }
+
+    if (op.fin == FIN_NONE) return;
+    block_reduce<kMaxDots>(dot, s_red);
+    if (publish_partials<kMaxDots>(sv, tile_id, sys, dot)) {
+        double tot[kMaxDots];
+        gather_partials<kMaxDots>(sv, sys, tot, s_red);
+        if (threadIdx.x == 0) finalize(sv, op.fin, sys, tot);
+    }
+}
+
+// ---------------------------------------------------------------- vector passes
+enum VOp : int {
+    VOP_DOT = 0,        // dots only
+    VOP_AXPY,           // y += a x             (a = op.scalar)
+    VOP_CG_UPDATE,      // x += alpha p ; r -= alpha q
+    VOP_BI_P,           // p = r + beta (p - omega v)   (first: p = r)
+    VOP_BI_S,           // s = r - alpha v
+    VOP_BI_XR,          // x += omega shat + alpha phat ; r = s - omega t  (finishing: x += alpha phat)
+    VOP_REF_CAST,       // r32 = float(r64 / scale); d = 0; z/r inner init
+    VOP_REF_UPDATE,     // x64 += scale * double(d)
+    VOP_FILL,           // v = scalar
+    VOP_COPY,           // y = x
+    VOP_SCALE_COPY,     // y = a x
+};
+
+struct VecOp {
+    int op;
+    int a, b, c, e, f, g;   // slots (meaning per op)
+    int ndot;
+    int da[kMaxDots], db[kMaxDots], dc[kMaxDots];
+    int fin;
+    int skip;
+    int count_body;
+    double scalar;
+};
+
+template <typename T>
+__device__ __forceinline__ T vpick(const T* const* v, int j, int code, int i, const T* dinv)
+{
+    if (code == OPND_ONE) return T(1);
+    if (code == OPND_D) return dinv[i];
+    return v[j][i];
+}
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(kBlock) k_vec(SetView sv, VecOp op)
+{
+    __shared__ double s_red[kMaxDots * 32];
+    const int tile_id = blockIdx.x;
+    const Tile tile = sv.tiles[tile_id];
+    const int sys = tile.sys;
+    const SysDesc& d = sv.desc[sys];
+    SysState& s = sv.st[sys];
+    if (op.count_body && tile_id == 0 && threadIdx.x == 0) {
+        int runs = atomicAdd(&sv.err[1], 1) + 1;
+        if (runs > sv.err[2] || *(volatile int*)sv.running <= 0) set_cond(sv, 0u);
+    }
+    if (skip_system(s, op.skip)) return;
+
+    const T* dinv = static_cast<const T*>(d.inv_diag);
+    const T* dv[3 * kMaxDots];
+    for (int j = 0; j < kMaxDots; ++j) {
+        dv[3 * j + 0] = (j < op.ndot && names_vector(op.da[j])) ? vptr<T>(d, op.da[j]) : nullptr;
+        dv[3 * j + 1] = (j < op.ndot && names_vector(op.db[j])) ? vptr<T>(d, op.db[j]) : nullptr;
+        dv[3 * j + 2] = (j < op.ndot && names_vector(op.dc[j])) ? vptr<T>(d, op.dc[j]) : nullptr;
+    }
+    T* A = op.a != SLOT_NONE ? vptr<T>(d, op.a) : nullptr;
+    T* B = op.b != SLOT_NONE ? vptr<T>(d, op.b) : nullptr;
+    T* C = op.c != SLOT_NONE ? vptr<T>(d, op.c) : nullptr;
+    T* E = op.e != SLOT_NONE ? vptr<T>(d, op.e) : nullptr;
+    T* F = op.f != SLOT_NONE ? vptr<T>(d, op.f) : nullptr;
+    T* G = op.g != SLOT_NONE ? vptr<T>(d, op.g) : nullptr;
+    const bool finishing = (s.flags & FLAG_FINISHING) != 0;
+    const T alpha = T(s.alpha), beta = T(s.beta), omega = T(s.omega);
+    const bool first = (s.iter <= 1);
+    double dot[kMaxDots] = {0.0, 0.0, 0.0, 0.0};
+
+    for (int i = tile.row_begin + threadIdx.x; i < tile.row_end; i += blockDim.x) {
+        if (OP == VOP_AXPY) {
+            A[i] = fma(T(op.scalar), B[i], A[i]);                       // A += s B
+        } else if (OP == VOP_CG_UPDATE) {
+            A[i] = fma(alpha, B[i], A[i]);                              // x += alpha p
+            C[i] = fma(-alpha, E[i], C[i]);                             // r -= alpha q
+        } else if (OP == VOP_BI_P) {
+            // p = r + beta * (p - omega * v)     (bicgstab.hpp:49-53)
+            A[i] = first ? B[i] : fma(beta, fma(-omega, C[i], A[i]), B[i]);
+        } else if (OP == VOP_BI_S) {
+            A[i] = fma(-alpha, C[i], B[i]);                             // s = r - alpha v
+        } else if (OP == VOP_BI_XR) {
+            // A x, B phat, C shat, E s, F t, G r
+            if (finishing) {
+                A[i] = fma(alpha, B[i], A[i]);                          // x += alpha phat
+            } else {
+                A[i] = A[i] + fma(omega, C[i], alpha * B[i]);           // x += omega shat + alpha phat
+                G[i] = fma(-omega, F[i], E[i]);                         // r = s - omega t
+            }
+        } else if (OP == VOP_REF_CAST) {
+            // inner right-hand side float(r64 / ||r64||); inner x = 0, r = b
+            const T bi = T(d.r64[i] / s.scale);
+            A[i] = bi;
+            if (B) B[i] = T(0);
+            if (C) C[i] = bi;
+            if (E) E[i] = bi;
+        } else if (OP == VOP_REF_UPDATE) {
+            d.x64[i] = fma(s.scale, double(A[i]), d.x64[i]);          // x += ||r|| * d
+        } else if (OP == VOP_FILL) {
+            A[i] = T(op.scalar);
+        } else if (OP == VOP_COPY) {
+            A[i] = B[i];
+        } else if (OP == VOP_SCALE_COPY) {
+            A[i] = T(op.scalar) * B[i];
+        }
+        for (int j = 0; j < op.ndot; ++j) {
+            dot[j] += double(vpick<T>(dv, 3 * j + 0, op.da[j], i, dinv) * vpick<T>(dv, 3 * j + 1, op.db[j], i, dinv) *
+                             vpick<T>(dv, 3 * j + 2, op.dc[j], i, dinv));
+        }
+    }
+    if (op.fin == FIN_NONE && !(OP == VOP_BI_XR && finishing)) return;
+    block_reduce<kMaxDots>(dot, s_red);
+    if (publish_partials<kMaxDots>(sv, tile_id, sys, dot)) {
+        double tot[kMaxDots];
+        gather_partials<kMaxDots>(sv, sys, tot, s_red);
+        if (threadIdx.x == 0) {
+            if (OP == VOP_BI_XR && finishing) {
+                s.flags &= ~FLAG_FINISHING;
+                retire(sv, s, (int)s.dots[3], s.error);
+            } else {
+                finalize(sv, op.fin, sys, tot);
+            }
+        }
+    }
+}
+
+}  // namespace mtlg

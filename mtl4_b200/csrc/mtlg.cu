@@ -1,0 +1,786 @@
+// mtl4_b200: C ABI of the sparse-solve hot path on one B200 (sm_100a).
+// The declarations and the reference interface each entry point replaces are
+// in include/mtl4_b200/mtlg.h.
+#include "host_solve.cuh"
+
+#include <map>
+
+using namespace mtlg;
+
+namespace mtlg {
+
+// Cache of single-system solve sets (reused across calls with the same
+// operator and preconditioner so their loop graphs are built once).
+struct SetKey {
+    const mtlg_csr* A;
+    const mtlg_pc* P;
+    int solver, f32, mixed;
+    bool operator<(const SetKey& o) const
+    {
+        return std::tie(A, P, solver, f32, mixed) < std::tie(o.A, o.P, o.solver, o.f32, o.mixed);
+    }
+};
+
+struct CtxExtra {
+    std::map<SetKey, std::unique_ptr<SolveSet>> sets;
+    // vector-only tile sets, by length
+    struct VecSet {
+        DBuf<Tile> tiles;
+        DBuf<int> stb;
+        DBuf<double> partials;
+        DBuf<unsigned> counters;
+        DBuf<SysDesc> desc;
+        DBuf<SysState> st;
+        DBuf<int> misc;
+        int n_tiles = 0;
+    };
+    std::map<int64_t, std::unique_ptr<VecSet>> vsets;
+};
+
+static std::mutex g_extra_mu;
+static std::map<const mtlg_ctx*, std::unique_ptr<CtxExtra>> g_extra;
+
+inline CtxExtra& extra(const mtlg_ctx* c)
+{
+    std::lock_guard<std::mutex> lk(g_extra_mu);
+    auto& e = g_extra[c];
+    if (!e) e.reset(new CtxExtra);
+    return *e;
+}
+
+inline void purge_sets(const mtlg_ctx* c, const void* obj)
+{
+    CtxExtra& e = extra(c);
+    for (auto it = e.sets.begin(); it != e.sets.end();) {
+        if (it->first.A == obj || it->first.P == obj) it = e.sets.erase(it);
+        else ++it;
+    }
+}
+
+inline int vec_set(mtlg_ctx* c, int64_t n, SetView& sv)
+{
+    auto& vs = extra(c).vsets[n];
+    if (!vs) {
+        vs.reset(new CtxExtra::VecSet);
+        std::vector<Tile> tiles;
+        for (int64_t r = 0; r < n; r += kTileRows) tiles.push_back({0, int(r), int(std::min<int64_t>(n, r + kTileRows)), TILE_STREAM});
+        vs->n_tiles = int(tiles.size());
+        MTLG_TRY(vs->tiles.upload(c, tiles.data(), std::max<size_t>(1, tiles.size())));
+        int stb[2] = {0, vs->n_tiles};
+        MTLG_TRY(vs->stb.upload(c, stb, 2));
+        MTLG_TRY(vs->partials.alloc(c, size_t(std::max(1, vs->n_tiles)) * kMaxDots));
+        MTLG_TRY(vs->counters.alloc(c, 1));
+        MTLG_CUDA(cudaMemsetAsync(vs->counters.p, 0, sizeof(unsigned), c->stream));
+        MTLG_TRY(vs->desc.alloc(c, 1));
+        MTLG_TRY(vs->st.alloc(c, 1));
+        MTLG_TRY(vs->misc.alloc(c, 4));
+        MTLG_CUDA(cudaMemsetAsync(vs->misc.p, 0, 4 * sizeof(int), c->stream));
+    }
+    sv = SetView{};
+    sv.tiles = vs->tiles.p;
+    sv.n_tiles = vs->n_tiles;
+    sv.n_sys = 1;
+    sv.sys_tile_begin = vs->stb.p;
+    sv.desc = vs->desc.p;
+    sv.st = vs->st.p;
+    sv.partials = vs->partials.p;
+    sv.counters = vs->counters.p;
+    sv.running = vs->misc.p;
+    sv.err = vs->misc.p + 1;
+    return MTLG_OK;
+}
+
+inline int read_dots(mtlg_ctx* c, SysState* st, double* out, int nd)
+{
+    SysState h;
+    MTLG_CUDA(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    for (int j = 0; j < nd; ++j) out[j] = h.dots[j];
+    return MTLG_OK;
+}
+
+inline bool ok_dtype(int d) { return d == MTLG_F64 || d == MTLG_F32; }
+
+}  // namespace mtlg
+
+namespace mtlg {
+template <typename T, typename S>
+int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
+{
+    mtlg_ctx* c = P->ctx;
+    SetView sv = SetView{};
+    sv.n_sys = 1;
+    sv.desc = P->desc.p;
+    sv.st = P->st.p;
+    sv.running = P->misc.p;
+    sv.err = P->misc.p + 1;
+    SysDesc d;
+    memset(&d, 0, sizeof d);
+    d.n = P->n;
+    d.x = x->p;
+    d.b = y->p;
+    d.ws = P->tmp.p;
+    d.ws_stride = 0;
+    d.L = TriFactor{P->L.rp.p, P->L.ci.p, P->L.val.p, P->L.dia.p, P->L.row_of.p};
+    d.U = TriFactor{P->U.rp.p, P->U.ci.p, P->U.val.p, P->U.dia.p, P->U.row_of.p};
+    MTLG_CUDA(cudaMemcpyAsync(P->desc.p, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
+    SweepOp op;
+    memset(&op, 0, sizeof op);
+    op.skip = SKIP_NONE;
+    op.fuse = SWF_NONE;
+    // y0 = L^{-1} x  (temp, slot 0); clears y row by row
+    op.tasks = P->L.tasks.p; op.ntasks = int(P->L.tasks.n); op.ticket = P->tickets.p + 0; op.which = 0;
+    op.in = SLOT_X; op.out = 0; op.reset = SLOT_B;
+    if (op.ntasks) { k_sweep<T, S><<<c->sweep_grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
+    // y = U^{-1} y0; clears the temp again
+    op.tasks = P->U.tasks.p; op.ntasks = int(P->U.tasks.n); op.ticket = P->tickets.p + 1; op.which = 1;
+    op.in = 0; op.out = SLOT_B; op.reset = 0;
+    if (op.ntasks) { k_sweep<T, S><<<c->sweep_grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
+    MTLG_CUDA(cudaGetLastError());
+    int err = 0;
+    MTLG_CUDA(cudaMemcpyAsync(&err, P->misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    if (err) {
+        int z = 0;
+        MTLG_CUDA(cudaMemcpy(P->misc.p + 1, &z, sizeof z, cudaMemcpyHostToDevice));
+        MTLG_CUDA(cudaMemset(P->tickets.p, 0, 8 * sizeof(int)));
+        MTLG_TRY(fill_sentinel(c, P->tmp.p, size_t(P->n) * 8));
+        set_error("triangular sweep dependency wait expired");
+        return MTLG_ERR_TIMEOUT;
+    }
+    return MTLG_OK;
+}
+
+}  // namespace mtlg
+
+extern "C" {
+
+const char* mtlg_status_string(int s)
+{
+    switch (s) {
+    case MTLG_OK: return "ok";
+    case MTLG_ERR_INVALID_ARG: return "invalid argument";
+    case MTLG_ERR_NOT_SQUARE: return "matrix not square";
+    case MTLG_ERR_MISSING_DIAGONAL: return "missing diagonal";
+    case MTLG_ERR_ZERO_PIVOT: return "zero pivot";
+    case MTLG_ERR_BREAKDOWN: return "unexpected orthogonality (breakdown)";
+    case MTLG_ERR_OOM: return "out of device memory";
+    case MTLG_ERR_TIMEOUT: return "device wait timed out";
+    case MTLG_ERR_CUDA: return "CUDA error";
+    case MTLG_ERR_INCOMPATIBLE_SIZE: return "incompatible size";
+    case MTLG_ERR_UNSORTED: return "CSR rows must be sorted and in range";
+    case MTLG_ERR_TOO_LARGE: return "too large for 32-bit device indexing";
+    case MTLG_ERR_NOT_SUPPORTED: return "not supported";
+    case MTLG_ERR_ADMISSION: return "request exceeds the device budget";
+    case MTLG_ERR_NOT_FOUND: return "unknown request";
+    case MTLG_PENDING: return "pending";
+    default: return "unknown status";
+    }
+}
+
+const char* mtlg_last_error_message(void) { return last_error(); }
+
+// ------------------------------------------------------------------ context
+int mtlg_ctx_create(int device, size_t hbm_budget, mtlg_ctx** out)
+{
+    MTLG_CHECK_ARG(out, "out");
+    *out = nullptr;
+    int ndev = 0;
+    MTLG_CUDA(cudaGetDeviceCount(&ndev));
+    MTLG_CHECK_ARG(device >= 0 && device < ndev, "device index");
+    MTLG_CUDA(cudaSetDevice(device));
+    std::unique_ptr<mtlg_ctx> c(new mtlg_ctx);
+    c->device = device;
+    c->budget = hbm_budget;
+    MTLG_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    MTLG_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    int nb = 1, nb2 = 1;
+    MTLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sweep<double, double>, kBlock, 0));
+    MTLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_ilu0_factor, kBlock, 0));
+    c->sweep_grid = c->sm_count * std::max(1, std::min(nb, nb2));
+    *out = c.release();
+    return MTLG_OK;
+}
+
+int mtlg_ctx_destroy(mtlg_ctx* c)
+{
+    if (!c) return MTLG_OK;
+    cudaStreamSynchronize(c->stream);
+    {
+        std::unique_ptr<CtxExtra> e;
+        {
+            std::lock_guard<std::mutex> lk(g_extra_mu);
+            auto it = g_extra.find(c);
+            if (it != g_extra.end()) {
+                e = std::move(it->second);
+                g_extra.erase(it);
+            }
+        }
+    }
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return MTLG_OK;
+}
+
+int mtlg_ctx_synchronize(mtlg_ctx* c)
+{
+    MTLG_CHECK_ARG(c, "ctx");
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    return MTLG_OK;
+}
+
+int mtlg_ctx_set_stream(mtlg_ctx* c, void* s)
+{
+    MTLG_CHECK_ARG(c, "ctx");
+    c->stream = s ? static_cast<cudaStream_t>(s) : c->own_stream;
+    return MTLG_OK;
+}
+
+void* mtlg_ctx_stream(mtlg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+int64_t mtlg_ctx_kernel_launches(mtlg_ctx* c) { return c ? c->launches : 0; }
+size_t mtlg_ctx_bytes_in_use(mtlg_ctx* c) { return c ? c->in_use : 0; }
+
+// ------------------------------------------------------------------ CSR
+int mtlg_csr_create(mtlg_ctx* c, int64_t n_rows, int64_t n_cols, int64_t nnz, const int64_t* row_ptr,
+                    const int32_t* col, const void* val, mtlg_dtype val_dtype, mtlg_csr** out)
+{
+    MTLG_CHECK_ARG(c && out, "ctx/out");
+    *out = nullptr;
+    MTLG_CHECK_ARG(n_rows >= 0 && n_cols >= 0 && nnz >= 0, "negative size");
+    MTLG_CHECK_ARG(row_ptr && (nnz == 0 || (col && val)), "null array");
+    MTLG_CHECK_ARG(ok_dtype(val_dtype), "dtype");
+    if (n_rows > INT32_MAX - 1 || n_cols > INT32_MAX || nnz > INT32_MAX - 1) {
+        set_error("n or nnz beyond 32-bit device indexing");
+        return MTLG_ERR_TOO_LARGE;
+    }
+    if (row_ptr[0] != 0 || row_ptr[n_rows] != nnz) {
+        set_error("row_ptr must start at 0 and end at nnz");
+        return MTLG_ERR_INVALID_ARG;
+    }
+    std::unique_ptr<mtlg_csr> A(new mtlg_csr);
+    A->ctx = c;
+    A->n_rows = n_rows;
+    A->n_cols = n_cols;
+    A->nnz = nnz;
+    A->h_rp.assign(row_ptr, row_ptr + n_rows + 1);
+    A->h_ci.assign(col, col + nnz);
+    A->h_dpos.assign(size_t(n_rows), -1);
+    std::vector<int> rp32(size_t(n_rows) + 1);
+    for (int64_t i = 0; i < n_rows; ++i) {
+        const int64_t a = row_ptr[i], e = row_ptr[i + 1];
+        if (e < a) {
+            set_error("row_ptr decreases at row %lld", (long long)i);
+            return MTLG_ERR_INVALID_ARG;
+        }
+        A->max_row = std::max<int>(A->max_row, int(e - a));
+        for (int64_t k = a; k < e; ++k) {
+            if (col[k] < 0 || col[k] >= n_cols || (k > a && col[k] <= col[k - 1])) {
+                set_error("row %lld: columns must be sorted, distinct and in range", (long long)i);
+                return MTLG_ERR_UNSORTED;
+            }
+            if (col[k] == i) A->h_dpos[i] = int(k);
+        }
+        rp32[i] = int(a);
+    }
+    rp32[n_rows] = int(nnz);
+    plan_tiles(A->h_rp.data(), int(n_rows), 0, A->tiles);
+    for (const Tile& t : A->tiles) A->tiles_by_kind[t.kind]++;
+    MTLG_TRY(A->rp.upload(c, rp32.data(), rp32.size()));
+    MTLG_TRY(A->ci.upload(c, col, size_t(nnz)));
+    MTLG_TRY(A->dpos.upload(c, A->h_dpos.data(), std::max<size_t>(1, A->h_dpos.size())));
+    if (val_dtype == MTLG_F64) {
+        MTLG_TRY(A->v64.upload(c, static_cast<const double*>(val), size_t(nnz)));
+    } else {
+        std::vector<double> w(static_cast<const float*>(val), static_cast<const float*>(val) + nnz);
+        MTLG_TRY(A->v64.upload(c, w.data(), size_t(nnz)));
+        MTLG_TRY(A->v32.upload(c, static_cast<const float*>(val), size_t(nnz)));
+    }
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    *out = A.release();
+    return MTLG_OK;
+}
+
+int mtlg_csr_destroy(mtlg_csr* A)
+{
+    if (!A) return MTLG_OK;
+    cudaStreamSynchronize(A->ctx->stream);
+    purge_sets(A->ctx, A);
+    delete A;
+    return MTLG_OK;
+}
+
+int mtlg_csr_info(const mtlg_csr* A, int64_t* n_rows, int64_t* n_cols, int64_t* nnz)
+{
+    MTLG_CHECK_ARG(A, "csr");
+    if (n_rows) *n_rows = A->n_rows;
+    if (n_cols) *n_cols = A->n_cols;
+    if (nnz) *nnz = A->nnz;
+    return MTLG_OK;
+}
+
+int mtlg_csr_update_values(mtlg_csr* A, const void* val, mtlg_dtype dt)
+{
+    MTLG_CHECK_ARG(A && (val || A->nnz == 0) && ok_dtype(dt), "csr/val/dtype");
+    mtlg_ctx* c = A->ctx;
+    if (dt == MTLG_F64) {
+        MTLG_CUDA(cudaMemcpyAsync(A->v64.p, val, size_t(A->nnz) * 8, cudaMemcpyHostToDevice, c->stream));
+    } else {
+        std::vector<double> w(static_cast<const float*>(val), static_cast<const float*>(val) + A->nnz);
+        MTLG_CUDA(cudaMemcpyAsync(A->v64.p, w.data(), size_t(A->nnz) * 8, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (A->v32.p) {
+        A->v32.release();
+        MTLG_TRY(ensure_f32_values(A));
+    }
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    return MTLG_OK;
+}
+
+int mtlg_csr_plan_info(const mtlg_csr* A, int64_t* tiles_by_kind3, int* max_row_len)
+{
+    MTLG_CHECK_ARG(A, "csr");
+    if (tiles_by_kind3) for (int k = 0; k < 3; ++k) tiles_by_kind3[k] = A->tiles_by_kind[k];
+    if (max_row_len) *max_row_len = A->max_row;
+    return MTLG_OK;
+}
+
+// ------------------------------------------------------------------ vectors
+int mtlg_vec_create(mtlg_ctx* c, int64_t n, mtlg_dtype dt, mtlg_vec** out)
+{
+    MTLG_CHECK_ARG(c && out && n >= 0 && ok_dtype(dt), "ctx/out/n/dtype");
+    *out = nullptr;
+    std::unique_ptr<mtlg_vec> v(new mtlg_vec);
+    v->ctx = c;
+    v->n = n;
+    v->dtype = dt;
+    v->owned = true;
+    MTLG_TRY(dalloc(c, &v->p, v->bytes()));
+    MTLG_CUDA(cudaMemsetAsync(v->p, 0, v->bytes(), c->stream));
+    *out = v.release();
+    return MTLG_OK;
+}
+
+int mtlg_vec_wrap(mtlg_ctx* c, int64_t n, mtlg_dtype dt, void* p, mtlg_vec** out)
+{
+    MTLG_CHECK_ARG(c && out && n >= 0 && ok_dtype(dt) && (p || n == 0), "ctx/out/n/dtype/ptr");
+    std::unique_ptr<mtlg_vec> v(new mtlg_vec);
+    v->ctx = c;
+    v->n = n;
+    v->dtype = dt;
+    v->p = p;
+    v->owned = false;
+    *out = v.release();
+    return MTLG_OK;
+}
+
+int mtlg_vec_destroy(mtlg_vec* v)
+{
+    if (!v) return MTLG_OK;
+    if (v->owned) {
+        cudaStreamSynchronize(v->ctx->stream);
+        dfree(v->ctx, v->p, v->bytes());
+    }
+    delete v;
+    return MTLG_OK;
+}
+
+int mtlg_vec_upload(mtlg_vec* v, const void* h, int64_t n)
+{
+    MTLG_CHECK_ARG(v && (h || n == 0), "vec/host");
+    if (n != v->n) {
+        set_error("upload of %lld elements into a vector of %lld", (long long)n, (long long)v->n);
+        return MTLG_ERR_INCOMPATIBLE_SIZE;
+    }
+    MTLG_CUDA(cudaMemcpyAsync(v->p, h, v->bytes(), cudaMemcpyHostToDevice, v->ctx->stream));
+    return MTLG_OK;
+}
+
+int mtlg_vec_download(const mtlg_vec* v, void* h, int64_t n)
+{
+    MTLG_CHECK_ARG(v && (h || n == 0), "vec/host");
+    if (n != v->n) {
+        set_error("download of %lld elements from a vector of %lld", (long long)n, (long long)v->n);
+        return MTLG_ERR_INCOMPATIBLE_SIZE;
+    }
+    MTLG_CUDA(cudaMemcpyAsync(h, v->p, v->bytes(), cudaMemcpyDeviceToHost, v->ctx->stream));
+    MTLG_CUDA(cudaStreamSynchronize(v->ctx->stream));
+    return MTLG_OK;
+}
+
+int mtlg_vec_fill(mtlg_vec* v, double value)
+{
+    MTLG_CHECK_ARG(v, "vec");
+    mtlg_ctx* c = v->ctx;
+    if (v->n == 0) return MTLG_OK;
+    SetView sv;
+    MTLG_TRY(vec_set(c, v->n, sv));
+    SysDesc d;
+    memset(&d, 0, sizeof d);
+    d.x = v->p;
+    MTLG_CUDA(cudaMemcpyAsync(sv.desc, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
+    VecOp op = vec_op_default(VOP_FILL);
+    op.a = SLOT_X;
+    op.scalar = value;
+    return v->dtype == MTLG_F64 ? launch_vec<double>(c, c->stream, sv, op) : launch_vec<float>(c, c->stream, sv, op);
+}
+
+void* mtlg_vec_device_ptr(const mtlg_vec* v) { return v ? v->p : nullptr; }
+int64_t mtlg_vec_size(const mtlg_vec* v) { return v ? v->n : -1; }
+
+// ------------------------------------------------------------------ SpMV / level 1
+static int spmv_impl(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, int assign, double* pq)
+{
+    MTLG_CHECK_ARG(c && A && x && y, "null handle");
+    MTLG_CHECK_ARG(x->dtype == y->dtype, "x and y dtypes differ");
+    MTLG_CHECK_ARG(assign >= MTLG_ASSIGN && assign <= MTLG_MINUS, "assign");
+    if (x->n != A->n_cols || y->n != A->n_rows) {
+        set_error("SpMV sizes: A %lldx%lld, x %lld, y %lld", (long long)A->n_rows, (long long)A->n_cols,
+                  (long long)x->n, (long long)y->n);
+        return MTLG_ERR_INCOMPATIBLE_SIZE;
+    }
+    const bool f32 = x->dtype == MTLG_F32;
+    if (f32) MTLG_TRY(ensure_f32_values(A));
+    SetView sv;
+    MTLG_TRY(csr_op_set(A, sv));
+    SysDesc d;
+    memset(&d, 0, sizeof d);
+    d.n = int(A->n_rows);
+    d.nnz = int(A->nnz);
+    d.rp = A->rp.p;
+    d.ci = A->ci.p;
+    d.val = f32 ? (const void*)A->v32.p : (const void*)A->v64.p;
+    d.val64 = A->v64.p;
+    d.x = x->p;
+    d.b = y->p;
+    MTLG_CUDA(cudaMemcpyAsync(sv.desc, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
+    SpmvOp op = spmv_op_default();
+    op.x = SLOT_X;
+    op.y = SLOT_B;
+    if (pq) {
+        set_dot(op, 0, OPND_XP, OPND_Y);
+        op.fin = FIN_STORE;
+    }
+    const int asg = assign == MTLG_ASSIGN ? ASG_SET : (assign == MTLG_PLUS ? ASG_ADD : ASG_SUB);
+    if (f32) MTLG_TRY(launch_spmv<float>(c, c->stream, sv, op, XF_PLAIN, asg));
+    else MTLG_TRY(launch_spmv<double>(c, c->stream, sv, op, XF_PLAIN, asg));
+    MTLG_CUDA(cudaGetLastError());
+    if (pq) return read_dots(c, sv.st, pq, 1);
+    return MTLG_OK;
+}
+
+int mtlg_spmv(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, int assign)
+{
+    return spmv_impl(c, A, x, y, assign, nullptr);
+}
+
+int mtlg_spmv_dot(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* p, mtlg_vec* q, double* pq)
+{
+    MTLG_CHECK_ARG(pq, "pq");
+    return spmv_impl(c, A, p, q, MTLG_ASSIGN, pq);
+}
+
+static int vec_binary(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, int kind, double scalar, double* out)
+{
+    MTLG_CHECK_ARG(c && x && y, "null handle");
+    MTLG_CHECK_ARG(x->dtype == y->dtype, "dtypes differ");
+    if (x->n != y->n) {
+        set_error("vector sizes %lld and %lld", (long long)x->n, (long long)y->n);
+        return MTLG_ERR_INCOMPATIBLE_SIZE;
+    }
+    if (x->n == 0) {
+        if (out) *out = 0.0;
+        return MTLG_OK;
+    }
+    SetView sv;
+    MTLG_TRY(vec_set(c, x->n, sv));
+    SysDesc d;
+    memset(&d, 0, sizeof d);
+    d.x = x->p;
+    d.b = y->p;
+    MTLG_CUDA(cudaMemcpyAsync(sv.desc, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
+    VecOp op = vec_op_default(kind);
+    if (kind == VOP_DOT) {
+        set_dot(op, 0, SLOT_X, SLOT_B);
+        op.fin = FIN_STORE;
+    } else {  // VOP_AXPY: y += a x
+        op.a = SLOT_B;
+        op.b = SLOT_X;
+        op.scalar = scalar;
+    }
+    if (x->dtype == MTLG_F64) MTLG_TRY(launch_vec<double>(c, c->stream, sv, op));
+    else MTLG_TRY(launch_vec<float>(c, c->stream, sv, op));
+    MTLG_CUDA(cudaGetLastError());
+    if (out) return read_dots(c, sv.st, out, 1);
+    return MTLG_OK;
+}
+
+int mtlg_dot(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, double* out)
+{
+    MTLG_CHECK_ARG(out, "out");
+    return vec_binary(c, x, y, VOP_DOT, 0.0, out);
+}
+
+int mtlg_two_norm(mtlg_ctx* c, const mtlg_vec* x, double* out)
+{
+    MTLG_CHECK_ARG(out, "out");
+    MTLG_TRY(vec_binary(c, x, x, VOP_DOT, 0.0, out));
+    *out = sqrt(fabs(*out));
+    return MTLG_OK;
+}
+
+int mtlg_axpy(mtlg_ctx* c, double a, const mtlg_vec* x, mtlg_vec* y) { return vec_binary(c, x, y, VOP_AXPY, a, nullptr); }
+
+// ------------------------------------------------------------------ preconditioners
+int mtlg_pc_create(mtlg_ctx* c, mtlg_csr* A, int kind, mtlg_dtype storage, mtlg_pc** out)
+{
+    MTLG_CHECK_ARG(c && A && out, "null handle");
+    MTLG_CHECK_ARG(kind >= MTLG_PC_IDENTITY && kind <= MTLG_PC_IC0, "pc kind");
+    MTLG_CHECK_ARG(ok_dtype(storage), "storage dtype");
+    *out = nullptr;
+    if (A->n_rows != A->n_cols) {
+        set_error("preconditioner of a %lldx%lld matrix", (long long)A->n_rows, (long long)A->n_cols);
+        return MTLG_ERR_NOT_SQUARE;
+    }
+    std::unique_ptr<mtlg_pc> P(new mtlg_pc);
+    P->ctx = c;
+    P->A = A;
+    P->kind = kind;
+    P->storage = storage;
+    P->n = int(A->n_rows);
+    MTLG_TRY(pc_build(P.get()));
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    *out = P.release();
+    return MTLG_OK;
+}
+
+int mtlg_pc_destroy(mtlg_pc* P)
+{
+    if (!P) return MTLG_OK;
+    cudaStreamSynchronize(P->ctx->stream);
+    purge_sets(P->ctx, P);
+    delete P;
+    return MTLG_OK;
+}
+
+int mtlg_pc_apply(mtlg_ctx* c, mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
+{
+    MTLG_CHECK_ARG(c && P && x && y, "null handle");
+    MTLG_CHECK_ARG(x->dtype == y->dtype, "x and y dtypes differ");
+    if (x->n != P->n || y->n != P->n) {
+        set_error("preconditioner of size %d applied to %lld -> %lld", P->n, (long long)x->n, (long long)y->n);
+        return MTLG_ERR_INCOMPATIBLE_SIZE;
+    }
+    if (P->n == 0) return MTLG_OK;
+    if (P->kind == MTLG_PC_IDENTITY) {
+        if (x->p != y->p) MTLG_CUDA(cudaMemcpyAsync(y->p, x->p, x->bytes(), cudaMemcpyDeviceToDevice, c->stream));
+        return MTLG_OK;
+    }
+    const bool t32 = x->dtype == MTLG_F32, s32 = P->storage == MTLG_F32;
+    if (t32 && !s32) return pc_sweeps<float, double>(P, x, y);
+    if (t32 && s32) return pc_sweeps<float, float>(P, x, y);
+    if (!t32 && s32) return pc_sweeps<double, float>(P, x, y);
+    return pc_sweeps<double, double>(P, x, y);
+}
+
+int mtlg_pc_adjoint_apply(mtlg_ctx* c, mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
+{
+    MTLG_CHECK_ARG(P, "pc");
+    // identity, diagonal (real) and IC(0) are self-adjoint (ic_0.hpp:88-100)
+    if (P->kind != MTLG_PC_ILU0) return mtlg_pc_apply(c, P, x, y);
+    set_error("adjoint ILU(0) apply is not implemented");
+    return MTLG_ERR_NOT_SUPPORTED;
+}
+
+int mtlg_pc_factor(const mtlg_pc* P, int which, int64_t* nnz, int64_t* row_ptr, int32_t* col, double* val)
+{
+    MTLG_CHECK_ARG(P && (which == 0 || which == 1), "pc/which");
+    if (!P->has_factors()) {
+        set_error("preconditioner has no triangular factors");
+        return MTLG_ERR_NOT_SUPPORTED;
+    }
+    const TriDev& T = which == 0 ? P->L : P->U;
+    const bool has_diag = !(P->kind == MTLG_PC_ILU0 && which == 0);
+    const bool diag_first = which == 1;  // U: diagonal first; IC's L: last
+    const int64_t total = T.nnz + (has_diag ? P->n : 0);
+    if (nnz) *nnz = total;
+    if (!row_ptr && !col && !val) return MTLG_OK;
+    mtlg_ctx* c = P->ctx;
+    const size_t ss = P->ssize();
+    std::vector<unsigned char> hv(size_t(std::max(T.nnz, 1)) * ss), hd(size_t(std::max(T.npad, 1)) * ss);
+    MTLG_CUDA(cudaMemcpyAsync(hv.data(), T.val.p, size_t(T.nnz) * ss, cudaMemcpyDeviceToHost, c->stream));
+    MTLG_CUDA(cudaMemcpyAsync(hd.data(), T.dia.p, size_t(T.npad) * ss, cudaMemcpyDeviceToHost, c->stream));
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    auto getv = [&](const std::vector<unsigned char>& b, size_t i) -> double {
+        if (ss == 8) { double v; memcpy(&v, &b[i * 8], 8); return v; }
+        float v; memcpy(&v, &b[i * 4], 4); return double(v);
+    };
+    std::vector<int> kof(P->n, -1);
+    for (int k = 0; k < T.npad; ++k) if (T.h_row_of[k] >= 0) kof[T.h_row_of[k]] = k;
+    int64_t o = 0;
+    if (row_ptr) row_ptr[0] = 0;
+    for (int i = 0; i < P->n; ++i) {
+        const int k = kof[i];
+        if (has_diag && diag_first) { if (col) col[o] = i; if (val) val[o] = getv(hd, k); ++o; }
+        for (int e = T.h_rp[k]; e < T.h_rp[k + 1]; ++e, ++o) {
+            if (col) col[o] = T.h_ci[e];
+            if (val) val[o] = getv(hv, e);
+        }
+        if (has_diag && !diag_first) { if (col) col[o] = i; if (val) val[o] = getv(hd, k); ++o; }
+        if (row_ptr) row_ptr[i + 1] = o;
+    }
+    return MTLG_OK;
+}
+
+int mtlg_pc_levels(const mtlg_pc* P, int* levels_L, int* levels_U)
+{
+    MTLG_CHECK_ARG(P, "pc");
+    if (levels_L) *levels_L = P->L.nlev;
+    if (levels_U) *levels_U = P->U.nlev;
+    return MTLG_OK;
+}
+
+// ------------------------------------------------------------------ solves
+static int check_solve_args(int solver, mtlg_csr* A, mtlg_vec* x, const mtlg_vec* b, const mtlg_pc* P)
+{
+    MTLG_CHECK_ARG(A && x && b, "null handle");
+    MTLG_CHECK_ARG(solver == MTLG_CG || solver == MTLG_BICGSTAB || solver == MTLG_GMRES, "solver");
+    if (A->n_rows != A->n_cols) {
+        set_error("solve with a %lldx%lld matrix", (long long)A->n_rows, (long long)A->n_cols);
+        return MTLG_ERR_NOT_SQUARE;
+    }
+    if (x->n != A->n_rows || b->n != A->n_rows || (P && P->n != A->n_rows)) {
+        set_error("solve sizes differ");
+        return MTLG_ERR_INCOMPATIBLE_SIZE;
+    }
+    return MTLG_OK;
+}
+
+int mtlg_gmres_impl(mtlg_ctx* c, mtlg_csr* A, mtlg_pc* L, mtlg_pc* R, mtlg_vec* x, const mtlg_vec* b,
+                    const mtlg_iter_params* p, mtlg_iter_result* r);
+
+static int timed_result(mtlg_ctx* c, SolveSet& ss, cudaEvent_t e0, cudaEvent_t e1, mtlg_iter_result* res)
+{
+    MTLG_CUDA(cudaEventRecord(e1, c->stream));
+    MTLG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    MTLG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    SysState h;
+    MTLG_CUDA(cudaMemcpy(&h, ss.st.p, sizeof h, cudaMemcpyDeviceToHost));
+    int flags[1] = {0};
+    MTLG_CUDA(cudaMemcpy(flags, ss.misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (res) {
+        fill_result(h, ss.mixed != 0, res);
+        res->seconds = ms * 1e-3;
+    }
+    if (flags[0]) {
+        int z = 0;
+        MTLG_CUDA(cudaMemcpy(ss.misc.p + 1, &z, sizeof z, cudaMemcpyHostToDevice));
+        MTLG_CUDA(cudaMemset(ss.tickets.p, 0, 8 * sizeof(int)));
+        set_error("a device-side wait expired during the solve");
+        return MTLG_ERR_TIMEOUT;
+    }
+    const int st = ss.mixed ? h.ostatus : h.status;
+    if (st == MTLG_ST_BREAKDOWN && ss.solver == MTLG_BICGSTAB) {
+        set_error("BiCGSTAB breakdown (zero rho, gamma or omega)");
+        return MTLG_ERR_BREAKDOWN;
+    }
+    return MTLG_OK;
+}
+
+int mtlg_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* L, mtlg_pc* R, mtlg_vec* x, const mtlg_vec* b,
+               const mtlg_iter_params* p, mtlg_iter_result* res)
+{
+    MTLG_CHECK_ARG(c && p, "ctx/params");
+    MTLG_TRY(check_solve_args(solver, A, x, b, L));
+    MTLG_CHECK_ARG(x->dtype == b->dtype, "x and b dtypes differ");
+    if (solver == MTLG_GMRES) return mtlg_gmres_impl(c, A, L, R, x, b, p, res);
+    const int f32 = x->dtype == MTLG_F32;
+    if (L && L->kind == MTLG_PC_IDENTITY) L = nullptr;   // is_identity(P) short-cut (cg.hpp:80-81)
+    SetKey key{A, L, solver, f32, 0};
+    auto& slot = extra(c).sets[key];
+    if (!slot) {
+        std::unique_ptr<SolveSet> ss(new SolveSet);
+        ss->solver = solver;
+        ss->f32 = f32;
+        SysInput si;
+        si.A = A;
+        si.P = L;
+        ss->in.push_back(si);
+        MTLG_TRY(build_set(c, *ss));
+        slot = std::move(ss);
+    }
+    SolveSet& ss = *slot;
+    SysInput& si = ss.in[0];
+    si.x = x->p;
+    si.b = b->p;
+    si.max_iter = p->max_iter;
+    si.rtol = p->rtol;
+    si.atol = p->atol;
+    si.norm_r0 = p->norm_r0;
+    ss.h_desc[0].x = x->p;
+    ss.h_desc[0].b = b->p;
+    MTLG_CUDA(cudaMemcpyAsync(ss.desc.p, ss.h_desc.data(), sizeof(SysDesc), cudaMemcpyHostToDevice, c->stream));
+    cudaEvent_t e0, e1;
+    MTLG_CUDA(cudaEventCreate(&e0));
+    MTLG_CUDA(cudaEventCreate(&e1));
+    MTLG_CUDA(cudaEventRecord(e0, c->stream));
+    int s = f32 ? run_plain<float>(ss) : run_plain<double>(ss);
+    if (s == MTLG_OK) s = timed_result(c, ss, e0, e1, res);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return s;
+}
+
+int mtlg_refine_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* P, mtlg_vec* x, const mtlg_vec* b,
+                      const mtlg_refine_params* rp, mtlg_iter_result* res)
+{
+    MTLG_CHECK_ARG(c && rp, "ctx/params");
+    MTLG_TRY(check_solve_args(solver, A, x, b, P));
+    MTLG_CHECK_ARG(x->dtype == MTLG_F64 && b->dtype == MTLG_F64, "refinement takes FP64 x and b");
+    MTLG_CHECK_ARG(solver != MTLG_GMRES, "refinement runs CG or BiCGSTAB inside");
+    if (P && P->kind == MTLG_PC_IDENTITY) P = nullptr;
+    if (P && P->storage != MTLG_F32) {
+        set_error("the inner FP32 solve needs a preconditioner stored in FP32");
+        return MTLG_ERR_INVALID_ARG;
+    }
+    SetKey key{A, P, solver, 1, 1};
+    auto& slot = extra(c).sets[key];
+    if (!slot) {
+        std::unique_ptr<SolveSet> ss(new SolveSet);
+        ss->solver = solver;
+        ss->f32 = 1;
+        ss->mixed = 1;
+        SysInput si;
+        si.A = A;
+        si.P = P;
+        si.x = x->p;
+        si.b = b->p;
+        ss->in.push_back(si);
+        MTLG_TRY(build_set(c, *ss));
+        slot = std::move(ss);
+    }
+    SolveSet& ss = *slot;
+    ss.in[0].x = x->p;
+    ss.in[0].b = b->p;
+    ss.h_desc[0].x64 = static_cast<double*>(x->p);
+    ss.h_desc[0].b64 = static_cast<const double*>(b->p);
+    ss.h_desc64[0].x = x->p;
+    ss.h_desc64[0].b = b->p;
+    MTLG_CUDA(cudaMemcpyAsync(ss.desc.p, ss.h_desc.data(), sizeof(SysDesc), cudaMemcpyHostToDevice, c->stream));
+    MTLG_CUDA(cudaMemcpyAsync(ss.desc64.p, ss.h_desc64.data(), sizeof(SysDesc), cudaMemcpyHostToDevice, c->stream));
+    cudaEvent_t e0, e1;
+    MTLG_CUDA(cudaEventCreate(&e0));
+    MTLG_CUDA(cudaEventCreate(&e1));
+    MTLG_CUDA(cudaEventRecord(e0, c->stream));
+    int s = run_refine(ss, *rp);
+    if (s == MTLG_OK) s = timed_result(c, ss, e0, e1, res);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return s;
+}
+
+}  // extern "C"
+
+#include "host_gmres.cuh"
+#include "host_batch.cuh"

@@ -1,0 +1,178 @@
+"""Python mirror of MTL4's iterative solvers (ITL) on the GPU.
+
+Same names and argument meaning as boost/numeric/itl:
+  basic_iteration(r0_or_norm, max_iter, rtol, atol)  itl/iteration/basic_iteration.hpp:24-164
+  cg(A, x, b, P, iter)                               itl/krylov/cg.hpp:76
+  bicgstab(A, x, b, P, iter)                         itl/krylov/bicgstab.hpp:29
+  gmres(A, x, b, L, R, iter, restart)                itl/krylov/gmres.hpp:124
+  pc.identity / diagonal / ilu_0 / ic_0 (A, value)   itl/pc/*.hpp
+  solve(P, x), adjoint_solve(P, x)
+The solvers return iter.error_code() as the reference does; BiCGSTAB
+breakdown raises unexpected_orthogonality.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, unexpected_orthogonality  # noqa: F401  (re-exported)
+from .mtl import compressed2D, dense_vector, two_norm
+
+
+class basic_iteration:
+    """Termination control.  Constructed from a vector (norm_r0 = ||r0||, e.g.
+    b) or from a number (basic_iteration.hpp:31-39)."""
+
+    def __init__(self, r0_or_norm, max_iter: int, rtol: float, atol: float = 0.0):
+        if isinstance(r0_or_norm, dense_vector):
+            self._norm_r0 = two_norm(r0_or_norm)
+        elif isinstance(r0_or_norm, np.ndarray):
+            self._norm_r0 = float(np.linalg.norm(r0_or_norm))
+        else:
+            self._norm_r0 = abs(float(r0_or_norm))
+        self.max_iter = int(max_iter)
+        self.rtol = float(rtol)
+        self._atol = float(atol)
+        self.i = 0
+        self.error = 0
+        self._resid = 0.0
+        self.status = _lib.ST_RUNNING
+        self.seconds = 0.0
+        self.outer = 0
+
+    # reference accessors
+    def iterations(self) -> int: return self.i
+    def max_iterations(self) -> int: return self.max_iter
+    def error_code(self) -> int: return self.error
+    def resid(self) -> float: return self._resid
+    def relresid(self) -> float: return self._resid / self._norm_r0 if self._norm_r0 else self._resid
+    def norm_r0(self) -> float: return self._norm_r0
+    def tol(self) -> float: return self.rtol
+    def atol(self) -> float: return self._atol
+    def is_converged(self) -> bool: return self.status == _lib.ST_CONVERGED and self.error == 0
+    def __int__(self) -> int: return self.error
+
+    def _params(self, restart: int = 0) -> _lib.IterParams:
+        return _lib.IterParams(self.max_iter, int(restart), self.rtol, self._atol, self._norm_r0)
+
+    def _take(self, r: _lib.IterResult):
+        self.i = r.iterations
+        self.error = r.error_code
+        self._resid = r.resid
+        self.status = r.status
+        self.seconds = r.seconds
+        self.outer = r.outer_iterations
+        if r.norm_r0 > 0 or self._norm_r0 == 0:
+            self._norm_r0 = r.norm_r0
+
+
+class pc:
+    """Preconditioners (itl::pc)."""
+
+    class _base:
+        kind = _lib.PC_IDENTITY
+
+        def __init__(self, A: compressed2D, value=np.float64):
+            self.A = A
+            self.ctx = A.ctx
+            self.value = np.dtype(value)
+            h = C.c_void_p()
+            st = _lib.F64 if self.value == np.float64 else _lib.F32
+            check(self.ctx._L.mtlg_pc_create(self.ctx.h, A.h, self.kind, st, C.byref(h)), type(self).__name__)
+            self.h = h
+
+        def levels(self):
+            a, b = C.c_int(), C.c_int()
+            check(self.ctx._L.mtlg_pc_levels(self.h, C.byref(a), C.byref(b)), "levels")
+            return a.value, b.value
+
+        def factor(self, which: str):
+            """Stored factor ('L' or 'U') as (row_ptr, col, val) host arrays."""
+            w = 0 if which == "L" else 1
+            nnz = C.c_int64()
+            check(self.ctx._L.mtlg_pc_factor(self.h, w, C.byref(nnz), None, None, None), "factor")
+            n = self.A.num_rows()
+            rp = np.zeros(n + 1, np.int64)
+            ci = np.zeros(max(nnz.value, 1), np.int32)
+            v = np.zeros(max(nnz.value, 1), np.float64)
+            check(self.ctx._L.mtlg_pc_factor(self.h, w, C.byref(nnz), C.c_void_p(rp.ctypes.data),
+                                             C.c_void_p(ci.ctypes.data), C.c_void_p(v.ctypes.data)), "factor")
+            return rp, ci[:nnz.value], v[:nnz.value]
+
+        def get_L(self):
+            return self.factor("L")
+
+        def get_U(self):
+            return self.factor("U")
+
+        def __del__(self):
+            try:
+                if getattr(self, "h", None) and self.ctx.h:
+                    self.ctx._L.mtlg_pc_destroy(self.h)
+            except Exception:
+                pass
+
+    class identity(_base):
+        kind = _lib.PC_IDENTITY
+
+    class diagonal(_base):
+        kind = _lib.PC_DIAGONAL
+
+    class ilu_0(_base):
+        kind = _lib.PC_ILU0
+
+    class ic_0(_base):
+        kind = _lib.PC_IC0
+
+
+def solve(P: pc._base, x: dense_vector, y: dense_vector | None = None) -> dense_vector:
+    """y = solve(P, x)."""
+    y = y or dense_vector(x.n, x.dtype, x.ctx)
+    check(P.ctx._L.mtlg_pc_apply(P.ctx.h, P.h, x.h, y.h), "solve")
+    return y
+
+
+def adjoint_solve(P: pc._base, x: dense_vector, y: dense_vector | None = None) -> dense_vector:
+    y = y or dense_vector(x.n, x.dtype, x.ctx)
+    check(P.ctx._L.mtlg_pc_adjoint_apply(P.ctx.h, P.h, x.h, y.h), "adjoint_solve")
+    return y
+
+
+def _solve(kind, A, x, b, L, R, it: basic_iteration, restart=0) -> int:
+    res = _lib.IterResult()
+    params = it._params(restart)
+    st = A.ctx._L.mtlg_solve(A.ctx.h, kind, A.h, L.h if L is not None else None, R.h if R is not None else None,
+                             x.h, b.h, C.byref(params), C.byref(res))
+    it._take(res)
+    check(st, ["cg", "bicgstab", "gmres"][kind])
+    return it.error_code()
+
+
+def cg(A, x, b, P, it: basic_iteration) -> int:
+    return _solve(_lib.CG, A, x, b, P, None, it)
+
+
+def bicgstab(A, x, b, P, it: basic_iteration) -> int:
+    return _solve(_lib.BICGSTAB, A, x, b, P, None, it)
+
+
+def gmres(A, x, b, L, R, it: basic_iteration, restart: int) -> int:
+    return _solve(_lib.GMRES, A, x, b, L, R, it, restart)
+
+
+def refine(solver: str, A: compressed2D, x: dense_vector, b: dense_vector, P, rtol: float = 1e-8,
+           inner_rtol: float = 1e-4, max_outer: int = 20, max_inner: int = 2000) -> basic_iteration:
+    """FP64 iterative refinement around an FP32 inner solve (no reference
+    counterpart).  x, b: FP64; P: preconditioner stored in FP32."""
+    kind = {"cg": _lib.CG, "bicgstab": _lib.BICGSTAB}[solver]
+    rp = _lib.RefineParams(int(max_outer), int(max_inner), 0, 0, float(rtol), float(inner_rtol))
+    res = _lib.IterResult()
+    st = A.ctx._L.mtlg_refine_solve(A.ctx.h, kind, A.h, P.h if P is not None else None, x.h, b.h, C.byref(rp),
+                                    C.byref(res))
+    it = basic_iteration(res.norm_r0 if res.norm_r0 else 1.0, max_inner, rtol)
+    it._take(res)
+    check(st, "refine")
+    return it

@@ -1,0 +1,227 @@
+"""Python mirror of MTL4's storage types and vector operations on the GPU.
+
+``compressed2D`` and ``dense_vector`` keep their data in device memory owned by
+the C ABI (include/mtl4_b200/mtlg.h).  Names and argument meanings follow
+boost/numeric/mtl (compressed2D.hpp:259,355; dense_vector.hpp:52,122;
+operation/dot.hpp:228; operation/two_norm.hpp:54;
+vector/crtp_base_vector.hpp:94-101 for w = A*v, w += A*v, w -= A*v).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+_DT = {np.dtype(np.float64): _lib.F64, np.dtype(np.float32): _lib.F32}
+
+
+class context:
+    """One device, one stream.  Not thread-safe (as the reference's ILU/IC
+    apply is not re-entrant, itl/pc/ilu.hpp:76)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self._L = _lib.lib()
+        h = C.c_void_p()
+        check(self._L.mtlg_ctx_create(device, hbm_budget, C.byref(h)), "ctx_create")
+        self.h = h
+        self.device = device
+
+    def synchronize(self):
+        check(self._L.mtlg_ctx_synchronize(self.h), "synchronize")
+
+    def kernel_launches(self) -> int:
+        return int(self._L.mtlg_ctx_kernel_launches(self.h))
+
+    def bytes_in_use(self) -> int:
+        return int(self._L.mtlg_ctx_bytes_in_use(self.h))
+
+    def set_stream(self, cuda_stream_ptr: int | None):
+        check(self._L.mtlg_ctx_set_stream(self.h, C.c_void_p(cuda_stream_ptr or 0)), "set_stream")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.mtlg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_DEFAULT: dict[int, context] = {}
+
+
+def default_context(device: int = 0) -> context:
+    if device not in _DEFAULT:
+        _DEFAULT[device] = context(device)
+    return _DEFAULT[device]
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+class compressed2D:
+    """CSR matrix on the device (row_ptr int64 on the host side, int32 on the
+    device; sorted, distinct, in-range columns in every row)."""
+
+    def __init__(self, row_ptr, col, val, shape=None, ctx: context | None = None):
+        self.ctx = ctx or default_context()
+        rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        ci = np.ascontiguousarray(col, dtype=np.int32)
+        v = np.asarray(val)
+        if v.dtype not in _DT:
+            v = v.astype(np.float64)
+        v = np.ascontiguousarray(v)
+        n_rows = rp.size - 1
+        n_cols = shape[1] if shape is not None else n_rows
+        h = C.c_void_p()
+        check(self.ctx._L.mtlg_csr_create(self.ctx.h, n_rows, n_cols, int(rp[-1]), _ptr(rp), _ptr(ci), _ptr(v),
+                                          _DT[v.dtype], C.byref(h)), "compressed2D")
+        self.h = h
+        self.shape = (n_rows, n_cols)
+        self.nnz = int(rp[-1])
+
+    @classmethod
+    def from_problem(cls, A, ctx: context | None = None) -> "compressed2D":
+        return cls(A.row_ptr, A.col, A.val, (A.n_rows, A.n_cols), ctx)
+
+    def num_rows(self) -> int:
+        return self.shape[0]
+
+    def num_cols(self) -> int:
+        return self.shape[1]
+
+    def plan_info(self):
+        k = (C.c_int64 * 3)()
+        mr = C.c_int()
+        check(self.ctx._L.mtlg_csr_plan_info(self.h, k, C.byref(mr)), "plan_info")
+        return {"stream_tiles": k[0], "long_tiles": k[1], "max_row": mr.value}
+
+    def update_values(self, val):
+        v = np.ascontiguousarray(val)
+        check(self.ctx._L.mtlg_csr_update_values(self.h, _ptr(v), _DT[v.dtype]), "update_values")
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.ctx.h:
+                self.ctx._L.mtlg_csr_destroy(self.h)
+        except Exception:
+            pass
+
+    def __mul__(self, v: "dense_vector") -> "_MatVec":
+        return _MatVec(self, v)
+
+
+class _MatVec:
+    """Lazy A*v, consumed by dense_vector.assign / += / -= as the reference's
+    mat_cvec_times_expr is."""
+
+    def __init__(self, A, v):
+        self.A, self.v = A, v
+
+
+class dense_vector:
+    """Device vector of float64 or float32."""
+
+    def __init__(self, n_or_array, dtype=np.float64, ctx: context | None = None, _wrap_ptr: int | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        if isinstance(n_or_array, (int, np.integer)):
+            n = int(n_or_array)
+            self.dtype = np.dtype(dtype)
+            if _wrap_ptr is not None:
+                check(self.ctx._L.mtlg_vec_wrap(self.ctx.h, n, _DT[self.dtype], C.c_void_p(_wrap_ptr), C.byref(h)),
+                      "dense_vector")
+            else:
+                check(self.ctx._L.mtlg_vec_create(self.ctx.h, n, _DT[self.dtype], C.byref(h)), "dense_vector")
+            self.h = h
+            self.n = n
+        else:
+            a = np.asarray(n_or_array)
+            self.dtype = np.dtype(dtype) if dtype is not None else a.dtype
+            a = np.ascontiguousarray(a, dtype=self.dtype)
+            self.n = a.size
+            check(self.ctx._L.mtlg_vec_create(self.ctx.h, self.n, _DT[self.dtype], C.byref(h)), "dense_vector")
+            self.h = h
+            self.upload(a)
+
+    def __len__(self):
+        return self.n
+
+    def size(self) -> int:
+        return self.n
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        check(self.ctx._L.mtlg_vec_upload(self.h, _ptr(a), a.size), "upload")
+
+    def numpy(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=self.dtype)
+        check(self.ctx._L.mtlg_vec_download(self.h, _ptr(out), self.n), "download")
+        return out
+
+    def fill(self, value: float):
+        check(self.ctx._L.mtlg_vec_fill(self.h, float(value)), "fill")
+
+    def device_ptr(self) -> int:
+        return int(self.ctx._L.mtlg_vec_device_ptr(self.h) or 0)
+
+    def assign(self, e: _MatVec):
+        mult(e.A, e.v, self, "=")
+        return self
+
+    def __iadd__(self, e):
+        if isinstance(e, _MatVec):
+            mult(e.A, e.v, self, "+=")
+            return self
+        return NotImplemented
+
+    def __isub__(self, e):
+        if isinstance(e, _MatVec):
+            mult(e.A, e.v, self, "-=")
+            return self
+        return NotImplemented
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.ctx.h:
+                self.ctx._L.mtlg_vec_destroy(self.h)
+        except Exception:
+            pass
+
+
+_ASSIGN = {"=": _lib.ASSIGN, "+=": _lib.PLUS, "-=": _lib.MINUS}
+
+
+def mult(A: compressed2D, x: dense_vector, y: dense_vector, assign: str = "="):
+    """y = A x, y += A x or y -= A x."""
+    check(A.ctx._L.mtlg_spmv(A.ctx.h, A.h, x.h, y.h, _ASSIGN[assign]), "mult")
+
+
+def mult_dot(A: compressed2D, p: dense_vector, q: dense_vector) -> float:
+    """(q = A p) || (alpha = dot(p, q)) in one pass (cg.hpp:103)."""
+    out = C.c_double()
+    check(A.ctx._L.mtlg_spmv_dot(A.ctx.h, A.h, p.h, q.h, C.byref(out)), "mult_dot")
+    return out.value
+
+
+def dot(x: dense_vector, y: dense_vector) -> float:
+    out = C.c_double()
+    check(x.ctx._L.mtlg_dot(x.ctx.h, x.h, y.h, C.byref(out)), "dot")
+    return out.value
+
+
+def two_norm(x: dense_vector) -> float:
+    out = C.c_double()
+    check(x.ctx._L.mtlg_two_norm(x.ctx.h, x.h, C.byref(out)), "two_norm")
+    return out.value
+
+
+def axpy(a: float, x: dense_vector, y: dense_vector):
+    check(x.ctx._L.mtlg_axpy(x.ctx.h, float(a), x.h, y.h), "axpy")

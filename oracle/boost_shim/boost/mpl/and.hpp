@@ -1,0 +1,2 @@
+// std-based stand-in for <boost/mpl/and.hpp>; see _shim_core.hpp.
+#include <boost/_shim_core.hpp>

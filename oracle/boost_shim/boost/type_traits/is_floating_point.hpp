@@ -1,0 +1,2 @@
+// std-based stand-in for <boost/type_traits/is_floating_point.hpp>; see _shim_core.hpp.
+#include <boost/_shim_core.hpp>

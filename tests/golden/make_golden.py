@@ -1,0 +1,73 @@
+"""Regenerates tests/golden/golden.npz from the reference-built oracle
+(oracle/_ref/libmtlref.so: MTL4's own headers compiled unchanged).
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+The fixtures pin the oracle restatement and the GPU library on machines
+where the MTL4 tree is not available.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from mtl4_b200 import problems as P  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def main():
+    out = {}
+    # 2D Laplacian (laplacian_setup) 32x32: CSR, SpMV, CG runs
+    A = P.laplacian_2d(32)
+    x_true, b = P.rhs_from_solution(A, 0)
+    R = O.RefMatrix(A)
+    rp, ci, v = O.ref_laplacian(32, 32)
+    out["lap32_rp"], out["lap32_ci"], out["lap32_val"] = rp, ci, v
+    xs = np.random.default_rng(11).standard_normal(A.n_rows)
+    out["lap32_x"] = xs
+    out["lap32_spmv"] = R.spmv(xs)
+    out["lap32_spmv_f32"] = R.spmv(xs.astype(np.float32))
+    out["lap32_b"] = b
+    for solver, pc in [("cg", "diagonal"), ("cg", "identity"), ("cg", "ic_0"), ("bicgstab", "ilu_0"),
+                       ("bicgstab", "diagonal")]:
+        r = R.solve(b, solver, pc, max_iter=2000, rtol=1e-8)
+        out[f"lap32_{solver}_{pc}_iters"] = np.array(r["iterations"])
+        out[f"lap32_{solver}_{pc}_x"] = r["x"]
+        out[f"lap32_{solver}_{pc}_relres"] = np.array(r["relresid"])
+    # 3D convection-diffusion 8^3: factors and applies in all precisions
+    C3 = P.convdiff_3d(8)
+    out["cd8_rp"], out["cd8_ci"], out["cd8_val"] = C3.row_ptr, C3.col, C3.val
+    R3 = O.RefMatrix(C3)
+    xc = np.random.default_rng(12).standard_normal(C3.n_rows)
+    out["cd8_x"] = xc
+    for kind in ["ilu_0", "ic_0"]:
+        (Lr, Lc, Lv), (Ur, Uc, Uv) = R3.factors(kind)
+        out[f"cd8_{kind}_L_rp"], out[f"cd8_{kind}_L_ci"], out[f"cd8_{kind}_L_val"] = Lr, Lc, Lv
+        out[f"cd8_{kind}_U_rp"], out[f"cd8_{kind}_U_ci"], out[f"cd8_{kind}_U_val"] = Ur, Uc, Uv
+    for kind in ["diagonal", "ilu_0", "ic_0"]:
+        out[f"cd8_{kind}_apply_f64"] = R3.pc_apply(kind, xc)
+        out[f"cd8_{kind}_apply_f64s32"] = R3.pc_apply(kind, xc, storage_f32=True)
+        out[f"cd8_{kind}_apply_f32"] = R3.pc_apply(kind, xc.astype(np.float32))
+    _, b3 = P.rhs_from_solution(C3, 1)
+    out["cd8_b"] = b3
+    r = R3.solve(b3, "bicgstab", "ilu_0", max_iter=500, rtol=1e-8)
+    out["cd8_bicgstab_ilu_0_iters"] = np.array(r["iterations"])
+    # irregular power-law CSR (small)
+    Q = P.powerlaw_csr(5000, seed=2)
+    out["pl_rp"], out["pl_ci"], out["pl_val"] = Q.row_ptr, Q.col, Q.val
+    RQ = O.RefMatrix(Q)
+    xq = np.random.default_rng(13).standard_normal(Q.n_rows)
+    out["pl_x"] = xq
+    out["pl_spmv"] = RQ.spmv(xq)
+    out["pl_spmv_f32"] = RQ.spmv(xq.astype(np.float32))
+    np.savez_compressed(Path(__file__).with_name("golden.npz"), **out)
+    print("wrote", len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,42 @@
+"""The C-ABI library loads and exports every symbol include/mtl4_b200/mtlg.h
+declares (no compute calls: runs without a GPU)."""
+import ctypes
+import re
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "mtl4_b200" / "mtlg.h").read_text()
+    return sorted(set(re.findall(r"\b(mtlg_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "mtlg_solve" in syms and "mtlg_spmv" in syms and len(syms) > 40
+
+
+def test_library_exports_every_declared_symbol():
+    from mtl4_b200 import _lib
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_binding_signatures_cover_header():
+    from mtl4_b200 import _lib
+    assert set(declared_symbols()) <= set(_lib.SIGNATURES)
+
+
+def test_status_strings_need_no_gpu():
+    from mtl4_b200 import _lib
+    L = _lib.load()
+    assert L.mtlg_status_string(0) == b"ok"
+    assert b"orthogonality" in L.mtlg_status_string(_lib.ERR_BREAKDOWN)
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    import pytest
+    from mtl4_b200 import _lib
+    with pytest.raises(ImportError):
+        _lib.load(tmp_path / "nope.so")
