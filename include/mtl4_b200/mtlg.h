@@ -123,6 +123,11 @@ void* mtlg_ctx_stream(mtlg_ctx* ctx);
 /* Kernels this library enqueued on the context since creation (graph replays
  * count every kernel node they run). */
 int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
+/* Launch-shape tuning (used by the autotuner): "sweep_blocks_per_sm"
+ * (0 = as many as fit), "sweep_sleep_ns" (poll back-off of the triangular
+ * sweeps).  Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
+int mtlg_ctx_set_tuning(mtlg_ctx* ctx, const char* key, int64_t value);
+int mtlg_ctx_get_tuning(mtlg_ctx* ctx, const char* key, int64_t* value);
 /* Bytes of device memory the context's objects hold. */
 size_t mtlg_ctx_bytes_in_use(mtlg_ctx* ctx);
 const char* mtlg_status_string(int status);
@@ -137,7 +142,7 @@ int mtlg_csr_destroy(mtlg_csr* A);
 int mtlg_csr_info(const mtlg_csr* A, int64_t* n_rows, int64_t* n_cols, int64_t* nnz);
 /* Replace the values (same pattern), e.g. a new operator with the old graph. */
 int mtlg_csr_update_values(mtlg_csr* A, const void* val, mtlg_dtype val_dtype);
-/* SpMV tiling statistics: tiles by kind (0 stream, 1 vector, 2 long row). */
+/* SpMV tiling statistics: tiles by kind (0 stream, 1 long row, 2 unused). */
 int mtlg_csr_plan_info(const mtlg_csr* A, int64_t* tiles_by_kind3, int* max_row_len);
 
 /* ---- dense vectors (dense_vector) ----------------------------------------- */

@@ -79,6 +79,8 @@ SIGNATURES = {
     "mtlg_ctx_stream": (VP, [VP]),
     "mtlg_ctx_kernel_launches": (I64, [VP]),
     "mtlg_ctx_bytes_in_use": (C.c_size_t, [VP]),
+    "mtlg_ctx_set_tuning": (C.c_int, [VP, C.c_char_p, I64]),
+    "mtlg_ctx_get_tuning": (C.c_int, [VP, C.c_char_p, PI64]),
     "mtlg_status_string": (C.c_char_p, [C.c_int]),
     "mtlg_last_error_message": (C.c_char_p, []),
     "mtlg_csr_create": (C.c_int, [VP, I64, I64, I64, VP, VP, VP, C.c_int, C.POINTER(VP)]),

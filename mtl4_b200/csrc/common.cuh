@@ -69,6 +69,8 @@ struct Tile {
     int row_begin;  // first row (system-local)
     int row_end;    // one past the last row
     int kind;       // TileKind
+    int nnz_begin;  // row_ptr[row_begin]
+    int nnz_end;    // row_ptr[row_end]
 };
 
 // One dependency-ordered sweep task: kSweepRows consecutive rows of a

@@ -15,7 +15,15 @@ struct mtlg_ctx {
     int64_t launches = 0;
     int sm_count = 148;
     int sweep_grid = 148;       // persistent grid of the sweep / factor kernels
+    int sweep_max_bpsm = 1;     // resident sweep CTAs per SM the device allows
+    int sweep_bpsm = 0;         // tuning: sweep CTAs per SM (0: as many as fit)
+    int sweep_sleep_ns = 32;    // tuning: back-off between polls of a dependency
     int* d_scratch_err = nullptr;
+    int sweep_blocks() const
+    {
+        const int b = sweep_bpsm > 0 ? std::min(sweep_bpsm, sweep_max_bpsm) : sweep_max_bpsm;
+        return sm_count * b;
+    }
 };
 
 namespace mtlg {
@@ -108,7 +116,7 @@ inline void plan_tiles(const int64_t* rp, int n, int sys, std::vector<Tile>& out
     while (r < n) {
         int64_t len = rp[r + 1] - rp[r];
         if (len > kTileNnz) {
-            out.push_back({sys, r, r + 1, TILE_LONG});
+            out.push_back({sys, r, r + 1, TILE_LONG, int(rp[r]), int(rp[r + 1])});
             ++r;
             continue;
         }
@@ -120,7 +128,7 @@ inline void plan_tiles(const int64_t* rp, int n, int sys, std::vector<Tile>& out
             nnz += len;
             ++r;
         }
-        out.push_back({sys, rb, r, TILE_STREAM});
+        out.push_back({sys, rb, r, TILE_STREAM, int(rp[rb]), int(rp[r])});
     }
 }
 
@@ -238,19 +246,57 @@ inline VecOp vec_op_default(int kind)
 }
 
 // Kernel dispatchers ---------------------------------------------------------
+// SpMV launch shape: persistent grid of (resident CTAs per SM) x SMs, two
+// staging buffers of dynamic shared memory per CTA.
+template <typename T, int XF, int ASG>
+struct SpmvShape {
+    static int occ;
+    static int init()
+    {
+        const int smem = 2 * StageLayout<T>::BYTES;
+        MTLG_CUDA(cudaFuncSetAttribute(k_spmv<T, XF, ASG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int o = 1;
+        MTLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_spmv<T, XF, ASG>, kBlock, smem));
+        occ = std::max(1, o);
+        return MTLG_OK;
+    }
+};
+template <typename T, int XF, int ASG> int SpmvShape<T, XF, ASG>::occ = 0;
+
+#define MTLG_SPMV_VARIANTS(M)      \
+    M(XF_PLAIN, ASG_SET)          \
+    M(XF_PLAIN, ASG_ADD)          \
+    M(XF_PLAIN, ASG_SUB)          \
+    M(XF_PLAIN, ASG_WMINUS)       \
+    M(XF_CG_P, ASG_SET)           \
+    M(XF_CG_P_JAC, ASG_SET)       \
+    M(XF_JAC, ASG_SET)
+
+// Called once per context (kernel attributes may not change inside a stream
+// capture).
+inline int init_kernel_shapes()
+{
+#define MTLG_SPMV_INIT(XF, ASG)                              \
+    MTLG_TRY((SpmvShape<double, XF, ASG>::init()));          \
+    MTLG_TRY((SpmvShape<float, XF, ASG>::init()));
+    MTLG_SPMV_VARIANTS(MTLG_SPMV_INIT)
+#undef MTLG_SPMV_INIT
+    return MTLG_OK;
+}
+
 template <typename T>
 inline int launch_spmv(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const SpmvOp& op, int xf, int asg)
 {
     if (sv.n_tiles == 0) return MTLG_OK;
-    dim3 g(sv.n_tiles), b(kBlock);
-#define MTLG_SPMV_CASE(XF, ASG) \
-    if (xf == XF && asg == ASG) { k_spmv<T, XF, ASG><<<g, b, 0, st>>>(sv, op); c->launches++; return MTLG_OK; }
-    MTLG_SPMV_CASE(XF_PLAIN, ASG_SET)
-    MTLG_SPMV_CASE(XF_PLAIN, ASG_ADD)
-    MTLG_SPMV_CASE(XF_PLAIN, ASG_SUB)
-    MTLG_SPMV_CASE(XF_PLAIN, ASG_WMINUS)
-    MTLG_SPMV_CASE(XF_CG_P, ASG_SET)
-    MTLG_SPMV_CASE(XF_CG_P_JAC, ASG_SET)
+    const int smem = 2 * StageLayout<T>::BYTES;
+#define MTLG_SPMV_CASE(XF, ASG)                                                                    \
+    if (xf == XF && asg == ASG) {                                                                 \
+        const int grid = std::min(sv.n_tiles, c->sm_count * SpmvShape<T, XF, ASG>::occ);          \
+        k_spmv<T, XF, ASG><<<grid, kBlock, smem, st>>>(sv, op);                                    \
+        c->launches++;                                                                            \
+        return MTLG_OK;                                                                           \
+    }
+    MTLG_SPMV_VARIANTS(MTLG_SPMV_CASE)
 #undef MTLG_SPMV_CASE
     set_error("unsupported SpMV variant %d/%d", xf, asg);
     return MTLG_ERR_NOT_SUPPORTED;

@@ -222,9 +222,11 @@ inline int launch_sweep(SolveSet& ss, cudaStream_t st, const SetView& sv, int wh
     op.reset = reset;
     op.skip = skip;
     op.fuse = SWF_NONE;
+    op.sleep_ns = ss.ctx->sweep_sleep_ns;
     if (op.ntasks == 0) return MTLG_OK;
-    if (ss.pc_f32) k_sweep<T, float><<<ss.ctx->sweep_grid, kBlock, 0, st>>>(sv, op);
-    else k_sweep<T, double><<<ss.ctx->sweep_grid, kBlock, 0, st>>>(sv, op);
+    const int grid = ss.ctx->sweep_blocks();
+    if (ss.pc_f32) k_sweep<T, float><<<grid, kBlock, 0, st>>>(sv, op);
+    else k_sweep<T, double><<<grid, kBlock, 0, st>>>(sv, op);
     ss.ctx->launches++;
     MTLG_CUDA(cudaGetLastError());
     return MTLG_OK;

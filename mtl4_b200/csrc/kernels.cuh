@@ -245,30 +245,12 @@ __device__ __forceinline__ T assign_out(T old_or_w, T acc)
     return old_or_w - acc;  // ASG_SUB and ASG_WMINUS
 }
 
-template <typename T, int ASG, int XF>
-struct RowEpilogue {
-    T* y;
-    T* y2;
-    const T* w;
-    T* pnew;
-    const T* dvec[2 * kMaxDots + kMaxDots];
-    int ndot;
-    const SpmvOp* op;
-    __device__ __forceinline__ void operator()(int i, T acc, T xp, const T* dinv, double (&dot)[kMaxDots]) const
-    {
-        T base = (ASG == ASG_SET) ? T(0) : ((ASG == ASG_WMINUS) ? w[i] : y[i]);
-        T out = assign_out<T, ASG>(base, acc);
-        y[i] = out;
-        if (y2) y2[i] = out;
-        if (XF != XF_PLAIN) pnew[i] = xp;
-        for (int j = 0; j < ndot; ++j) {
-            T a = pick(op->da[j], i, out, xp, dinv, dvec[3 * j + 0]);
-            T b = pick(op->db[j], i, out, xp, dinv, dvec[3 * j + 1]);
-            T c = pick(op->dc[j], i, out, xp, dinv, dvec[3 * j + 2]);
-            dot[j] += double(a * b * c);
-        }
-    }
-    __device__ __forceinline__ static T pick(int code, int i, T y, T xp, const T* dinv, const T* v)
+// Per-row epilogue operand (a dot factor): a vector, or y / x' / D of the row.
+template <typename T>
+struct Opnd1 {
+    int code;
+    const T* v;
+    __device__ __forceinline__ T get(int i, T y, T xp, const T* dinv) const
     {
         switch (code) {
         case OPND_ONE: return T(1);
@@ -280,119 +262,206 @@ struct RowEpilogue {
     }
 };
 
-// One CTA per tile.  Stream tiles stage the tile's values and column
-// indices in shared memory with coalesced loads, then every thread sums one
-// row; rows longer than kShortRow are summed by a warp from shared memory.
-// Long tiles hold one row with more than kTileNnz entries, summed by the CTA
-// straight from global memory.
+template <typename T, int ASG, int XF>
+struct RowEpilogue {
+    T* y;
+    T* y2;
+    const T* w;
+    T* pnew;
+    int ndot;
+    Opnd1<T> a0, b0, c0, a1, b1, c1;
+    __device__ __forceinline__ void operator()(int i, T acc, T xp, const T* dinv, double& d0, double& d1) const
+    {
+        const T base = (ASG == ASG_SET) ? T(0) : ((ASG == ASG_WMINUS) ? w[i] : y[i]);
+        const T out = assign_out<T, ASG>(base, acc);
+        y[i] = out;
+        if (y2) y2[i] = out;
+        if (XF != XF_PLAIN) pnew[i] = xp;
+        if (ndot > 0) d0 += double(a0.get(i, out, xp, dinv) * b0.get(i, out, xp, dinv) * c0.get(i, out, xp, dinv));
+        if (ndot > 1) d1 += double(a1.get(i, out, xp, dinv) * b1.get(i, out, xp, dinv) * c1.get(i, out, xp, dinv));
+    }
+};
+
+// ---- shared-memory staging of a stream tile (16-byte cp.async copies)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Buffer layout: values (kTileNnz + one chunk), columns (kTileNnz + one
+// chunk), row pointers (kTileRows + 1 + one chunk).  Every copy is widened to
+// 16-byte boundaries; the device arrays carry 16 bytes of tail padding, so
+// the widened range stays inside the allocation.
+template <typename T>
+struct StageLayout {
+    static constexpr int VE = 16 / sizeof(T);
+    static constexpr int VBYTES = (kTileNnz + 2 * VE) * sizeof(T);
+    static constexpr int CBYTES = (kTileNnz + 8) * 4;
+    static constexpr int RBYTES = ((kTileRows + 1 + 8) * 4 + 15) / 16 * 16;
+    static constexpr int BYTES = VBYTES + CBYTES + RBYTES;
+    static_assert(VBYTES % 16 == 0 && CBYTES % 16 == 0 && BYTES % 16 == 0, "16-byte aligned sections");
+};
+
+template <typename T>
+__device__ __forceinline__ void stage_tile(const Tile& t, const int* rp, const int* ci, const T* va, unsigned char* buf)
+{
+    typedef StageLayout<T> SL;
+    const int ka = t.nnz_begin & ~(SL::VE - 1);
+    const int kb = (t.nnz_end + SL::VE - 1) & ~(SL::VE - 1);
+    for (int c = threadIdx.x; c < (kb - ka) / SL::VE; c += blockDim.x)
+        cp_async16(buf + c * 16, va + ka + c * SL::VE);
+    const int ca = t.nnz_begin & ~3, cb = (t.nnz_end + 3) & ~3;
+    for (int c = threadIdx.x; c < (cb - ca) / 4; c += blockDim.x)
+        cp_async16(buf + SL::VBYTES + c * 16, ci + ca + c * 4);
+    const int ra = t.row_begin & ~3, rb = (t.row_end + 1 + 3) & ~3;
+    for (int c = threadIdx.x; c < (rb - ra) / 4; c += blockDim.x)
+        cp_async16(buf + SL::VBYTES + SL::CBYTES + c * 16, rp + ra + c * 4);
+}
+
+// Persistent CTAs walk the tiles with a stride of the grid.  A stream tile's
+// values, columns and row pointers are copied into one of two shared-memory
+// buffers while the previous tile is summed from the other.  Every thread
+// then sums one row sequentially; rows longer than kShortRow are summed by a
+// warp from shared memory.  A long tile (one row with more than kTileNnz
+// entries) is summed by the whole CTA straight from global memory.
 template <typename T, int XF, int ASG>
 __global__ void __launch_bounds__(kBlock) k_spmv(SetView sv, SpmvOp op)
 {
-    __shared__ T s_val[kTileNnz];
-    __shared__ int s_col[kTileNnz];
+    typedef StageLayout<T> SL;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_med[kTileRows];
     __shared__ int s_nmed;
     __shared__ double s_red[kMaxDots * 32];
+    __shared__ T s_acc[32];
 
-    const int tile_id = blockIdx.x;
-    const Tile tile = sv.tiles[tile_id];
-    const int sys = tile.sys;
-    const SysDesc& d = sv.desc[sys];
-    const SysState& s = sv.st[sys];
-
-    if (op.count_body && tile_id == 0 && threadIdx.x == 0) {
-        // loop-body counter: bounds a graph while-loop independently of
-        // the solver's own termination test
+    if (op.count_body && blockIdx.x == 0 && threadIdx.x == 0) {
+        // loop-body counter: bounds a graph while-loop independently of the
+        // solver's own termination test
         int runs = atomicAdd(&sv.err[1], 1) + 1;
         if (runs > sv.err[2] || *(volatile int*)sv.running <= 0) set_cond(sv, 0u);
     }
-    if (skip_system(s, op.skip)) return;
+    const int G = gridDim.x;
+    int t = blockIdx.x;
+    if (t >= sv.n_tiles) return;
 
-    const int* __restrict__ rp = d.rp;
-    const int* __restrict__ ci = d.ci;
-    const T* __restrict__ va = static_cast<const T*>(d.val);
-    XIn<T, XF> xin;
-    xin.x = vptr<T>(d, op.x);
-    xin.p = op.p != SLOT_NONE ? vptr<T>(d, op.p) : nullptr;
-    xin.z = op.z != SLOT_NONE ? vptr<T>(d, op.z) : nullptr;
-    xin.dinv = static_cast<const T*>(d.inv_diag);
-    xin.beta = T(s.beta);
-    xin.first = (s.iter == 0);
-
-    RowEpilogue<T, ASG, XF> epi;
-    epi.y = vptr<T>(d, op.y);
-    epi.y2 = op.y2 != SLOT_NONE ? vptr<T>(d, op.y2) : nullptr;
-    epi.w = op.w != SLOT_NONE ? vptr<T>(d, op.w) : nullptr;
-    epi.pnew = op.pnew != SLOT_NONE ? vptr<T>(d, op.pnew) : nullptr;
-    epi.ndot = op.ndot;
-    epi.op = &op;
-    for (int j = 0; j < kMaxDots; ++j) {
-        epi.dvec[3 * j + 0] = (j < op.ndot && names_vector(op.da[j])) ? vptr<T>(d, op.da[j]) : nullptr;
-        epi.dvec[3 * j + 1] = (j < op.ndot && names_vector(op.db[j])) ? vptr<T>(d, op.db[j]) : nullptr;
-        epi.dvec[3 * j + 2] = (j < op.ndot && names_vector(op.dc[j])) ? vptr<T>(d, op.dc[j]) : nullptr;
+    Tile cur = sv.tiles[t];
+    {
+        const SysDesc& d0 = sv.desc[cur.sys];
+        if (cur.kind == TILE_STREAM && !skip_system(sv.st[cur.sys], op.skip))
+            stage_tile<T>(cur, d0.rp, d0.ci, static_cast<const T*>(d0.val), smem_raw);
+        cp_async_commit();
     }
-    double dot[kMaxDots] = {0.0, 0.0, 0.0, 0.0};
-    const T* dinv = xin.dinv;
+    Tile nxt = (t + G < sv.n_tiles) ? sv.tiles[t + G] : cur;
 
-    if (tile.kind == TILE_STREAM) {
-        const int rb = tile.row_begin, re = tile.row_end;
-        const int k0 = rp[rb], k1 = rp[re];
-        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-            s_val[k - k0] = va[k];
-            s_col[k - k0] = ci[k];
+    for (int it = 0; t < sv.n_tiles; t += G, ++it) {
+        const int tn = t + G;
+        Tile nn = (tn + G < sv.n_tiles) ? sv.tiles[tn + G] : nxt;   // metadata one tile ahead
+        unsigned char* buf = smem_raw + (it & 1) * SL::BYTES;
+        if (tn < sv.n_tiles) {
+            const SysDesc& dn = sv.desc[nxt.sys];
+            if (nxt.kind == TILE_STREAM && !skip_system(sv.st[nxt.sys], op.skip))
+                stage_tile<T>(nxt, dn.rp, dn.ci, static_cast<const T*>(dn.val), smem_raw + ((it + 1) & 1) * SL::BYTES);
         }
-        if (threadIdx.x == 0) s_nmed = 0;
+        cp_async_commit();
+        cp_async_wait_1();
         __syncthreads();
-        const int i = rb + threadIdx.x;
-        if (i < re) {
-            const int a = rp[i] - k0, e = rp[i + 1] - k0;
-            if (e - a <= kShortRow) {
-                T acc = T(0);
-                for (int k = a; k < e; ++k) acc = mac(acc, s_val[k], xin(s_col[k]));
-                epi(i, acc, xin(i), dinv, dot);
+
+        const Tile tile = cur;
+        const int sys = tile.sys;
+        const SysDesc& d = sv.desc[sys];
+        const SysState& s = sv.st[sys];
+        if (!skip_system(s, op.skip)) {
+            XIn<T, XF> xin;
+            xin.x = vptr<T>(d, op.x);
+            xin.p = op.p != SLOT_NONE ? vptr<T>(d, op.p) : nullptr;
+            xin.z = op.z != SLOT_NONE ? vptr<T>(d, op.z) : nullptr;
+            xin.dinv = static_cast<const T*>(d.inv_diag);
+            xin.beta = T(s.beta);
+            xin.first = (s.iter == 0);
+            const T* dinv = xin.dinv;
+
+            RowEpilogue<T, ASG, XF> epi;
+            epi.y = vptr<T>(d, op.y);
+            epi.y2 = op.y2 != SLOT_NONE ? vptr<T>(d, op.y2) : nullptr;
+            epi.w = op.w != SLOT_NONE ? vptr<T>(d, op.w) : nullptr;
+            epi.pnew = op.pnew != SLOT_NONE ? vptr<T>(d, op.pnew) : nullptr;
+            epi.ndot = op.ndot;
+            epi.a0 = {op.da[0], names_vector(op.da[0]) ? vptr<T>(d, op.da[0]) : nullptr};
+            epi.b0 = {op.db[0], names_vector(op.db[0]) ? vptr<T>(d, op.db[0]) : nullptr};
+            epi.c0 = {op.dc[0], names_vector(op.dc[0]) ? vptr<T>(d, op.dc[0]) : nullptr};
+            epi.a1 = {op.da[1], names_vector(op.da[1]) ? vptr<T>(d, op.da[1]) : nullptr};
+            epi.b1 = {op.db[1], names_vector(op.db[1]) ? vptr<T>(d, op.db[1]) : nullptr};
+            epi.c1 = {op.dc[1], names_vector(op.dc[1]) ? vptr<T>(d, op.dc[1]) : nullptr};
+            double d0 = 0.0, d1 = 0.0;
+
+            if (tile.kind == TILE_STREAM) {
+                const T* s_val = reinterpret_cast<const T*>(buf);
+                const int* s_col = reinterpret_cast<const int*>(buf + SL::VBYTES);
+                const int* s_rp = reinterpret_cast<const int*>(buf + SL::VBYTES + SL::CBYTES);
+                const int ka = tile.nnz_begin & ~(SL::VE - 1), ca = tile.nnz_begin & ~3, ra = tile.row_begin & ~3;
+                if (threadIdx.x == 0) s_nmed = 0;
+                __syncthreads();
+                const int i = tile.row_begin + threadIdx.x;
+                if (i < tile.row_end) {
+                    const int a = s_rp[i - ra], e = s_rp[i + 1 - ra];
+                    if (e - a <= kShortRow) {
+                        T acc = T(0);
+                        for (int k = a; k < e; ++k) acc = mac(acc, s_val[k - ka], xin(s_col[k - ca]));
+                        epi(i, acc, xin(i), dinv, d0, d1);
+                    } else {
+                        s_med[atomicAdd(&s_nmed, 1)] = i;
+                    }
+                }
+                __syncthreads();
+                const int nmed = s_nmed;
+                const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+                for (int m = warp; m < nmed; m += nw) {
+                    const int r = s_med[m];
+                    const int a = s_rp[r - ra], e = s_rp[r + 1 - ra];
+                    T acc = T(0);
+                    for (int k = a + lane; k < e; k += 32) acc = mac(acc, s_val[k - ka], xin(s_col[k - ca]));
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                    if (lane == 0) epi(r, acc, xin(r), dinv, d0, d1);
+                }
             } else {
-                s_med[atomicAdd(&s_nmed, 1)] = i;
+                const int r = tile.row_begin;
+                const int* __restrict__ ci = d.ci;
+                const T* __restrict__ va = static_cast<const T*>(d.val);
+                T acc = T(0);
+                for (int k = tile.nnz_begin + threadIdx.x; k < tile.nnz_end; k += blockDim.x)
+                    acc = mac(acc, va[k], xin(ci[k]));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+                if (lane == 0) s_acc[warp] = acc;
+                __syncthreads();
+                if (warp == 0) {
+                    acc = lane < (int)(blockDim.x >> 5) ? s_acc[lane] : T(0);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                    if (lane == 0) epi(r, acc, xin(r), dinv, d0, d1);
+                }
+            }
+            if (op.fin != FIN_NONE) {
+                double dd[kMaxDots] = {d0, d1, 0.0, 0.0};
+                block_reduce<kMaxDots>(dd, s_red);
+                if (publish_partials<kMaxDots>(sv, t, sys, dd)) {
+                    double tot[kMaxDots];
+                    gather_partials<kMaxDots>(sv, sys, tot, s_red);
+                    if (threadIdx.x == 0) finalize(sv, op.fin, sys, tot);
+                }
             }
         }
-        __syncthreads();
-        const int nmed = s_nmed;
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        for (int m = warp; m < nmed; m += nw) {
-            const int r = s_med[m];
-            const int a = rp[r] - k0, e = rp[r + 1] - k0;
-            T acc = T(0);
-            for (int k = a + lane; k < e; k += 32) acc = mac(acc, s_val[k], xin(s_col[k]));
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-            if (lane == 0) epi(r, acc, xin(r), dinv, dot);
-        }
-    } else {
-        const int r = tile.row_begin;
-        const int a = rp[r], e = rp[r + 1];
-        T acc = T(0);
-        for (int k = a + threadIdx.x; k < e; k += blockDim.x) acc = mac(acc, va[k], xin(ci[k]));
-        // fixed-shape CTA tree
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        __shared__ T s_acc[32];
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        if (lane == 0) s_acc[warp] = acc;
-        __syncthreads();
-        if (warp == 0) {
-            acc = lane < (int)(blockDim.x >> 5) ? s_acc[lane] : T(0);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-            if (lane == 0) epi(r, acc, xin(r), dinv, dot);
-        }
+        __syncthreads();   // the buffer is refilled two tiles later
+        cur = nxt;
+        nxt = nn;
     }
-
-    if (op.fin == FIN_NONE) return;
-    block_reduce<kMaxDots>(dot, s_red);
-    if (publish_partials<kMaxDots>(sv, tile_id, sys, dot)) {
-        double tot[kMaxDots];
-        gather_partials<kMaxDots>(sv, sys, tot, s_red);
-        if (threadIdx.x == 0) finalize(sv, op.fin, sys, tot);
-    }
+    cp_async_wait_0();
 }
 
 // ---------------------------------------------------------------- vector passes

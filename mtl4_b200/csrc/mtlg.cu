@@ -63,7 +63,7 @@ inline int vec_set(mtlg_ctx* c, int64_t n, SetView& sv)
     if (!vs) {
         vs.reset(new CtxExtra::VecSet);
         std::vector<Tile> tiles;
-        for (int64_t r = 0; r < n; r += kTileRows) tiles.push_back({0, int(r), int(std::min<int64_t>(n, r + kTileRows)), TILE_STREAM});
+        for (int64_t r = 0; r < n; r += kTileRows) tiles.push_back({0, int(r), int(std::min<int64_t>(n, r + kTileRows)), TILE_STREAM, 0, 0});
         vs->n_tiles = int(tiles.size());
         MTLG_TRY(vs->tiles.upload(c, tiles.data(), std::max<size_t>(1, tiles.size())));
         int stb[2] = {0, vs->n_tiles};
@@ -128,14 +128,16 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
     memset(&op, 0, sizeof op);
     op.skip = SKIP_NONE;
     op.fuse = SWF_NONE;
+    op.sleep_ns = c->sweep_sleep_ns;
+    const int grid = c->sweep_blocks();
     // y0 = L^{-1} x  (temp, slot 0); clears y row by row
     op.tasks = P->L.tasks.p; op.ntasks = int(P->L.tasks.n); op.ticket = P->tickets.p + 0; op.which = 0;
     op.in = SLOT_X; op.out = 0; op.reset = SLOT_B;
-    if (op.ntasks) { k_sweep<T, S><<<c->sweep_grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
+    if (op.ntasks) { k_sweep<T, S><<<grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
     // y = U^{-1} y0; clears the temp again
     op.tasks = P->U.tasks.p; op.ntasks = int(P->U.tasks.n); op.ticket = P->tickets.p + 1; op.which = 1;
     op.in = 0; op.out = SLOT_B; op.reset = 0;
-    if (op.ntasks) { k_sweep<T, S><<<c->sweep_grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
+    if (op.ntasks) { k_sweep<T, S><<<grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
     MTLG_CUDA(cudaGetLastError());
     int err = 0;
     MTLG_CUDA(cudaMemcpyAsync(&err, P->misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -198,7 +200,9 @@ int mtlg_ctx_create(int device, size_t hbm_budget, mtlg_ctx** out)
     int nb = 1, nb2 = 1;
     MTLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sweep<double, double>, kBlock, 0));
     MTLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_ilu0_factor, kBlock, 0));
-    c->sweep_grid = c->sm_count * std::max(1, std::min(nb, nb2));
+    c->sweep_max_bpsm = std::max(1, std::min(nb, nb2));
+    c->sweep_grid = c->sm_count * c->sweep_max_bpsm;
+    MTLG_TRY(init_kernel_shapes());
     *out = c.release();
     return MTLG_OK;
 }
@@ -238,6 +242,34 @@ int mtlg_ctx_set_stream(mtlg_ctx* c, void* s)
 }
 
 void* mtlg_ctx_stream(mtlg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
+{
+    MTLG_CHECK_ARG(c && key, "ctx/key");
+    const std::string k(key);
+    if (k == "sweep_blocks_per_sm") c->sweep_bpsm = int(std::max<int64_t>(0, value));
+    else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
+    else {
+        set_error("unknown tuning key '%s'", key);
+        return MTLG_ERR_INVALID_ARG;
+    }
+    return MTLG_OK;
+}
+
+int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
+{
+    MTLG_CHECK_ARG(c && key && value, "ctx/key/value");
+    const std::string k(key);
+    if (k == "sweep_blocks_per_sm") *value = c->sweep_bpsm;
+    else if (k == "sweep_max_blocks_per_sm") *value = c->sweep_max_bpsm;
+    else if (k == "sweep_sleep_ns") *value = c->sweep_sleep_ns;
+    else if (k == "sm_count") *value = c->sm_count;
+    else {
+        set_error("unknown tuning key '%s'", key);
+        return MTLG_ERR_INVALID_ARG;
+    }
+    return MTLG_OK;
+}
 int64_t mtlg_ctx_kernel_launches(mtlg_ctx* c) { return c ? c->launches : 0; }
 size_t mtlg_ctx_bytes_in_use(mtlg_ctx* c) { return c ? c->in_use : 0; }
 

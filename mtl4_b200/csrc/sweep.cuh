@@ -34,6 +34,7 @@ struct SweepOp {
     int skip;
     int fuse;           // SWF_* input transform of the L sweep
     int fuse_a, fuse_b, fuse_c;  // slots used by the transform
+    int sleep_ns;       // back-off between polls
 };
 
 enum SweepFuse : int { SWF_NONE = 0, SWF_BI_P = 1 };
@@ -56,7 +57,7 @@ __device__ __forceinline__ int grab_task(int* ticket, int ntasks)
 // err[0]) or as soon as another wait has given up, so a failed sweep drains
 // in one bounded wait instead of one per row.
 template <typename T>
-__device__ __forceinline__ T wait_value(const T* p, int* err)
+__device__ __forceinline__ T wait_value(const T* p, int* err, int sleep_ns)
 {
     T w = ld_volatile(p);
     if (!is_sentinel(w)) return w;
@@ -67,7 +68,7 @@ __device__ __forceinline__ T wait_value(const T* p, int* err)
             atomicExch(err, 1);
             return T(0);
         }
-        __nanosleep(32);
+        if (sleep_ns > 0) __nanosleep(sleep_ns);
         w = ld_volatile(p);
     } while (is_sentinel(w));
     return w;
@@ -130,9 +131,9 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            if (j < nr) rr = sweep_step<T, S>(rr, av[j], wait_value(y + cc[j], sv.err));
+            if (j < nr) rr = sweep_step<T, S>(rr, av[j], wait_value(y + cc[j], sv.err, op.sleep_ns));
         }
-        for (int j = a + 8; j < e; ++j) rr = sweep_step<T, S>(rr, fv[j], wait_value(y + fc[j], sv.err));
+        for (int j = a + 8; j < e; ++j) rr = sweep_step<T, S>(rr, fv[j], wait_value(y + fc[j], sv.err, op.sleep_ns));
         const S dia = static_cast<const S*>(F.dia)[k];
         typedef typename std::conditional<(sizeof(S) > sizeof(T)), S, T>::type W;   // promoted type
         st_volatile(y + row, unsentinel(T(W(rr) * W(dia))));

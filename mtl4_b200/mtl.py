@@ -38,6 +38,14 @@ class context:
     def bytes_in_use(self) -> int:
         return int(self._L.mtlg_ctx_bytes_in_use(self.h))
 
+    def set_tuning(self, key: str, value: int):
+        check(self._L.mtlg_ctx_set_tuning(self.h, key.encode(), int(value)), "set_tuning")
+
+    def get_tuning(self, key: str) -> int:
+        v = C.c_int64()
+        check(self._L.mtlg_ctx_get_tuning(self.h, key.encode(), C.byref(v)), "get_tuning")
+        return v.value
+
     def set_stream(self, cuda_stream_ptr: int | None):
         check(self._L.mtlg_ctx_set_stream(self.h, C.c_void_p(cuda_stream_ptr or 0)), "set_stream")
 

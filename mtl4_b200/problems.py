@@ -147,10 +147,10 @@ def vardiff_2d(m: int, sigma: float = 1.0, seed: int = 3, beta=None) -> CSR:
     return _face_diffusion((m, m), kappa, beta)
 
 
-# Continuous Pareto(alpha) floored and clipped to [1, 4096]; x_min is chosen
-# so the mean row length is ~9.5 (about 40M entries on 4,194,304 rows).  With
-# x_min = 1 the mean would be ~6.2 (~26M entries).
-POWERLAW_XMIN = 5.0
+# Continuous Pareto (density ~ x^-alpha, alpha = 2.1) floored and clipped to
+# [1, 4096].  x_min = 1.55 gives a mean row length of ~9.5, i.e. ~40M entries
+# on 4,194,304 rows; x_min = 1 would give ~6.3 (~26M entries).
+POWERLAW_XMIN = 1.55
 
 
 def powerlaw_csr(n: int = 4 * 2 ** 20, alpha: float = 2.1, lo: int = 1, hi: int = 4096,
