@@ -124,8 +124,9 @@ void* mtlg_ctx_stream(mtlg_ctx* ctx);
  * count every kernel node they run). */
 int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
 /* Launch-shape tuning (used by the autotuner): "sweep_blocks_per_sm"
- * (0 = as many as fit), "sweep_sleep_ns" (poll back-off of the triangular
- * sweeps).  Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
+ * (default 1), "sweep_blocks" (absolute grid of the triangular sweeps,
+ * overrides the former when > 0), "sweep_sleep_ns" (poll back-off, default
+ * 0).  Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
 int mtlg_ctx_set_tuning(mtlg_ctx* ctx, const char* key, int64_t value);
 int mtlg_ctx_get_tuning(mtlg_ctx* ctx, const char* key, int64_t* value);
 /* Bytes of device memory the context's objects hold. */

@@ -126,7 +126,7 @@ struct SysState {
     double nb;              // refinement: ||b||
     int iter, max_iter, status, error;
     int ostatus;            // refinement (outer) status
-    int pad1;
+    int phase;              // served solves: PH_* (ignored by the other engines)
     int first, flags;
     int outer, max_outer;
     int inner_total, inner_max;
@@ -264,6 +264,17 @@ __device__ __forceinline__ void gather_partials(const SetView& sv, int sys, doub
     block_reduce<ND>(out, smem);
 }
 
+// Phases of a served solve (continuous batching): each engine step runs the
+// kernels of every phase, and each kernel acts only on the slots in its
+// phase, so requests admitted at different times share the same launches.
+enum Phase : int { PH_INIT = 0, PH_OUTER = 1, PH_CAST = 2, PH_INNER = 3, PH_UPDATE = 4, PH_DONE = 5 };
+
+__device__ __forceinline__ void inner_done(SysState& s)
+{
+    // refinement solves go back for an FP64 update, plain ones are finished
+    if (s.phase == PH_INNER) s.phase = (s.max_outer > 0) ? PH_UPDATE : PH_DONE;
+}
+
 __device__ __forceinline__ void set_cond(const SetView& sv, unsigned v)
 {
     if (sv.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)sv.cond, v);
@@ -289,6 +300,7 @@ __device__ __forceinline__ bool check_finished(const SetView& sv, SysState& s, d
     } else {
         return false;
     }
+    inner_done(s);
     if (atomicSub(sv.running, 1) == 1) set_cond(sv, 0u);
     return true;
 }
@@ -297,6 +309,7 @@ __device__ __forceinline__ void retire(const SetView& sv, SysState& s, int statu
 {
     s.status = status;
     s.error = error;
+    inner_done(s);
     if (atomicSub(sv.running, 1) == 1) set_cond(sv, 0u);
 }
 

@@ -17,11 +17,13 @@ struct mtlg_ctx {
     int sweep_grid = 148;       // persistent grid of the sweep / factor kernels
     int sweep_max_bpsm = 1;     // resident sweep CTAs per SM the device allows
     int sweep_bpsm = 0;         // tuning: sweep CTAs per SM (0: as many as fit)
-    int sweep_sleep_ns = 32;    // tuning: back-off between polls of a dependency
+    int sweep_sleep_ns = 0;     // tuning: back-off between polls of a dependency
+    int sweep_nblocks = 0;      // tuning: absolute sweep grid (0: use sweep_bpsm)
     int* d_scratch_err = nullptr;
     int sweep_blocks() const
     {
-        const int b = sweep_bpsm > 0 ? std::min(sweep_bpsm, sweep_max_bpsm) : sweep_max_bpsm;
+        if (sweep_nblocks > 0) return std::min(sweep_nblocks, sm_count * sweep_max_bpsm);
+        const int b = sweep_bpsm > 0 ? std::min(sweep_bpsm, sweep_max_bpsm) : 1;
         return sm_count * b;
     }
 };

@@ -250,7 +250,7 @@ inline void set_dot(VecOp& op, int j, int a, int b, int c = OPND_ONE)
 //   (r -= alpha q) || (rr = r.r);  loop while !finished(sqrt(|rr|)).
 // Identity PC: cg.hpp:40-71 (z = r).
 template <typename T>
-inline int cg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inner_refine)
+inline int cg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inner_refine, int skip = -1)
 {
     mtlg_ctx* c = ss.ctx;
     if (inner_refine) {
@@ -259,7 +259,7 @@ inline int cg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inner_
         set_dot(op, 0, V_R, V_R);
         if (ss.path == PATH_JACOBI) { set_dot(op, 1, V_R, V_R, OPND_D); op.fin = FIN_REF_CG_INIT_JAC; }
         else op.fin = FIN_REF_CG_INIT;
-        op.skip = SKIP_OUTER;
+        op.skip = skip >= 0 ? skip : SKIP_OUTER;
         return launch_vec<T>(c, st, sv, op);
     }
     SpmvOp op = spmv_op_default();
@@ -267,6 +267,7 @@ inline int cg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inner_
     set_dot(op, 0, OPND_Y, OPND_Y);
     if (ss.path == PATH_JACOBI) { set_dot(op, 1, OPND_Y, OPND_Y, OPND_D); op.fin = FIN_CG_INIT_JAC; }
     else op.fin = FIN_CG_INIT;
+    if (skip >= 0) op.skip = skip;
     return launch_spmv<T>(c, st, sv, op, XF_PLAIN, ASG_WMINUS);
 }
 
@@ -310,7 +311,7 @@ inline int cg_half(SolveSet& ss, cudaStream_t st, const SetView& sv, int pin, in
 // Reference body (itl/krylov/bicgstab.hpp:29-77), see k_vec VOP_BI_* and the
 // FIN_BI_* finalize steps for the scalar updates and breakdown tests.
 template <typename T>
-inline int bicg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inner_refine)
+inline int bicg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inner_refine, int skip = -1)
 {
     mtlg_ctx* c = ss.ctx;
     if (inner_refine) {
@@ -319,7 +320,7 @@ inline int bicg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inne
         set_dot(op, 0, V_RT, V_R);
         set_dot(op, 1, V_R, V_R);
         op.fin = FIN_REF_BI_INIT;
-        op.skip = SKIP_OUTER;
+        op.skip = skip >= 0 ? skip : SKIP_OUTER;
         return launch_vec<T>(c, st, sv, op);
     }
     SpmvOp op = spmv_op_default();
@@ -327,6 +328,7 @@ inline int bicg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inne
     set_dot(op, 0, OPND_Y, OPND_Y);
     set_dot(op, 1, OPND_Y, OPND_Y);
     op.fin = FIN_BI_TOP;
+    if (skip >= 0) op.skip = skip;
     return launch_spmv<T>(c, st, sv, op, XF_PLAIN, ASG_WMINUS);
 }
 

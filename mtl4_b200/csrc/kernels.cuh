@@ -52,6 +52,7 @@ enum Fin : int {
     FIN_REF_CG_INIT,    // inner CG init on the scaled residual (norm_r0 = ||r||)
     FIN_REF_CG_INIT_JAC,
     FIN_REF_BI_INIT,    // inner BiCGSTAB init (norm_r0 = ||r||)
+    FIN_PHASE_OUTER,    // served refinement: back to the outer residual
 };
 
 // Status flags
@@ -84,28 +85,33 @@ __device__ void finalize(const SetView& sv, int fin, int sys, const double* dots
         s.nb = sqrt(fabs(dots[0]));
         break;
     case FIN_REF_CG_INIT:
+        s.phase = PH_INNER;
         s.norm_r0 = sqrt(fabs(dots[0]));
         s.rr = dots[0];
         s.rho = dots[0];
         check_finished(sv, s, sqrt(fabs(dots[0])));
         break;
     case FIN_REF_CG_INIT_JAC:
+        s.phase = PH_INNER;
         s.norm_r0 = sqrt(fabs(dots[0]));
         s.rr = dots[0];
         s.rho = dots[1];
         check_finished(sv, s, sqrt(fabs(dots[0])));
         break;
     case FIN_REF_BI_INIT:
+        s.phase = PH_INNER;
         s.norm_r0 = sqrt(fabs(dots[1]));
         bicg_top(sv, s, dots[0], dots[1], true);
         break;
     case FIN_CG_INIT:
+        s.phase = PH_INNER;
         s.rr = dots[0];
         s.rho = dots[0];
         s.iter = 0;
         check_finished(sv, s, sqrt(fabs(dots[0])));
         break;
     case FIN_CG_INIT_JAC:
+        s.phase = PH_INNER;
         s.rr = dots[0];
         s.rho = dots[1];
         s.iter = 0;
@@ -142,7 +148,11 @@ __device__ void finalize(const SetView& sv, int fin, int sys, const double* dots
         s.beta = s.rho / s.rho_1;
         break;
     case FIN_BI_TOP:
+        if (s.iter == 0) s.phase = PH_INNER;
         bicg_top(sv, s, dots[0], dots[1], s.iter == 0);
+        break;
+    case FIN_PHASE_OUTER:
+        s.phase = PH_OUTER;
         break;
     case FIN_BI_GAMMA:
         s.gamma = dots[0];
@@ -172,14 +182,15 @@ __device__ void finalize(const SetView& sv, int fin, int sys, const double* dots
         s.resid = rn;
         s.flags = 0;
         if (rn <= s.outer_rtol * s.nb) {
-            s.ostatus = MTLG_ST_CONVERGED; s.status = MTLG_ST_CONVERGED; s.error = 0;
+            s.ostatus = MTLG_ST_CONVERGED; s.status = MTLG_ST_CONVERGED; s.error = 0; s.phase = PH_DONE;
         } else if (isnan(rn) || isinf(rn)) {
-            s.ostatus = MTLG_ST_BREAKDOWN; s.status = MTLG_ST_BREAKDOWN; s.error = 1;
+            s.ostatus = MTLG_ST_BREAKDOWN; s.status = MTLG_ST_BREAKDOWN; s.error = 1; s.phase = PH_DONE;
         } else if (s.outer >= s.max_outer) {
-            s.ostatus = MTLG_ST_MAXIT; s.status = MTLG_ST_MAXIT; s.error = 1;
+            s.ostatus = MTLG_ST_MAXIT; s.status = MTLG_ST_MAXIT; s.error = 1; s.phase = PH_DONE;
         } else {
             s.outer += 1;
             s.status = MTLG_ST_RUNNING;
+            s.phase = PH_CAST;
             atomicAdd(sv.running, 1);
         }
         break;
@@ -192,7 +203,8 @@ __device__ void finalize(const SetView& sv, int fin, int sys, const double* dots
 // ---------------------------------------------------------------- SpMV
 enum XForm : int { XF_PLAIN = 0, XF_CG_P = 1, XF_CG_P_JAC = 2, XF_JAC = 3 };
 enum Assign : int { ASG_SET = 0, ASG_ADD = 1, ASG_SUB = 2, ASG_WMINUS = 3 };
-enum Skip : int { SKIP_NONE = 0, SKIP_INNER = 1, SKIP_OUTER = 2, SKIP_RUNNING = 3 };
+enum Skip : int { SKIP_NONE = 0, SKIP_INNER = 1, SKIP_OUTER = 2, SKIP_RUNNING = 3, SKIP_PH_BASE = 16 };
+// SKIP_PH_BASE + p: act only on systems in phase p (served solves)
 
 struct SpmvOp {
     int x, y, w;        // input slot, output slot, W for y = W - A x
@@ -210,6 +222,7 @@ __device__ __forceinline__ bool skip_system(const SysState& s, int mode)
     if (mode == SKIP_INNER) return s.status != MTLG_ST_RUNNING || (s.flags & FLAG_FINISHING);
     if (mode == SKIP_OUTER) return s.ostatus != MTLG_ST_RUNNING;
     if (mode == SKIP_RUNNING) return s.status != MTLG_ST_RUNNING;
+    if (mode >= SKIP_PH_BASE) return s.phase != mode - SKIP_PH_BASE;
     return false;
 }
 
@@ -409,8 +422,21 @@ __global__ void __launch_bounds__(kBlock) k_spmv(SetView sv, SpmvOp op)
                 if (i < tile.row_end) {
                     const int a = s_rp[i - ra], e = s_rp[i + 1 - ra];
                     if (e - a <= kShortRow) {
+                        // gathers issued 8 at a time, summed in storage order
                         T acc = T(0);
-                        for (int k = a; k < e; ++k) acc = mac(acc, s_val[k - ka], xin(s_col[k - ca]));
+                        int k = a;
+                        for (; k + 8 <= e; k += 8) {
+                            T xv[8];
+#pragma unroll
+                            for (int u = 0; u < 8; ++u) xv[u] = xin(s_col[k + u - ca]);
+#pragma unroll
+                            for (int u = 0; u < 8; ++u) acc = mac(acc, s_val[k + u - ka], xv[u]);
+                        }
+                        T xv[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) if (k + u < e) xv[u] = xin(s_col[k + u - ca]);
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) if (k + u < e) acc = mac(acc, s_val[k + u - ka], xv[u]);
                         epi(i, acc, xin(i), dinv, d0, d1);
                     } else {
                         s_med[atomicAdd(&s_nmed, 1)] = i;
@@ -423,7 +449,16 @@ __global__ void __launch_bounds__(kBlock) k_spmv(SetView sv, SpmvOp op)
                     const int r = s_med[m];
                     const int a = s_rp[r - ra], e = s_rp[r + 1 - ra];
                     T acc = T(0);
-                    for (int k = a + lane; k < e; k += 32) acc = mac(acc, s_val[k - ka], xin(s_col[k - ca]));
+                    int k = a + lane;
+                    for (; k + 3 * 32 < e; k += 4 * 32) {
+                        const T x0 = xin(s_col[k - ca]), x1 = xin(s_col[k + 32 - ca]);
+                        const T x2 = xin(s_col[k + 64 - ca]), x3 = xin(s_col[k + 96 - ca]);
+                        acc = mac(acc, s_val[k - ka], x0);
+                        acc = mac(acc, s_val[k + 32 - ka], x1);
+                        acc = mac(acc, s_val[k + 64 - ka], x2);
+                        acc = mac(acc, s_val[k + 96 - ka], x3);
+                    }
+                    for (; k < e; k += 32) acc = mac(acc, s_val[k - ka], xin(s_col[k - ca]));
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
                     if (lane == 0) epi(r, acc, xin(r), dinv, d0, d1);
@@ -433,8 +468,18 @@ __global__ void __launch_bounds__(kBlock) k_spmv(SetView sv, SpmvOp op)
                 const int* __restrict__ ci = d.ci;
                 const T* __restrict__ va = static_cast<const T*>(d.val);
                 T acc = T(0);
-                for (int k = tile.nnz_begin + threadIdx.x; k < tile.nnz_end; k += blockDim.x)
-                    acc = mac(acc, va[k], xin(ci[k]));
+                int k = tile.nnz_begin + threadIdx.x;
+                const int B = blockDim.x;
+                for (; k + 3 * B < tile.nnz_end; k += 4 * B) {
+                    const int c0 = ci[k], c1 = ci[k + B], c2 = ci[k + 2 * B], c3 = ci[k + 3 * B];
+                    const T v0 = va[k], v1 = va[k + B], v2 = va[k + 2 * B], v3 = va[k + 3 * B];
+                    const T x0 = xin(c0), x1 = xin(c1), x2 = xin(c2), x3 = xin(c3);
+                    acc = mac(acc, v0, x0);
+                    acc = mac(acc, v1, x1);
+                    acc = mac(acc, v2, x2);
+                    acc = mac(acc, v3, x3);
+                }
+                for (; k < tile.nnz_end; k += B) acc = mac(acc, va[k], xin(ci[k]));
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
                 const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

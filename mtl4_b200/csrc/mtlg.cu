@@ -153,6 +153,54 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
     return MTLG_OK;
 }
 
+// SpMV on raw device pointers of the CSR's size (GMRES workspace vectors);
+// w (optional) is the W of y = W - A x.
+int spmv_raw(mtlg_ctx* c, mtlg_csr* A, int dtype, const void* x, void* y, const void* w, int asg)
+{
+    const bool f32 = dtype == MTLG_F32;
+    if (f32) MTLG_TRY(ensure_f32_values(A));
+    SetView sv;
+    MTLG_TRY(csr_op_set(A, sv));
+    SysDesc d;
+    memset(&d, 0, sizeof d);
+    d.n = int(A->n_rows);
+    d.nnz = int(A->nnz);
+    d.rp = A->rp.p;
+    d.ci = A->ci.p;
+    d.val = f32 ? (const void*)A->v32.p : (const void*)A->v64.p;
+    d.val64 = A->v64.p;
+    d.x = const_cast<void*>(x);
+    d.b = y;
+    d.ws = const_cast<void*>(w);
+    d.ws_stride = 0;
+    MTLG_CUDA(cudaMemcpyAsync(sv.desc, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
+    SpmvOp op = spmv_op_default();
+    op.x = SLOT_X;
+    op.y = SLOT_B;
+    op.w = w ? 0 : SLOT_NONE;
+    if (f32) return launch_spmv<float>(c, c->stream, sv, op, XF_PLAIN, asg);
+    return launch_spmv<double>(c, c->stream, sv, op, XF_PLAIN, asg);
+}
+
+}  // namespace mtlg
+
+extern "C" int mtlg_pc_apply(mtlg_ctx* c, mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y);
+
+namespace mtlg {
+int pc_apply_raw(mtlg_ctx* c, mtlg_pc* P, int dtype, int64_t n, const void* x, void* y)
+{
+    if (!P || P->kind == MTLG_PC_IDENTITY) {
+        if (x != y) MTLG_CUDA(cudaMemcpyAsync(y, x, size_t(n) * (dtype == MTLG_F32 ? 4 : 8), cudaMemcpyDeviceToDevice, c->stream));
+        return MTLG_OK;
+    }
+    mtlg_vec xv, yv;
+    xv.ctx = yv.ctx = c;
+    xv.n = yv.n = n;
+    xv.dtype = yv.dtype = dtype;
+    xv.p = const_cast<void*>(x);
+    yv.p = y;
+    return mtlg_pc_apply(c, P, &xv, &yv);
+}
 }  // namespace mtlg
 
 extern "C" {
@@ -248,6 +296,7 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     MTLG_CHECK_ARG(c && key, "ctx/key");
     const std::string k(key);
     if (k == "sweep_blocks_per_sm") c->sweep_bpsm = int(std::max<int64_t>(0, value));
+    else if (k == "sweep_blocks") c->sweep_nblocks = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 16)));
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
     else {
         set_error("unknown tuning key '%s'", key);
@@ -261,6 +310,7 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     MTLG_CHECK_ARG(c && key && value, "ctx/key/value");
     const std::string k(key);
     if (k == "sweep_blocks_per_sm") *value = c->sweep_bpsm;
+    else if (k == "sweep_blocks") *value = c->sweep_blocks();
     else if (k == "sweep_max_blocks_per_sm") *value = c->sweep_max_bpsm;
     else if (k == "sweep_sleep_ns") *value = c->sweep_sleep_ns;
     else if (k == "sm_count") *value = c->sm_count;

@@ -286,3 +286,47 @@ def test_refinement_fp32_inner_fp64_outer(ctx, solver, pc):
     assert rel <= 1e-10
     x64 = O.port_solve(A, b, solver, pc, max_iter=5000, rtol=1e-13)["x"]
     assert np.abs(xs - x64).max() <= 1e-6 * np.abs(x64).max()
+
+
+# ---------------------------------------------------------------- GMRES
+def test_gmres_kat_small_laplacian(ctx):
+    # libs/numeric/itl/test/gmres_test.cpp:52-128: 2x2-grid Laplacian,
+    # GMRES(k) for k = 1..8 reaches ||r|| < 5e-5
+    from mtl4_b200 import itl, mtl
+    A = P.laplacian_2d(2)
+    Ad = dev(A, ctx)
+    b = np.ones(4)
+    for k in range(1, 9):
+        x = mtl.dense_vector(4, np.float64, ctx)
+        bd = vec(b, ctx)
+        it = itl.basic_iteration(bd, 100, 1e-10)
+        itl.gmres(Ad, x, bd, None, None, it, k)
+        assert np.linalg.norm(A.matvec(x.numpy()) - b) < 5e-5
+
+
+@pytest.mark.parametrize("restart,pc", [(10, "identity"), (30, "identity"), (20, "ilu_0"), (8, "diagonal")])
+def test_gmres_matches_restatement(ctx, golden, restart, pc):
+    from mtl4_b200 import itl, mtl
+    A = csr_from(golden, "lap32")
+    b = golden["lap32_b"]
+    Ad = dev(A, ctx)
+    L = None if pc == "identity" else getattr(itl.pc, pc)(Ad)
+    x = mtl.dense_vector(A.n_rows, np.float64, ctx)
+    bd = vec(b, ctx)
+    it = itl.basic_iteration(bd, 3000, 1e-8)
+    itl.gmres(Ad, x, bd, L, None, it, restart)
+    ref = O.port_solve(A, b, "gmres", pc, max_iter=3000, rtol=1e-8, restart=restart)
+    assert it.error_code() == ref["error"] == 0
+    assert abs(it.iterations() - ref["iterations"]) <= restart   # same number of restart cycles (+-1)
+    assert np.linalg.norm(A.matvec(x.numpy()) - b) <= 1.05e-8 * np.linalg.norm(b)
+
+
+def test_gmres_max_iterations(ctx):
+    from mtl4_b200 import itl, mtl
+    A, b, _ = P.config1()
+    Ad = dev(A, ctx)
+    x = mtl.dense_vector(A.n_rows, np.float64, ctx)
+    bd = vec(b, ctx)
+    it = itl.basic_iteration(bd, 25, 1e-8)
+    itl.gmres(Ad, x, bd, None, None, it, 10)
+    assert it.error_code() == 1 and it.iterations() == 25
