@@ -191,7 +191,9 @@ def main():
     from mtl4_b200 import problems as P
 
     torch.cuda.set_device(local)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream: kernels and timing events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = mtl.context(local)
     ctx.set_stream(stream.cuda_stream)
     mtl._DEFAULT[local] = ctx
