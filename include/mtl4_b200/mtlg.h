@@ -164,6 +164,19 @@ int64_t mtlg_vec_size(const mtlg_vec* v);
 int mtlg_spmv(mtlg_ctx* ctx, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, int assign);
 /* Fused q = A p and the dot p.q (cg.hpp:103 lazy pair) in one pass. */
 int mtlg_spmv_dot(mtlg_ctx* ctx, mtlg_csr* A, const mtlg_vec* p, mtlg_vec* q, double* pq);
+/* Allocation-free q = A p with p.q, for callers that cannot allocate device
+ * memory (a fully reserved budget, a foreign memory pool, a real-time loop
+ * where cudaMalloc may block).  No counterpart in the reference.  All
+ * pointers are caller-owned device memory (CSR with int32 row_ptr/col, FP64
+ * values; *dot written on the device); stream is a cudaStream_t (NULL: the
+ * legacy default stream).  Scratch is a file-scope device array of 4096 CTA
+ * partial sums (~32 KiB per GPU, held until exit), so n_rows <= 1,048,576
+ * (MTLG_ERR_TOO_LARGE beyond); square matrices only.  Calls share that
+ * array: calls that can overlap on the GPU race and must be serialized.  The
+ * first call on a device looks up the array's address; make it before any
+ * stream capture. */
+int mtlg_spmv_dot_noalloc(int64_t n_rows, int64_t n_cols, const int32_t* row_ptr, const int32_t* col,
+                          const double* val, const double* p, double* q, double* dot, void* stream);
 int mtlg_dot(mtlg_ctx* ctx, const mtlg_vec* x, const mtlg_vec* y, double* out);
 int mtlg_two_norm(mtlg_ctx* ctx, const mtlg_vec* x, double* out);
 /* y += a x */

@@ -26,7 +26,7 @@ def needs_build() -> bool:
 
 def build_library(force: bool = False, verbose: bool = False) -> Path:
     if force or needs_build():
-        cmd = [NVCC, *FLAGS, str(SRC / "mtlg.cu"), "-o", str(OUT)]
+        cmd = [NVCC, *FLAGS, str(SRC / "mtlg.cu"), str(SRC / "noalloc.cu"), "-o", str(OUT)]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
