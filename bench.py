@@ -171,6 +171,40 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ profiling cases
+def run_kernel_case(args):
+    """One kernel on its bench case, `reps` times (no timing output): the
+    command line the committed ncu summaries under profiles/ were made with."""
+    from mtl4_b200 import itl, mtl
+    from mtl4_b200 import problems as P
+    ctx = mtl.context(0)
+    if args.kernel in ("spmv_powerlaw", "spmv_stencil"):
+        A = P.config2_spmv() if args.kernel == "spmv_powerlaw" else P.config2_solve(128)[0]
+        Ad = mtl.compressed2D.from_problem(A, ctx)
+        x = mtl.dense_vector(np.random.default_rng(0).standard_normal(A.n_rows), np.float64, ctx)
+        y = mtl.dense_vector(A.n_rows, np.float64, ctx)
+        for _ in range(args.reps):
+            mtl.mult(Ad, x, y)
+    elif args.kernel == "sweep_ilu0":
+        A, b, _ = P.config2_solve(128)
+        Ad = mtl.compressed2D.from_problem(A, ctx)
+        Pc = itl.pc.ilu_0(Ad, np.float32)
+        bf = mtl.dense_vector(b.astype(np.float32), np.float32, ctx)
+        yf = mtl.dense_vector(A.n_rows, np.float32, ctx)
+        for _ in range(args.reps):
+            itl.solve(Pc, bf, yf)
+    else:
+        A, b, _ = P.config2_solve(128)
+        Ad = mtl.compressed2D.from_problem(A, ctx)
+        Pc = itl.pc.ilu_0(Ad, np.float32)
+        bd = mtl.dense_vector(b, np.float64, ctx)
+        for _ in range(args.reps):
+            x = mtl.dense_vector(A.n_rows, np.float64, ctx)
+            itl.refine("bicgstab", Ad, x, bd, Pc, rtol=1e-8, inner_rtol=1e-4)
+    ctx.synchronize()
+    print(json.dumps({"kernel": args.kernel, "reps": args.reps, "launches": ctx.kernel_launches()}))
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -179,8 +213,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mtl4_b200", choices=["mtl4_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", choices=["spmv_powerlaw", "spmv_stencil", "sweep_ilu0", "solve_mixed"],
+                    help="run one kernel on its bench case a few times and exit (for profilers)")
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup) if args.impl != "reference" else args.warmup
+    if args.kernel:
+        run_kernel_case(args)
+        return
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world)
