@@ -126,7 +126,11 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
 /* Launch-shape tuning (used by the autotuner): "sweep_blocks_per_sm"
  * (default 1), "sweep_blocks" (absolute grid of the triangular sweeps,
  * overrides the former when > 0), "sweep_sleep_ns" (poll back-off, default
- * 0).  Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
+ * 0), "loop_mode" (0: the Krylov loop runs as chunks of 8 iterations in
+ * plain CUDA graphs, two in flight; 1: one graph with a WHILE conditional
+ * node per solve), "spmv_kernel" (standalone SpMV: 0 chooses by row
+ * lengths, 1 shared-memory stream tiles, 2 row-aligned warp tasks).
+ * Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
 int mtlg_ctx_set_tuning(mtlg_ctx* ctx, const char* key, int64_t value);
 int mtlg_ctx_get_tuning(mtlg_ctx* ctx, const char* key, int64_t* value);
 /* Bytes of device memory the context's objects hold. */

@@ -19,6 +19,8 @@ struct mtlg_ctx {
     int sweep_bpsm = 0;         // tuning: sweep CTAs per SM (0: as many as fit)
     int sweep_sleep_ns = 0;     // tuning: back-off between polls of a dependency
     int sweep_nblocks = 0;      // tuning: absolute sweep grid (0: use sweep_bpsm)
+    int loop_mode = 0;          // tuning: 0 chunked plain graphs, 1 WHILE conditional graph
+    int spmv_kernel = 0;        // tuning: 0 auto (row-length statistics), 1 stream tiles, 2 warp tasks
     int* d_scratch_err = nullptr;
     int sweep_blocks() const
     {
@@ -134,6 +136,29 @@ inline void plan_tiles(const int64_t* rp, int n, int sys, std::vector<Tile>& out
     }
 }
 
+// Row-aligned warp tasks (see k_spmv_rows).
+inline void plan_warp_tasks(const int64_t* rp, int n, std::vector<WarpTask>& out)
+{
+    int r = 0;
+    while (r < n) {
+        int64_t len = rp[r + 1] - rp[r];
+        if (len > kWarpNnz) {
+            out.push_back({r, r + 1, int(rp[r]), int(rp[r + 1])});
+            ++r;
+            continue;
+        }
+        const int rb = r;
+        int64_t nnz = 0;
+        while (r < n && r - rb < kWarpNnz) {
+            len = rp[r + 1] - rp[r];
+            if (len > kWarpNnz || nnz + len > kWarpNnz) break;
+            nnz += len;
+            ++r;
+        }
+        out.push_back({rb, r, int(rp[rb]), int(rp[r])});
+    }
+}
+
 }  // namespace mtlg
 
 using namespace mtlg;
@@ -160,6 +185,9 @@ struct mtlg_csr {
     std::vector<Tile> tiles;
     int max_row = 0;
     int64_t tiles_by_kind[3] = {0, 0, 0};
+    std::vector<WarpTask> wtasks;  // row-aligned warp tasks (irregular matrices)
+    DBuf<WarpTask> d_wtasks;
+    bool irregular = false;        // some row longer than kShortRow entries
     // single-system operation set (standalone SpMV / dot)
     DBuf<Tile> d_tiles;
     DBuf<int> d_stb;

@@ -50,10 +50,20 @@ struct SolveSet {
     int body_kernels = 0;
     int iters_per_body = 1;
     bool graph_failed = false;
+    // chunked loop: kChunkBodies bodies in a plain graph, two chunks in flight
+    cudaGraph_t chunk_graph = nullptr;
+    cudaGraphExec_t chunk_exec = nullptr;
+    int chunk_kernels = 0;
+    int* h_running = nullptr;       // pinned host copies of the running count
+    cudaEvent_t chunk_ev[2] = {nullptr, nullptr};
     ~SolveSet()
     {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
+        if (chunk_graph) cudaGraphDestroy(chunk_graph);
+        if (h_running) cudaFreeHost(h_running);
+        for (auto& e : chunk_ev) if (e) cudaEventDestroy(e);
         if (cap_stream) cudaStreamDestroy(cap_stream);
     }
 
@@ -460,16 +470,68 @@ inline int build_graph(SolveSet& ss)
     return MTLG_OK;
 }
 
-// Runs the loop until no system is running.  Graph path: one launch; the
-// fallback path replays the body from the host in chunks and polls.
+constexpr int kChunkBodies = 8;
+
+// Chunked loop (default): kChunkBodies loop bodies captured in a plain CUDA
+// graph; the host keeps two chunks in flight and reads the running count of
+// the older one (pinned memory, event) before queueing the next, so the GPU
+// never waits for the host.  Bodies queued after the last system stopped
+// return at once.  Kernels of plain graphs can be profiled node by node.
+template <typename T>
+inline int run_loop_chunked(SolveSet& ss, int max_iter)
+{
+    mtlg_ctx* c = ss.ctx;
+    if (!ss.chunk_exec) {
+        if (!ss.cap_stream) MTLG_CUDA(cudaStreamCreateWithFlags(&ss.cap_stream, cudaStreamNonBlocking));
+        if (!ss.h_running) MTLG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ss.h_running), 2 * sizeof(int), 0));
+        for (auto& e : ss.chunk_ev)
+            if (!e) MTLG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        const int64_t before = c->launches;
+        MTLG_CUDA(cudaStreamBeginCapture(ss.cap_stream, cudaStreamCaptureModeThreadLocal));
+        int s = MTLG_OK;
+        const SetView sv = ss.view(false, false);
+        for (int k = 0; k < kChunkBodies && s == MTLG_OK; ++k) s = enqueue_body<T>(ss, ss.cap_stream, sv);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ss.cap_stream, &g);
+        ss.chunk_kernels = int(c->launches - before);
+        c->launches = before;
+        MTLG_TRY(s);
+        MTLG_CUDA(e);
+        ss.chunk_graph = g;
+        MTLG_CUDA(cudaGraphInstantiate(&ss.chunk_exec, g, 0));
+    }
+    const int ipb = iters_per_body(ss);
+    const int max_chunks = max_iter / (ipb * kChunkBodies) + 2;
+    int launched = 0;
+    for (int k = 0; k < max_chunks; ++k) {
+        MTLG_CUDA(cudaGraphLaunch(ss.chunk_exec, c->stream));
+        c->launches += ss.chunk_kernels;
+        MTLG_CUDA(cudaMemcpyAsync(ss.h_running + (k & 1), ss.misc.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        MTLG_CUDA(cudaEventRecord(ss.chunk_ev[k & 1], c->stream));
+        ++launched;
+        if (k >= 1) {
+            MTLG_CUDA(cudaEventSynchronize(ss.chunk_ev[(k - 1) & 1]));
+            if (ss.h_running[(k - 1) & 1] <= 0) break;
+        }
+    }
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    (void)launched;
+    return MTLG_OK;
+}
+
+// Runs the loop until no system is running.  Default: chunked plain graphs
+// (run_loop_chunked).  loop_mode 1: one graph with a WHILE conditional node,
+// one launch per solve.  If a graph cannot be built, the body is replayed
+// from the host in chunks.
 template <typename T>
 inline int run_loop(SolveSet& ss, int max_iter)
 {
     mtlg_ctx* c = ss.ctx;
-    MTLG_TRY(build_graph<T>(ss));
     const int ipb = iters_per_body(ss);
     int hdr[3] = {0, 0, max_iter / ipb + 4};   // err flag, body runs, cap
     MTLG_CUDA(cudaMemcpyAsync(ss.misc.p + 1, hdr, sizeof hdr, cudaMemcpyHostToDevice, c->stream));
+    if (c->loop_mode == 0) return run_loop_chunked<T>(ss, max_iter);
+    MTLG_TRY(build_graph<T>(ss));
     if (ss.exec) {
         MTLG_CUDA(cudaGraphLaunch(ss.exec, c->stream));
         int runs = 0;

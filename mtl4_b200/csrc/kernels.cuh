@@ -229,6 +229,10 @@ __device__ __forceinline__ bool skip_system(const SysState& s, int mode)
 // acc + a*x with the product rounded first (no contraction)
 __device__ __forceinline__ double mac(double acc, double a, double x) { return __dadd_rn(acc, __dmul_rn(a, x)); }
 __device__ __forceinline__ float mac(float acc, float a, float x) { return __fadd_rn(acc, __fmul_rn(a, x)); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 
 template <typename T, int XF>
 struct XIn {
@@ -342,7 +346,7 @@ __device__ __forceinline__ void stage_tile(const Tile& t, const int* rp, const i
 // warp from shared memory.  A long tile (one row with more than kTileNnz
 // entries) is summed by the whole CTA straight from global memory.
 template <typename T, int XF, int ASG>
-__global__ void __launch_bounds__(kBlock) k_spmv(SetView sv, SpmvOp op)
+__global__ void __launch_bounds__(kBlock, 3) k_spmv(SetView sv, SpmvOp op)
 {
     typedef StageLayout<T> SL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -507,6 +511,83 @@ __global__ void __launch_bounds__(kBlock) k_spmv(SetView sv, SpmvOp op)
         nxt = nn;
     }
     cp_async_wait_0();
+}
+
+// ---------------------------------------------------------------- SpMV, warp tasks
+// Row-aligned warp tasks for matrices with irregular row lengths.  A task is
+// either a run of consecutive rows with at most kWarpNnz entries in total
+// (and at most kWarpNnz rows), or one row with more entries.
+constexpr int kWarpNnz = 256;
+
+struct WarpTask {
+    int row_begin, row_end, nnz_begin, nnz_end;
+};
+
+// Run tasks: lanes load values and columns with coalesced loads and issue up
+// to 8 independent x gathers each; the rounded products go to shared memory
+// and every lane then sums whole rows from there, sequentially in storage
+// order (so each row's result is bitwise that of a sequential row sum).  No
+// CTA barrier: warps proceed independently.  Long-row tasks: the warp strides
+// over the row (8 gathers in flight per lane) and reduces with a fixed tree.
+template <typename T, int ASG>
+__global__ void __launch_bounds__(kBlock, 3)
+k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restrict__ rp, const int* __restrict__ ci,
+            const T* __restrict__ va, const T* __restrict__ x, T* __restrict__ y)
+{
+    __shared__ T s_prod[kBlock / 32][kWarpNnz];
+    __shared__ int s_rp[kBlock / 32][kWarpNnz + 1];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + wib, nwarps = gridDim.x * (blockDim.x >> 5);
+    T* prod = s_prod[wib];
+    int* srp = s_rp[wib];
+    for (int t = gw; t < ntasks; t += nwarps) {
+        const WarpTask task = tasks[t];
+        const int k0 = task.nnz_begin, k1 = task.nnz_end;
+        if (task.row_end - task.row_begin == 1 && k1 - k0 > kWarpNnz) {
+            T acc = T(0);
+            for (int kb = k0; kb < k1; kb += 32 * 8) {
+                T xv[8], av[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int k = kb + lane + 32 * u;
+                    if (k < k1) { av[u] = va[k]; xv[u] = x[ci[k]]; }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (kb + lane + 32 * u < k1) acc = mac(acc, av[u], xv[u]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) {
+                const int r = task.row_begin;
+                const T base = (ASG == ASG_SET) ? T(0) : y[r];
+                y[r] = assign_out<T, ASG>(base, acc);
+            }
+            continue;
+        }
+        T xv[8], av[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int k = k0 + lane + 32 * u;
+            if (k < k1) { av[u] = va[k]; xv[u] = x[ci[k]]; }
+        }
+        const int nr = task.row_end - task.row_begin;
+        for (int r = lane; r <= nr; r += 32) srp[r] = rp[task.row_begin + r] - k0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int k = k0 + lane + 32 * u;
+            if (k < k1) prod[lane + 32 * u] = mul_rn(av[u], xv[u]);
+        }
+        __syncwarp();
+        for (int r = lane; r < nr; r += 32) {
+            T acc = T(0);
+            for (int e = srp[r]; e < srp[r + 1]; ++e) acc = add_rn(acc, prod[e]);
+            const int row = task.row_begin + r;
+            const T base = (ASG == ASG_SET) ? T(0) : y[row];
+            y[row] = assign_out<T, ASG>(base, acc);
+        }
+        __syncwarp();
+    }
 }
 
 // ---------------------------------------------------------------- vector passes

@@ -4,6 +4,7 @@
 #include "host_solve.cuh"
 
 #include <map>
+#include <type_traits>
 
 using namespace mtlg;
 
@@ -184,6 +185,27 @@ int spmv_raw(mtlg_ctx* c, mtlg_csr* A, int dtype, const void* x, void* y, const 
 
 }  // namespace mtlg
 
+namespace mtlg {
+template <typename T>
+int launch_spmv_rows(mtlg_ctx* c, mtlg_csr* A, const void* x, void* y, int asg)
+{
+    if (A->wtasks.empty()) return MTLG_OK;
+    if (!A->d_wtasks.p) MTLG_TRY(A->d_wtasks.upload(c, A->wtasks.data(), A->wtasks.size()));
+    const int ntasks = int(A->wtasks.size());
+    const int grid = std::min((ntasks + 7) / 8, c->sm_count * 4);
+    const T* va = std::is_same<T, float>::value ? (const T*)A->v32.p : (const T*)A->v64.p;
+    switch (asg) {
+    case ASG_SET: k_spmv_rows<T, ASG_SET><<<grid, kBlock, 0, c->stream>>>(A->d_wtasks.p, ntasks, A->rp.p, A->ci.p, va, (const T*)x, (T*)y); break;
+    case ASG_ADD: k_spmv_rows<T, ASG_ADD><<<grid, kBlock, 0, c->stream>>>(A->d_wtasks.p, ntasks, A->rp.p, A->ci.p, va, (const T*)x, (T*)y); break;
+    default: k_spmv_rows<T, ASG_SUB><<<grid, kBlock, 0, c->stream>>>(A->d_wtasks.p, ntasks, A->rp.p, A->ci.p, va, (const T*)x, (T*)y); break;
+    }
+    c->launches++;
+    MTLG_CUDA(cudaGetLastError());
+    return MTLG_OK;
+}
+
+}  // namespace mtlg
+
 extern "C" int mtlg_pc_apply(mtlg_ctx* c, mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y);
 
 namespace mtlg {
@@ -297,6 +319,8 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     const std::string k(key);
     if (k == "sweep_blocks_per_sm") c->sweep_bpsm = int(std::max<int64_t>(0, value));
     else if (k == "sweep_blocks") c->sweep_nblocks = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 16)));
+    else if (k == "loop_mode") c->loop_mode = value ? 1 : 0;
+    else if (k == "spmv_kernel") c->spmv_kernel = int(std::max<int64_t>(0, std::min<int64_t>(value, 2)));
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
     else {
         set_error("unknown tuning key '%s'", key);
@@ -311,6 +335,8 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     const std::string k(key);
     if (k == "sweep_blocks_per_sm") *value = c->sweep_bpsm;
     else if (k == "sweep_blocks") *value = c->sweep_blocks();
+    else if (k == "loop_mode") *value = c->loop_mode;
+    else if (k == "spmv_kernel") *value = c->spmv_kernel;
     else if (k == "sweep_max_blocks_per_sm") *value = c->sweep_max_bpsm;
     else if (k == "sweep_sleep_ns") *value = c->sweep_sleep_ns;
     else if (k == "sm_count") *value = c->sm_count;
@@ -368,6 +394,8 @@ int mtlg_csr_create(mtlg_ctx* c, int64_t n_rows, int64_t n_cols, int64_t nnz, co
     rp32[n_rows] = int(nnz);
     plan_tiles(A->h_rp.data(), int(n_rows), 0, A->tiles);
     for (const Tile& t : A->tiles) A->tiles_by_kind[t.kind]++;
+    A->irregular = A->max_row > kShortRow;
+    plan_warp_tasks(A->h_rp.data(), int(n_rows), A->wtasks);
     MTLG_TRY(A->rp.upload(c, rp32.data(), rp32.size()));
     MTLG_TRY(A->ci.upload(c, col, size_t(nnz)));
     MTLG_TRY(A->dpos.upload(c, A->h_dpos.data(), std::max<size_t>(1, A->h_dpos.size())));
@@ -544,6 +572,11 @@ static int spmv_impl(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, i
         op.fin = FIN_STORE;
     }
     const int asg = assign == MTLG_ASSIGN ? ASG_SET : (assign == MTLG_PLUS ? ASG_ADD : ASG_SUB);
+    const bool warp = !pq && (c->spmv_kernel == 2 || (c->spmv_kernel == 0 && A->irregular));
+    if (warp) {
+        if (f32) return launch_spmv_rows<float>(c, A, x->p, y->p, asg);
+        return launch_spmv_rows<double>(c, A, x->p, y->p, asg);
+    }
     if (f32) MTLG_TRY(launch_spmv<float>(c, c->stream, sv, op, XF_PLAIN, asg));
     else MTLG_TRY(launch_spmv<double>(c, c->stream, sv, op, XF_PLAIN, asg));
     MTLG_CUDA(cudaGetLastError());
