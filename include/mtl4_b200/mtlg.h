@@ -129,7 +129,8 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * 0), "loop_mode" (0: the Krylov loop runs as chunks of 8 iterations in
  * plain CUDA graphs, two in flight; 1: one graph with a WHILE conditional
  * node per solve), "spmv_kernel" (standalone SpMV: 0 chooses by row
- * lengths, 1 shared-memory stream tiles, 2 row-aligned warp tasks).
+ * lengths, 1 shared-memory stream tiles, 2 row-aligned warp tasks, 3 one
+ * thread per row from global memory).
  * Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
 int mtlg_ctx_set_tuning(mtlg_ctx* ctx, const char* key, int64_t value);
 int mtlg_ctx_get_tuning(mtlg_ctx* ctx, const char* key, int64_t* value);

@@ -590,6 +590,35 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restric
     }
 }
 
+// Thread per row straight from global memory (rows of consecutive threads are
+// adjacent, so a warp's value and column loads stay in the sectors L1 just
+// fetched); gathers issued 8 at a time, summed in storage order.
+template <typename T, int ASG>
+__global__ void __launch_bounds__(kBlock)
+k_spmv_scalar(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ va,
+              const T* __restrict__ x, T* __restrict__ y)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int a = rp[i], e = rp[i + 1];
+        T acc = T(0);
+        int k = a;
+        for (; k + 8 <= e; k += 8) {
+            T xv[8], av[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) { av[u] = va[k + u]; xv[u] = x[ci[k + u]]; }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc = mac(acc, av[u], xv[u]);
+        }
+        T xv[8], av[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) if (k + u < e) { av[u] = va[k + u]; xv[u] = x[ci[k + u]]; }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) if (k + u < e) acc = mac(acc, av[u], xv[u]);
+        const T base = (ASG == ASG_SET) ? T(0) : y[i];
+        y[i] = assign_out<T, ASG>(base, acc);
+    }
+}
+
 // ---------------------------------------------------------------- vector passes
 enum VOp : int {
     VOP_DOT = 0,        // dots only

@@ -320,7 +320,7 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     if (k == "sweep_blocks_per_sm") c->sweep_bpsm = int(std::max<int64_t>(0, value));
     else if (k == "sweep_blocks") c->sweep_nblocks = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 16)));
     else if (k == "loop_mode") c->loop_mode = value ? 1 : 0;
-    else if (k == "spmv_kernel") c->spmv_kernel = int(std::max<int64_t>(0, std::min<int64_t>(value, 2)));
+    else if (k == "spmv_kernel") c->spmv_kernel = int(std::max<int64_t>(0, std::min<int64_t>(value, 3)));
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
     else {
         set_error("unknown tuning key '%s'", key);
@@ -572,6 +572,18 @@ static int spmv_impl(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, i
         op.fin = FIN_STORE;
     }
     const int asg = assign == MTLG_ASSIGN ? ASG_SET : (assign == MTLG_PLUS ? ASG_ADD : ASG_SUB);
+    if (!pq && c->spmv_kernel == 3) {
+        const int grid = int(std::min<int64_t>((A->n_rows + kBlock - 1) / kBlock, int64_t(c->sm_count) * 16));
+        if (A->n_rows == 0) return MTLG_OK;
+        const void* va = f32 ? (const void*)A->v32.p : (const void*)A->v64.p;
+#define MTLG_SCALAR(T, ASG) k_spmv_scalar<T, ASG><<<grid, kBlock, 0, c->stream>>>(int(A->n_rows), A->rp.p, A->ci.p, (const T*)va, (const T*)x->p, (T*)y->p)
+        if (f32) { if (asg == ASG_SET) MTLG_SCALAR(float, ASG_SET); else if (asg == ASG_ADD) MTLG_SCALAR(float, ASG_ADD); else MTLG_SCALAR(float, ASG_SUB); }
+        else { if (asg == ASG_SET) MTLG_SCALAR(double, ASG_SET); else if (asg == ASG_ADD) MTLG_SCALAR(double, ASG_ADD); else MTLG_SCALAR(double, ASG_SUB); }
+#undef MTLG_SCALAR
+        c->launches++;
+        MTLG_CUDA(cudaGetLastError());
+        return MTLG_OK;
+    }
     const bool warp = !pq && (c->spmv_kernel == 2 || (c->spmv_kernel == 0 && A->irregular));
     if (warp) {
         if (f32) return launch_spmv_rows<float>(c, A, x->p, y->p, asg);

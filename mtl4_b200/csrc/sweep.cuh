@@ -129,20 +129,9 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
         for (int j = 0; j < 8; ++j) {
             if (j < nr) { cc[j] = fc[a + j]; av[j] = fv[a + j]; }
         }
-        // All dependency values are requested at once (one L2 round trip
-        // when they are ready); only the ones still missing are polled again.
-        T wv[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            if (j < nr) wv[j] = ld_volatile(y + cc[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            if (j < nr && is_sentinel(wv[j])) wv[j] = wait_value(y + cc[j], sv.err, op.sleep_ns);
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            if (j < nr) rr = sweep_step<T, S>(rr, av[j], wv[j]);
+            if (j < nr) rr = sweep_step<T, S>(rr, av[j], wait_value(y + cc[j], sv.err, op.sleep_ns));
         }
         for (int j = a + 8; j < e; ++j) rr = sweep_step<T, S>(rr, fv[j], wait_value(y + fc[j], sv.err, op.sleep_ns));
         const S dia = static_cast<const S*>(F.dia)[k];
