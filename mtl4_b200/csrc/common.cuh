@@ -59,6 +59,7 @@ constexpr int kBlock = 256;
 constexpr int kSweepRows = 32;        // rows per sweep task (one warp, one row per lane)
 constexpr int kMaxDots = 4;           // dots a fused pass can reduce at once
 constexpr int kNumVec = 16;           // workspace vectors per system
+constexpr int kScalarMeanRow = 12;   // SpMV auto choice: thread per row up to this mean row length
 constexpr long long kSpinLimit = 1LL << 20;  // polls before a device wait gives up (~0.5 s)
 
 // Tile kinds of the SpMV / vector tiling.
@@ -80,6 +81,12 @@ struct SweepTask {
     int first;      // first level-ordered row of the task
 };
 
+// One segment of a chunked triangular factor: waves [w0, w0 + nw), positions
+// [p0, p0 + np), entries [e0, e0 + ne); w0, p0 and e0 are multiples of 4.
+struct __align__(16) SegRec {
+    int w0, nw, p0, np, e0, ne, pad0, pad1;
+};
+
 // Level-ordered triangular factor (device pointers).  Row k of the factor is
 // original row `row_of[k]` (-1 marks padding that aligns levels to warps);
 // its off-diagonal entries keep the reference's storage order and `dia[k]`
@@ -90,6 +97,36 @@ struct TriFactor {
     const void* val;   // T
     const void* dia;   // T
     const int* row_of;
+    // Chunked layout (k_sweep_chunk).  Chunk q holds rows [q*chunk_rows,
+    // (q+1)*chunk_rows); chunks are stored in processing order (ascending
+    // rows for L, descending for U).  A chunk's rows are grouped in waves of
+    // one dependency level (at most the launch's thread count rows each),
+    // consecutive waves in segments that one bulk copy per array stages in
+    // shared memory.  A wave's entries are column-major: entry k of its t-th
+    // row sits at k * rows + t after the wave's first entry (column -1 past
+    // the row's own entries).  Every segment starts 16-byte aligned in every
+    // array.
+    int chunk_rows;    // 0: no chunked layout
+    int nch;
+    int seg_rows;      // rows per segment, at most
+    int pad1;
+    const int* cseg;   // [nch + 1] segment range of each chunk
+    const SegRec* segs;          // [segments]
+    const unsigned* wv;// [waves] rows | entries per row << 16
+    const int* crow;   // row at each position
+    const int* ccol;   // entries' columns
+    const void* cval;  // entries' values (S)
+    const void* cdia;  // multiplier per position (S)
+};
+
+// A group of consecutive chunks of one system's triangular factor, by
+// processing position: chunks pos0 .. pos0 + count - 1, one per CTA of a
+// thread-block cluster.
+struct GroupTask {
+    int sys;
+    int pos0;
+    int count;
+    int pad;
 };
 
 // Workspace vector slots.

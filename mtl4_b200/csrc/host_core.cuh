@@ -14,6 +14,8 @@ struct mtlg_ctx {
     size_t in_use = 0;
     int64_t launches = 0;
     int sm_count = 148;
+    int max_threads_per_sm = 2048, regs_per_sm = 65536;
+    int smem_per_sm = 228 * 1024, smem_reserved_per_block = 1024;
     int sweep_grid = 148;       // persistent grid of the sweep / factor kernels
     int sweep_max_bpsm = 1;     // resident sweep CTAs per SM the device allows
     int sweep_bpsm = 0;         // tuning: sweep CTAs per SM (0: as many as fit)
@@ -21,6 +23,9 @@ struct mtlg_ctx {
     int sweep_nblocks = 0;      // tuning: absolute sweep grid (0: use sweep_bpsm)
     int loop_mode = 0;          // tuning: 0 chunked plain graphs, 1 WHILE conditional graph
     int spmv_kernel = 0;        // tuning: 0 auto (row-length statistics), 1 stream tiles, 2 warp tasks
+    int chunk_rows = 0;         // tuning: rows per sweep chunk of new preconditioners (0: by size)
+    int sweep_kernel = 0;       // tuning: 0 chunked waves, 1 flat level order
+    int sweep_cluster = 0;      // tuning: chunks per cluster of the chunked sweeps (0: 8, 1: no cluster)
     int* d_scratch_err = nullptr;
     int sweep_blocks() const
     {

@@ -24,7 +24,347 @@ struct TriDev {
     DBuf<int> row_of, rp, ci, src, mul;
     DBuf<unsigned char> val, dia;      // storage type S
     DBuf<SweepTask> tasks;             // single-system task list (sys = 0)
+    // chunked layout (k_sweep_chunk); nch == 0: not built (flat sweeps only)
+    int chunk_rows = 0, nch = 0, nseg = 0, nwaves = 0, cnpos = 0, cnent = 0;
+    int kmax = 0;       // entries per row, at most
+    int threads = 0;    // rows per wave, at most (the launch's CTA size)
+    int seg_rows = 0;   // rows per segment, at most
+    int seg_ents = 0;   // entries per segment, at most
+    DBuf<int> cseg, crow, ccol, csrc, cmul;
+    DBuf<SegRec> segs;
+    DBuf<unsigned> wv;
+    DBuf<unsigned char> cval, cdia;    // storage type S
 };
+
+constexpr int kChunkMaxEntries = 16;   // longer factor rows: flat sweeps only
+
+inline int round4(int v) { return (v + 3) & ~3; }
+inline int entries_bucket(int k) { return k <= 4 ? 4 : k <= 8 ? 8 : 16; }
+
+// Chunked layout of a triangular factor: chunks of B contiguous rows in
+// processing order; inside a chunk the rows are grouped by dependency level
+// (waves, split to at most `threads` rows), a wave's rows in the order of
+// the flat layout; consecutive waves form segments of at most seg_rows rows
+// and seg_ents entries; entries wave-major as described at TriFactor.
+inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& lev, int n, bool lower, int B,
+                        TriDev& T)
+{
+    T.nch = 0;
+    int kmax = 0;
+    for (int i = 0; i < n; ++i) kmax = std::max(kmax, F.rp[i + 1] - F.rp[i]);
+    if (n == 0 || B <= 0 || kmax > kChunkMaxEntries) return MTLG_OK;
+    B = std::max(32, (B + 31) / 32 * 32);
+    const int nch = (n + B - 1) / B;
+    // rows of each chunk sorted by (level, flat order) and the largest wave
+    std::vector<int> order;
+    order.reserve(n);
+    std::vector<int> cbeg(nch + 1, 0);
+    std::vector<std::pair<int, int>> key;
+    int maxw = 0;
+    for (int p = 0; p < nch; ++p) {
+        const int ch = lower ? p : nch - 1 - p;
+        const int r0 = ch * B, r1 = std::min(n, r0 + B);
+        key.clear();
+        for (int r = r0; r < r1; ++r) key.push_back({lev[r], lower ? r : -r});
+        std::sort(key.begin(), key.end());
+        int run = 0;
+        for (size_t q = 0; q < key.size(); ++q) {
+            run = (q > 0 && key[q].first == key[q - 1].first) ? run + 1 : 1;
+            maxw = std::max(maxw, run);
+            order.push_back(lower ? key[q].second : -key[q].second);
+        }
+        cbeg[p + 1] = int(order.size());
+    }
+    const int NT = std::min(256, std::max(32, (maxw + 31) / 32 * 32));
+    const int KB = entries_bucket(kmax);
+    const int SR = std::max(NT, 2048 / KB);
+    const int SE = SR * KB;
+    std::vector<int> cseg(1, 0), crow, ccol, csrc, cmul;
+    std::vector<unsigned> wv;
+    std::vector<SegRec> segs;
+    SegRec cur{};
+    bool open = false;
+    auto close_seg = [&]() {
+        if (!open) return;
+        cur.np = int(crow.size()) - cur.p0;
+        cur.ne = int(ccol.size()) - cur.e0;
+        cur.nw = int(wv.size()) - cur.w0;
+        segs.push_back(cur);
+        open = false;
+    };
+    auto open_seg = [&]() {
+        wv.resize(round4(int(wv.size())), 0u);
+        crow.resize(round4(int(crow.size())), -1);
+        const int e = round4(int(ccol.size()));
+        ccol.resize(e, -1);
+        csrc.resize(e, 0);
+        cmul.resize(e, -1);
+        cur = SegRec{int(wv.size()), 0, int(crow.size()), 0, int(ccol.size()), 0, 0, 0};
+        open = true;
+    };
+    for (int p = 0; p < nch; ++p) {
+        int q = cbeg[p];
+        while (q < cbeg[p + 1]) {
+            int qe = q + 1;
+            while (qe < cbeg[p + 1] && qe - q < NT && lev[order[qe]] == lev[order[q]]) ++qe;
+            const int nw = qe - q;
+            int K = 0;
+            for (int j = q; j < qe; ++j) K = std::max(K, F.rp[order[j] + 1] - F.rp[order[j]]);
+            if (open && (int(crow.size()) - cur.p0 + nw > SR || int(ccol.size()) - cur.e0 + K * nw > SE)) close_seg();
+            if (!open) open_seg();
+            wv.push_back(unsigned(nw) | (unsigned(K) << 16));
+            const size_t ent = ccol.size();
+            for (int j = q; j < qe; ++j) crow.push_back(order[j]);
+            ccol.resize(ent + size_t(K) * nw, -1);
+            csrc.resize(ent + size_t(K) * nw, 0);
+            cmul.resize(ent + size_t(K) * nw, -1);
+            for (int t = 0; t < nw; ++t) {
+                const int r = order[q + t];
+                for (int k = 0; k < F.rp[r + 1] - F.rp[r]; ++k) {
+                    const size_t e = ent + size_t(k) * nw + t;
+                    ccol[e] = F.col[F.rp[r] + k];
+                    csrc[e] = F.src[F.rp[r] + k];
+                    cmul[e] = F.mul[F.rp[r] + k];
+                }
+            }
+            q = qe;
+        }
+        close_seg();
+        cseg.push_back(int(segs.size()));
+    }
+    // tails: a staged copy rounds each array's segment up to 16 bytes
+    wv.resize(round4(int(wv.size())) + 4, 0u);
+    crow.resize(round4(int(crow.size())) + 4, -1);
+    const int e = round4(int(ccol.size())) + 4;
+    ccol.resize(e, -1);
+    csrc.resize(e, 0);
+    cmul.resize(e, -1);
+    T.chunk_rows = B;
+    T.nch = nch;
+    T.nseg = int(segs.size());
+    T.nwaves = int(wv.size());
+    T.cnpos = int(crow.size());
+    T.cnent = int(ccol.size());
+    T.kmax = kmax;
+    T.threads = NT;
+    T.seg_rows = SR;
+    T.seg_ents = SE;
+    MTLG_TRY(T.cseg.upload(c, cseg.data(), cseg.size()));
+    MTLG_TRY(T.segs.upload(c, segs.data(), segs.size()));
+    MTLG_TRY(T.wv.upload(c, wv.data(), wv.size()));
+    MTLG_TRY(T.crow.upload(c, crow.data(), crow.size()));
+    MTLG_TRY(T.ccol.upload(c, ccol.data(), ccol.size()));
+    MTLG_TRY(T.csrc.upload(c, csrc.data(), csrc.size()));
+    MTLG_TRY(T.cmul.upload(c, cmul.data(), cmul.size()));
+    return MTLG_OK;
+}
+
+// ------------------------------------------------------------ chunked sweeps
+constexpr int kChunkSmemMax = 225 * 1024;   // dynamic shared memory of one chunk CTA, at most
+
+// Launch plan of the chunked sweeps of a set of factors (computed outside
+// any stream capture: it queries the occupancy of clusters).
+struct ChunkPlan {
+    bool ok = false;
+    int nt = 0, km = 0;          // CTA size, entries per row
+    int rows = 0;                // rows of the largest chunk
+    int seg_rows = 0, seg_ents = 0;
+    int cluster = 1;             // CTAs per cluster (chunks per group)
+    int inbox = 0;               // predecessor results pushed into shared memory
+    int smem = 0;                // dynamic shared memory per CTA
+    int max_clusters = 1;        // clusters resident at once
+    int vec_bytes = 0;
+    DBuf<GroupTask> tl, tu;
+    int ntl = 0, ntu = 0;
+    void add(const TriDev& T)
+    {
+        nt = std::max(nt, T.threads);
+        km = std::max(km, T.kmax);
+        rows = std::max(rows, T.chunk_rows);
+        seg_rows = std::max(seg_rows, T.seg_rows);
+        seg_ents = std::max(seg_ents, T.seg_ents);
+    }
+    int threads() const { return nt <= 32 ? 32 : nt <= 64 ? 64 : nt <= 128 ? 128 : 256; }
+    int entries() const { return entries_bucket(km); }
+};
+
+template <typename T, typename S, int NT, int KM>
+struct ChunkShape {
+    static int init()
+    {
+        MTLG_CUDA(cudaFuncSetAttribute(k_sweep_chunk<T, S, NT, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kChunkSmemMax));
+        return MTLG_OK;
+    }
+    static cudaLaunchConfig_t config(dim3 grid, int smem, cudaStream_t st, cudaLaunchAttribute* attr, int cluster)
+    {
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof cfg);
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(NT, 1, 1);
+        cfg.dynamicSmemBytes = size_t(smem);
+        cfg.stream = st;
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = unsigned(cluster);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cfg;
+    }
+    // clusters of `cluster` CTAs resident at once (0: the shape does not fit)
+    static int max_clusters(int smem, int cluster)
+    {
+        cudaLaunchAttribute attr[1];
+        cudaLaunchConfig_t cfg = config(dim3(unsigned(cluster) * 64u, 1, 1), smem, nullptr, attr, cluster);
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_sweep_chunk<T, S, NT, KM>, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return n;
+    }
+    static int launch(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const ChunkSweepOp& op, const ChunkPlan& pl)
+    {
+        const int groups = std::max(1, std::min(op.ntasks, pl.max_clusters));
+        cudaLaunchAttribute attr[1];
+        cudaLaunchConfig_t cfg = config(dim3(unsigned(groups * pl.cluster), 1, 1), pl.smem, st, attr, pl.cluster);
+        MTLG_CUDA(cudaLaunchKernelEx(&cfg, k_sweep_chunk<T, S, NT, KM>, sv, op));
+        c->launches++;
+        return MTLG_OK;
+    }
+};
+
+#define MTLG_CHUNK_SHAPES(M, T, S) \
+    M(T, S, 32, 4) M(T, S, 32, 8) M(T, S, 32, 16) \
+    M(T, S, 64, 4) M(T, S, 64, 8) M(T, S, 64, 16) \
+    M(T, S, 128, 4) M(T, S, 128, 8) M(T, S, 128, 16) \
+    M(T, S, 256, 4) M(T, S, 256, 8) M(T, S, 256, 16)
+
+inline int init_chunk_shapes()
+{
+#define MTLG_CHUNK_INIT(T, S, NT, KM) MTLG_TRY((ChunkShape<T, S, NT, KM>::init()));
+    MTLG_CHUNK_SHAPES(MTLG_CHUNK_INIT, double, double)
+    MTLG_CHUNK_SHAPES(MTLG_CHUNK_INIT, double, float)
+    MTLG_CHUNK_SHAPES(MTLG_CHUNK_INIT, float, float)
+    MTLG_CHUNK_SHAPES(MTLG_CHUNK_INIT, float, double)
+#undef MTLG_CHUNK_INIT
+    return MTLG_OK;
+}
+
+template <typename T, typename S>
+inline int chunk_max_clusters(const ChunkPlan& pl, int smem, int cluster)
+{
+    const int nt = pl.threads(), km = pl.entries();
+#define MTLG_CHUNK_Q(TT, SS, NT, KM) \
+    if (nt == NT && km == KM) return ChunkShape<TT, SS, NT, KM>::max_clusters(smem, cluster);
+    MTLG_CHUNK_SHAPES(MTLG_CHUNK_Q, T, S)
+#undef MTLG_CHUNK_Q
+    return 0;
+}
+
+// Shape, cluster size and group lists of a set of systems' factors (pcs[s]:
+// the system's factors or null for an unused slot).  Groups of up to
+// `cluster` consecutive chunks of one system, interleaved across systems.
+template <typename T, typename S>
+inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, const TriDev*>>& f, ChunkPlan& pl)
+{
+    pl.ok = false;
+    pl.nt = pl.km = pl.rows = pl.seg_rows = pl.seg_ents = 0;
+    pl.ntl = pl.ntu = 0;
+    bool any = false;
+    for (const auto& lu : f) {
+        if (!lu.first) continue;
+        any = true;
+        if (lu.first->nch == 0 || lu.second->nch == 0 || !lu.first->cval.p || !lu.second->cval.p) return MTLG_OK;
+        pl.add(*lu.first);
+        pl.add(*lu.second);
+    }
+    if (!any || c->sweep_kernel != 0) return MTLG_OK;
+    pl.vec_bytes = int((size_t(pl.rows) * sizeof(T) + 15) / 16 * 16);
+    const int stage = kStageBufs * stage_bytes<S>(pl.seg_rows, pl.seg_ents);
+    // largest cluster (8, 4, 2) whose CTAs fit with the inbox; else no cluster
+    pl.cluster = 1;
+    pl.inbox = 0;
+    pl.smem = pl.vec_bytes + stage;
+    if (pl.smem > kChunkSmemMax) return MTLG_OK;
+    const int want = c->sweep_cluster > 0 ? c->sweep_cluster : 8;
+    if (2 * pl.vec_bytes + stage <= kChunkSmemMax) {
+        for (int cl = want; cl >= 2; cl /= 2) {
+            const int n = chunk_max_clusters<T, S>(pl, 2 * pl.vec_bytes + stage, cl);
+            if (n >= 1) {
+                pl.cluster = cl;
+                pl.inbox = 1;
+                pl.smem = 2 * pl.vec_bytes + stage;
+                pl.max_clusters = n;
+                break;
+            }
+        }
+    }
+    if (pl.cluster == 1) {
+        pl.max_clusters = std::max(1, chunk_max_clusters<T, S>(pl, pl.smem, 1));
+    }
+    std::vector<GroupTask> tl, tu;
+    int maxch = 0;
+    for (const auto& lu : f)
+        if (lu.first) maxch = std::max({maxch, lu.first->nch, lu.second->nch});
+    for (int p0 = 0; p0 < maxch; p0 += pl.cluster) {
+        for (size_t s = 0; s < f.size(); ++s) {
+            if (!f[s].first) continue;
+            const int nl = f[s].first->nch, nu = f[s].second->nch;
+            if (p0 < nl) tl.push_back({int(s), p0, std::min(pl.cluster, nl - p0), 0});
+            if (p0 < nu) tu.push_back({int(s), p0, std::min(pl.cluster, nu - p0), 0});
+        }
+    }
+    pl.ntl = int(tl.size());
+    pl.ntu = int(tu.size());
+    MTLG_TRY(pl.tl.upload(c, tl.data(), std::max<size_t>(1, tl.size())));
+    MTLG_TRY(pl.tu.upload(c, tu.data(), std::max<size_t>(1, tu.size())));
+    pl.ok = true;
+    return MTLG_OK;
+}
+
+template <typename T, typename S>
+inline int launch_chunk_sweep(mtlg_ctx* c, cudaStream_t st, const SetView& sv, ChunkSweepOp op, const ChunkPlan& pl)
+{
+    if (op.ntasks == 0) return MTLG_OK;
+    op.vec_bytes = pl.vec_bytes;
+    op.rows_cap = pl.seg_rows;
+    op.ents_cap = pl.seg_ents;
+    op.inbox = pl.inbox;
+    const int nt = pl.threads(), km = pl.entries();
+#define MTLG_CHUNK_CASE(TT, SS, NT, KM) \
+    if (nt == NT && km == KM) return ChunkShape<TT, SS, NT, KM>::launch(c, st, sv, op, pl);
+    MTLG_CHUNK_SHAPES(MTLG_CHUNK_CASE, T, S)
+#undef MTLG_CHUNK_CASE
+    set_error("chunk sweep shape %d/%d", nt, km);
+    return MTLG_ERR_NOT_SUPPORTED;
+}
+
+// Device view of a factor (both layouts).
+inline TriFactor tri_view(const TriDev& T)
+{
+    TriFactor f;
+    memset(&f, 0, sizeof f);
+    f.rp = T.rp.p;
+    f.ci = T.ci.p;
+    f.val = T.val.p;
+    f.dia = T.dia.p;
+    f.row_of = T.row_of.p;
+    if (T.nch > 0 && T.cval.p && T.cdia.p) {
+        f.chunk_rows = T.chunk_rows;
+        f.nch = T.nch;
+        f.seg_rows = T.seg_rows;
+        f.cseg = T.cseg.p;
+        f.segs = T.segs.p;
+        f.wv = T.wv.p;
+        f.crow = T.crow.p;
+        f.ccol = T.ccol.p;
+        f.cval = T.cval.p;
+        f.cdia = T.cdia.p;
+    }
+    return f;
+}
 
 inline void compute_levels(const RowLists& F, int n, bool lower, std::vector<int>& lev, int& nlev)
 {
@@ -48,7 +388,15 @@ inline void compute_levels(const RowLists& F, int n, bool lower, std::vector<int
     nlev = mx + 1;
 }
 
-inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& T)
+// Rows per sweep chunk: 64 KB of vector values per CTA (8192 FP64 or 16384
+// FP32 rows), or the context's setting.
+inline int default_chunk_rows(const mtlg_ctx* c, int storage)
+{
+    if (c->chunk_rows > 0) return c->chunk_rows;
+    return storage == MTLG_F32 ? 16384 : 8192;
+}
+
+inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& T, int chunk_rows)
 {
     T.n = n;
     T.lower = lower;
@@ -100,7 +448,7 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
     MTLG_TRY(T.src.upload(c, T.h_src.data(), T.h_src.size()));
     MTLG_TRY(T.mul.upload(c, T.h_mul.data(), T.h_mul.size()));
     MTLG_TRY(T.tasks.upload(c, tasks.data(), tasks.size()));
-    return MTLG_OK;
+    return build_chunks(c, F, lev, n, lower, chunk_rows, T);
 }
 
 }  // namespace mtlg
@@ -119,6 +467,8 @@ struct mtlg_pc {
     DBuf<SysDesc> desc;
     DBuf<SysState> st;
     DBuf<int> misc;
+    ChunkPlan plan[2];              // chunked sweeps with FP64 [0] / FP32 [1] vectors
+    int plan_kernel[2] = {-1, -1};  // context's sweep_kernel / cluster setting the plan was made for
     RowLists lt;                    // IC(0): transposed upper pattern (natural order)
     DBuf<int> lt_rp, lt_row, lt_src;
     bool has_factors() const { return kind == MTLG_PC_ILU0 || kind == MTLG_PC_IC0; }
@@ -153,6 +503,28 @@ inline int pc_setup_single_set(mtlg_pc* P)
 
 inline int launch_grid(int64_t n, int maxg = 8192) { return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, maxg))); }
 
+// Values of the chunked layout: entries from `srcvals` (times the inverse
+// pivot named by cmul), multipliers from inv_dia (1 for a unit diagonal).
+inline int fill_chunk_values(mtlg_pc* P, TriDev& T, const double* srcvals, const double* inv_dia, int unit)
+{
+    mtlg_ctx* c = P->ctx;
+    if (T.nch == 0) return MTLG_OK;
+    const int f32 = P->storage == MTLG_F32;
+    MTLG_TRY(T.cval.alloc(c, size_t(std::max(T.cnent, 4)) * P->ssize()));
+    MTLG_TRY(T.cdia.alloc(c, size_t(std::max(T.cnpos, 4)) * P->ssize()));
+    if (T.cnent) {
+        k_fill_factor<<<launch_grid(T.cnent), 256, 0, c->stream>>>(T.cnent, T.csrc.p, T.cmul.p, srcvals, inv_dia,
+                                                                   T.cval.p, f32);
+        c->launches++;
+    }
+    if (T.cnpos) {
+        k_fill_dia<<<launch_grid(T.cnpos), 256, 0, c->stream>>>(T.cnpos, T.crow.p, inv_dia, unit, T.cdia.p, f32);
+        c->launches++;
+    }
+    MTLG_CUDA(cudaGetLastError());
+    return MTLG_OK;
+}
+
 // Structure + device factorization.
 inline int pc_build(mtlg_pc* P)
 {
@@ -172,8 +544,9 @@ inline int pc_build(mtlg_pc* P)
         // L: no entries, dia = 1/a_ii; U: no entries, dia = 1.
         RowLists E;
         E.rp.assign(n + 1, 0);
-        MTLG_TRY(build_tri(c, E, n, true, P->L));
-        MTLG_TRY(build_tri(c, E, n, false, P->U));
+        const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
+        MTLG_TRY(build_tri(c, E, n, true, P->L, B));
+        MTLG_TRY(build_tri(c, E, n, false, P->U, B));
         MTLG_TRY(P->L.val.alloc(c, 16));
         MTLG_TRY(P->U.val.alloc(c, 16));
         MTLG_TRY(P->L.dia.alloc(c, size_t(P->L.npad) * P->ssize()));
@@ -189,6 +562,7 @@ inline int pc_build(mtlg_pc* P)
             c->launches += 3;
             MTLG_CUDA(cudaGetLastError());
         }
+        for (TriDev* T : {&P->L, &P->U}) MTLG_TRY(fill_chunk_values(P, *T, P->inv_dia.p, P->inv_dia.p, T == &P->U));
         return pc_setup_single_set(P);
     }
     if (!P->has_factors()) return pc_setup_single_set(P);
@@ -240,8 +614,9 @@ inline int pc_build(mtlg_pc* P)
         MTLG_TRY(P->lt_row.upload(c, Lr.col.data(), std::max<size_t>(1, Lr.col.size())));
         MTLG_TRY(P->lt_src.upload(c, Lr.src.data(), std::max<size_t>(1, Lr.src.size())));
     }
-    MTLG_TRY(build_tri(c, Lr, n, true, P->L));
-    MTLG_TRY(build_tri(c, Ur, n, false, P->U));
+    const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
+    MTLG_TRY(build_tri(c, Lr, n, true, P->L, B));
+    MTLG_TRY(build_tri(c, Ur, n, false, P->U, B));
     MTLG_TRY(pc_setup_single_set(P));
 
     // ---- numeric factorization on the device (FP64)
@@ -295,6 +670,7 @@ inline int pc_build(mtlg_pc* P)
             c->launches++;
         }
         MTLG_CUDA(cudaGetLastError());
+        MTLG_TRY(fill_chunk_values(P, *T, srcvals, P->inv_dia.p, unit));
     }
     int err = 0;
     MTLG_CUDA(cudaMemcpyAsync(&err, P->misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

@@ -159,8 +159,8 @@ inline int srv_admit(mtlg_server* S, mtlg_server::Req& R, int e, int slot)
     d.ws_stride = stride;
     d.pc = R.P->kind;
     if (R.P->kind == MTLG_PC_DIAGONAL) d.inv_diag = R.P->inv_diag.p;
-    d.L = TriFactor{R.P->L.rp.p, R.P->L.ci.p, R.P->L.val.p, R.P->L.dia.p, R.P->L.row_of.p};
-    d.U = TriFactor{R.P->U.rp.p, R.P->U.ci.p, R.P->U.val.p, R.P->U.dia.p, R.P->U.row_of.p};
+    d.L = tri_view(R.P->L);
+    d.U = tri_view(R.P->U);
     if (S->refine) {
         d.x = R.ws.p + size_t(V_W1) * stride * vb;
         d.b = R.ws.p + size_t(V_W0) * stride * vb;
@@ -247,6 +247,12 @@ inline int srv_rebuild(mtlg_server* S, int e)
     ss.ntu = int(tu.size());
     MTLG_TRY(ss.tl.upload(c, tl.data(), std::max<size_t>(1, tl.size())));
     MTLG_TRY(ss.tu.upload(c, tu.data(), std::max<size_t>(1, tu.size())));
+    {
+        std::vector<const mtlg_pc*> pcs(ss.S, nullptr);
+        for (int s = 0; s < ss.S; ++s)
+            if (E.slot_req[s] >= 0) pcs[s] = S->reqs[E.slot_req[s]]->P;
+        MTLG_TRY(plan_set_chunks(ss, pcs));
+    }
     MTLG_CUDA(cudaMemcpyAsync(ss.desc.p, ss.h_desc.data(), sizeof(SysDesc) * ss.S, cudaMemcpyHostToDevice, c->stream));
     MTLG_CUDA(cudaMemcpyAsync(ss.desc64.p, ss.h_desc64.data(), sizeof(SysDesc) * ss.S, cudaMemcpyHostToDevice,
                               c->stream));

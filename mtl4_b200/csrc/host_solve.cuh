@@ -39,6 +39,8 @@ struct SolveSet {
     DBuf<int> misc;       // [0] running, [1] timeout flag, [2] body runs, [3] body cap
     DBuf<SweepTask> tl, tu;
     int ntl = 0, ntu = 0;
+    // chunked sweeps: groups of chunks of all systems
+    ChunkPlan cplan;
     DBuf<int> tickets;
     DBuf<unsigned char> ws, ws64;
     long long stride = 0;
@@ -85,6 +87,8 @@ struct SolveSet {
         return v;
     }
 };
+
+inline int plan_set_chunks(SolveSet& ss, const std::vector<const mtlg_pc*>& pcs);
 
 inline size_t vsize(int f32) { return f32 ? 4 : 8; }
 
@@ -162,8 +166,8 @@ inline int build_set(mtlg_ctx* c, SolveSet& ss)
         d.pc = si.P ? si.P->kind : MTLG_PC_IDENTITY;
         if (si.P && si.P->kind == MTLG_PC_DIAGONAL) d.inv_diag = si.P->inv_diag.p;
         if (si.P && (si.P->kind == MTLG_PC_DIAGONAL || si.P->has_factors())) {
-            d.L = TriFactor{si.P->L.rp.p, si.P->L.ci.p, si.P->L.val.p, si.P->L.dia.p, si.P->L.row_of.p};
-            d.U = TriFactor{si.P->U.rp.p, si.P->U.ci.p, si.P->U.val.p, si.P->U.dia.p, si.P->U.row_of.p};
+            d.L = tri_view(si.P->L);
+            d.U = tri_view(si.P->U);
         }
         if (ss.mixed) {
             // inner problem: x = d (slot V_W1), b = float(r / ||r||) (slot V_W0)
@@ -213,14 +217,48 @@ inline int build_set(mtlg_ctx* c, SolveSet& ss)
         ss.ntu = int(tu.size());
         MTLG_TRY(ss.tl.upload(c, tl.data(), std::max<size_t>(1, tl.size())));
         MTLG_TRY(ss.tu.upload(c, tu.data(), std::max<size_t>(1, tu.size())));
+        std::vector<const mtlg_pc*> pcs(ss.S);
+        for (int s = 0; s < ss.S; ++s) pcs[s] = ss.in[s].P;
+        MTLG_TRY(plan_set_chunks(ss, pcs));
     }
     return MTLG_OK;
+}
+
+// Chunked-sweep plan of the systems with a preconditioner (pcs[s] ==
+// nullptr: slot unused); the set runs chunked sweeps only if every one of
+// them has the chunked layout.
+inline int plan_set_chunks(SolveSet& ss, const std::vector<const mtlg_pc*>& pcs)
+{
+    std::vector<std::pair<const TriDev*, const TriDev*>> f(pcs.size(), {nullptr, nullptr});
+    for (size_t s = 0; s < pcs.size(); ++s)
+        if (pcs[s]) f[s] = {&pcs[s]->L, &pcs[s]->U};
+    if (ss.f32) {
+        if (ss.pc_f32) return plan_chunks<float, float>(ss.ctx, f, ss.cplan);
+        return plan_chunks<float, double>(ss.ctx, f, ss.cplan);
+    }
+    if (ss.pc_f32) return plan_chunks<double, float>(ss.ctx, f, ss.cplan);
+    return plan_chunks<double, double>(ss.ctx, f, ss.cplan);
 }
 
 template <typename T>
 inline int launch_sweep(SolveSet& ss, cudaStream_t st, const SetView& sv, int which, int in, int out, int reset,
                         int skip, int ticket)
 {
+    if (ss.cplan.ok && ss.ctx->sweep_kernel == 0) {
+        ChunkSweepOp op;
+        memset(&op, 0, sizeof op);
+        op.tasks = which == 0 ? ss.cplan.tl.p : ss.cplan.tu.p;
+        op.ntasks = which == 0 ? ss.cplan.ntl : ss.cplan.ntu;
+        op.ticket = ss.tickets.p + 4 + ticket;
+        op.which = which;
+        op.in = in;
+        op.out = out;
+        op.reset = reset;
+        op.skip = skip;
+        op.sleep_ns = ss.ctx->sweep_sleep_ns;
+        if (ss.pc_f32) return launch_chunk_sweep<T, float>(ss.ctx, st, sv, op, ss.cplan);
+        return launch_chunk_sweep<T, double>(ss.ctx, st, sv, op, ss.cplan);
+    }
     SweepOp op;
     memset(&op, 0, sizeof op);
     op.tasks = which == 0 ? ss.tl.p : ss.tu.p;

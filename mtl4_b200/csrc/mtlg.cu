@@ -122,23 +122,44 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
     d.b = y->p;
     d.ws = P->tmp.p;
     d.ws_stride = 0;
-    d.L = TriFactor{P->L.rp.p, P->L.ci.p, P->L.val.p, P->L.dia.p, P->L.row_of.p};
-    d.U = TriFactor{P->U.rp.p, P->U.ci.p, P->U.val.p, P->U.dia.p, P->U.row_of.p};
+    d.L = tri_view(P->L);
+    d.U = tri_view(P->U);
     MTLG_CUDA(cudaMemcpyAsync(P->desc.p, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
-    SweepOp op;
-    memset(&op, 0, sizeof op);
-    op.skip = SKIP_NONE;
-    op.fuse = SWF_NONE;
-    op.sleep_ns = c->sweep_sleep_ns;
-    const int grid = c->sweep_blocks();
-    // y0 = L^{-1} x  (temp, slot 0); clears y row by row
-    op.tasks = P->L.tasks.p; op.ntasks = int(P->L.tasks.n); op.ticket = P->tickets.p + 0; op.which = 0;
-    op.in = SLOT_X; op.out = 0; op.reset = SLOT_B;
-    if (op.ntasks) { k_sweep<T, S><<<grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
-    // y = U^{-1} y0; clears the temp again
-    op.tasks = P->U.tasks.p; op.ntasks = int(P->U.tasks.n); op.ticket = P->tickets.p + 1; op.which = 1;
-    op.in = 0; op.out = SLOT_B; op.reset = 0;
-    if (op.ntasks) { k_sweep<T, S><<<grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
+    ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
+    int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
+    const int setting = c->sweep_kernel * 64 + c->sweep_cluster;
+    if (made != setting) {
+        std::vector<std::pair<const TriDev*, const TriDev*>> f(1, {&P->L, &P->U});
+        MTLG_TRY((plan_chunks<T, S>(c, f, pl)));
+        made = setting;
+    }
+    if (pl.ok) {
+        ChunkSweepOp op;
+        memset(&op, 0, sizeof op);
+        op.skip = SKIP_NONE;
+        op.sleep_ns = c->sweep_sleep_ns;
+        // y0 = L^{-1} x  (temp, slot 0); clears y row by row
+        op.tasks = pl.tl.p; op.ntasks = pl.ntl; op.ticket = P->tickets.p + 2; op.which = 0;
+        op.in = SLOT_X; op.out = 0; op.reset = SLOT_B;
+        MTLG_TRY((launch_chunk_sweep<T, S>(c, c->stream, sv, op, pl)));
+        // y = U^{-1} y0; clears the temp again
+        op.tasks = pl.tu.p; op.ntasks = pl.ntu; op.ticket = P->tickets.p + 3; op.which = 1;
+        op.in = 0; op.out = SLOT_B; op.reset = 0;
+        MTLG_TRY((launch_chunk_sweep<T, S>(c, c->stream, sv, op, pl)));
+    } else {
+        SweepOp op;
+        memset(&op, 0, sizeof op);
+        op.skip = SKIP_NONE;
+        op.fuse = SWF_NONE;
+        op.sleep_ns = c->sweep_sleep_ns;
+        const int grid = c->sweep_blocks();
+        op.tasks = P->L.tasks.p; op.ntasks = int(P->L.tasks.n); op.ticket = P->tickets.p + 0; op.which = 0;
+        op.in = SLOT_X; op.out = 0; op.reset = SLOT_B;
+        if (op.ntasks) { k_sweep<T, S><<<grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
+        op.tasks = P->U.tasks.p; op.ntasks = int(P->U.tasks.n); op.ticket = P->tickets.p + 1; op.which = 1;
+        op.in = 0; op.out = SLOT_B; op.reset = 0;
+        if (op.ntasks) { k_sweep<T, S><<<grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
+    }
     MTLG_CUDA(cudaGetLastError());
     int err = 0;
     MTLG_CUDA(cudaMemcpyAsync(&err, P->misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -267,12 +288,17 @@ int mtlg_ctx_create(int device, size_t hbm_budget, mtlg_ctx** out)
     MTLG_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
     c->stream = c->own_stream;
     MTLG_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    MTLG_CUDA(cudaDeviceGetAttribute(&c->max_threads_per_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device));
+    MTLG_CUDA(cudaDeviceGetAttribute(&c->regs_per_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device));
+    MTLG_CUDA(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
+    MTLG_CUDA(cudaDeviceGetAttribute(&c->smem_reserved_per_block, cudaDevAttrReservedSharedMemoryPerBlock, device));
     int nb = 1, nb2 = 1;
     MTLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_sweep<double, double>, kBlock, 0));
     MTLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_ilu0_factor, kBlock, 0));
     c->sweep_max_bpsm = std::max(1, std::min(nb, nb2));
     c->sweep_grid = c->sm_count * c->sweep_max_bpsm;
     MTLG_TRY(init_kernel_shapes());
+    MTLG_TRY(init_chunk_shapes());
     *out = c.release();
     return MTLG_OK;
 }
@@ -322,6 +348,9 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "loop_mode") c->loop_mode = value ? 1 : 0;
     else if (k == "spmv_kernel") c->spmv_kernel = int(std::max<int64_t>(0, std::min<int64_t>(value, 3)));
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
+    else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
+    else if (k == "sweep_cluster") c->sweep_cluster = int(std::max<int64_t>(0, std::min<int64_t>(value, 8)));
+    else if (k == "chunk_rows") c->chunk_rows = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 15)));
     else {
         set_error("unknown tuning key '%s'", key);
         return MTLG_ERR_INVALID_ARG;
@@ -340,6 +369,9 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     else if (k == "sweep_max_blocks_per_sm") *value = c->sweep_max_bpsm;
     else if (k == "sweep_sleep_ns") *value = c->sweep_sleep_ns;
     else if (k == "sm_count") *value = c->sm_count;
+    else if (k == "sweep_kernel") *value = c->sweep_kernel;
+    else if (k == "sweep_cluster") *value = c->sweep_cluster;
+    else if (k == "chunk_rows") *value = c->chunk_rows;
     else {
         set_error("unknown tuning key '%s'", key);
         return MTLG_ERR_INVALID_ARG;
@@ -572,7 +604,12 @@ static int spmv_impl(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, i
         op.fin = FIN_STORE;
     }
     const int asg = assign == MTLG_ASSIGN ? ASG_SET : (assign == MTLG_PLUS ? ASG_ADD : ASG_SUB);
-    if (!pq && c->spmv_kernel == 3) {
+    // auto: thread per row for short regular rows, warp tasks for irregular
+    // row lengths, stream tiles otherwise
+    const int kern = c->spmv_kernel != 0 ? c->spmv_kernel
+                     : A->irregular ? 2
+                     : (A->n_rows > 0 && A->nnz <= int64_t(kScalarMeanRow) * A->n_rows) ? 3 : 1;
+    if (!pq && kern == 3) {
         const int grid = int(std::min<int64_t>((A->n_rows + kBlock - 1) / kBlock, int64_t(c->sm_count) * 16));
         if (A->n_rows == 0) return MTLG_OK;
         const void* va = f32 ? (const void*)A->v32.p : (const void*)A->v64.p;
@@ -584,7 +621,7 @@ static int spmv_impl(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, i
         MTLG_CUDA(cudaGetLastError());
         return MTLG_OK;
     }
-    const bool warp = !pq && (c->spmv_kernel == 2 || (c->spmv_kernel == 0 && A->irregular));
+    const bool warp = !pq && kern == 2;
     if (warp) {
         if (f32) return launch_spmv_rows<float>(c, A, x->p, y->p, asg);
         return launch_spmv_rows<double>(c, A, x->p, y->p, asg);
@@ -765,6 +802,45 @@ int mtlg_pc_levels(const mtlg_pc* P, int* levels_L, int* levels_U)
     if (levels_L) *levels_L = P->L.nlev;
     if (levels_U) *levels_U = P->U.nlev;
     return MTLG_OK;
+}
+
+extern "C++" {
+template <typename T, typename S>
+static int sweep_plan_of(mtlg_ctx* c, mtlg_pc* P, int32_t* out)
+{
+    ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
+    int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
+    const int setting = c->sweep_kernel * 64 + c->sweep_cluster;
+    if (made != setting) {
+        std::vector<std::pair<const TriDev*, const TriDev*>> f(1, {&P->L, &P->U});
+        MTLG_TRY((plan_chunks<T, S>(c, f, pl)));
+        made = setting;
+    }
+    for (int i = 0; i < 8; ++i) out[i] = 0;
+    if (!pl.ok) return MTLG_OK;
+    out[0] = pl.rows;
+    out[1] = P->L.nch;
+    out[2] = pl.cluster;
+    out[3] = pl.max_clusters;
+    out[4] = pl.smem;
+    out[5] = pl.threads();
+    out[6] = pl.entries();
+    out[7] = pl.inbox;
+    return MTLG_OK;
+}
+}
+
+int mtlg_pc_sweep_plan(mtlg_ctx* c, mtlg_pc* P, int dtype, int32_t* out8)
+{
+    MTLG_CHECK_ARG(c && P && out8, "null handle");
+    MTLG_CHECK_ARG(ok_dtype(dtype), "dtype");
+    for (int i = 0; i < 8; ++i) out8[i] = 0;
+    if (!P->has_factors() && P->kind != MTLG_PC_DIAGONAL) return MTLG_OK;
+    const bool t32 = dtype == MTLG_F32, s32 = P->storage == MTLG_F32;
+    if (t32 && !s32) return sweep_plan_of<float, double>(c, P, out8);
+    if (t32 && s32) return sweep_plan_of<float, float>(c, P, out8);
+    if (!t32 && s32) return sweep_plan_of<double, float>(c, P, out8);
+    return sweep_plan_of<double, double>(c, P, out8);
 }
 
 // ------------------------------------------------------------------ solves

@@ -146,6 +146,403 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
     }
 }
 
+// ------------------------------------------------------------ chunked sweep
+// One CTA per chunk of contiguous rows (TriFactor's chunked layout), taken
+// in processing order through one ticket.  The chunk's inputs are loaded
+// into shared memory, then its waves run one after the other: a row reads
+// the rows of its own chunk from shared memory (finished in earlier waves,
+// made visible by the barrier between waves) and polls only rows of earlier
+// chunks in global memory.  Every result is also published to global memory
+// with a relaxed store for later chunks.  Chunks depend on earlier chunks
+// only and waves on earlier waves, and a chunk is held by a running CTA, so
+// the waits end; they are bounded all the same (wait_value).
+//
+// The chunk's structure (wave sizes, rows, multipliers, entries) streams
+// through kStageBufs shared-memory buffers, one segment of waves per buffer,
+// each segment brought in by one bulk copy per array (TMA, completion on an
+// mbarrier) issued kStageBufs - 1 segments ahead of its use, so a wave's
+// critical path is shared-memory reads, the arithmetic and the barrier.  The
+// arithmetic per row is k_sweep's (same entry order, same roundings).
+constexpr int kStageBufs = 3;
+
+struct ChunkSweepOp {
+    const GroupTask* tasks;
+    int ntasks;
+    int* ticket;        // zero before the launch; returned to zero by the last grab
+    int which;          // 0: L, 1: U
+    int in, out, reset; // vector slots (reset: SLOT_NONE or cleared to the sentinel)
+    int skip;
+    int sleep_ns;
+    int vec_bytes;      // shared vector: rows of the largest chunk x sizeof(T), 16-byte multiple
+    int rows_cap;       // staging buffer capacity in rows (multiple of 4)
+    int ents_cap;       // ... and in entries (multiple of 4)
+    int inbox;          // 1: a second shared vector receives the predecessor chunk's results
+};
+
+// Staging buffer layout: [wave sizes: rows_cap u32][rows: rows_cap int]
+// [multipliers: rows_cap S][columns: ents_cap int][values: ents_cap S].
+template <typename S>
+__host__ __device__ __forceinline__ int stage_bytes(int rows_cap, int ents_cap)
+{
+    return rows_cap * (8 + int(sizeof(S))) + ents_cap * (4 + int(sizeof(S)));
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return unsigned(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for a staged segment: after kSpinLimit polls it records a
+// timeout and keeps waiting up to the same bound again for the copy itself.
+__device__ __forceinline__ void mbar_wait(unsigned long long* bar, unsigned parity, int* err)
+{
+    long long spins = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++spins == kSpinLimit) atomicExch(err, 1);
+        if (spins > 2 * kSpinLimit) return;
+    }
+}
+
+// Global -> shared bulk copy (16-byte aligned addresses, 16-byte multiple size).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ unsigned round16u(unsigned v) { return (v + 15u) & ~15u; }
+
+// Issues the copies of segment `sg` into staging buffer `buf` (one thread).
+template <typename S>
+__device__ __forceinline__ void stage_segment(const TriFactor& F, const SegRec& sg, unsigned char* buf, int rows_cap,
+                                              int ents_cap, unsigned long long* bar)
+{
+    const unsigned bw = round16u(unsigned(sg.nw) * 4u), br = round16u(unsigned(sg.np) * 4u);
+    const unsigned bd = round16u(unsigned(sg.np) * unsigned(sizeof(S)));
+    const unsigned bc = round16u(unsigned(sg.ne) * 4u), bv = round16u(unsigned(sg.ne) * unsigned(sizeof(S)));
+    mbar_expect_tx(bar, bw + br + bd + bc + bv);
+    unsigned char* o = buf;
+    bulk_g2s(o, F.wv + sg.w0, bw, bar);
+    o += rows_cap * 4;
+    bulk_g2s(o, F.crow + sg.p0, br, bar);
+    o += rows_cap * 4;
+    bulk_g2s(o, static_cast<const S*>(F.cdia) + sg.p0, bd, bar);
+    o += rows_cap * int(sizeof(S));
+    if (bc) bulk_g2s(o, F.ccol + sg.e0, bc, bar);
+    o += ents_cap * 4;
+    if (bv) bulk_g2s(o, static_cast<const S*>(F.cval) + sg.e0, bv, bar);
+}
+
+// Relaxed accesses without a compiler memory clobber: the chunk kernel orders
+// its shared-memory traffic with barriers, so these need not pin every other
+// access in place (which would serialize a row's loads).
+__device__ __forceinline__ float ld_relaxed_gpu(const float* p)
+{
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_relaxed_gpu(const double* p)
+{
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(float* p, float v)
+{
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v));
+}
+__device__ __forceinline__ void st_relaxed_gpu(double* p, double v)
+{
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v));
+}
+
+// wait_value without the clobber (same bound and drain rule)
+template <typename T>
+__device__ __noinline__ T poll_value(const T* p, int* err, int sleep_ns)
+{
+    T w = ld_relaxed_gpu(p);
+    long long spins = 0;
+    while (is_sentinel(w)) {
+        if ((++spins & 255) == 0 && *(volatile int*)err) return T(0);
+        if (spins > kSpinLimit) {
+            atomicExch(err, 1);
+            return T(0);
+        }
+        if (sleep_ns > 0) __nanosleep(sleep_ns);
+        w = ld_relaxed_gpu(p);
+    }
+    return w;
+}
+
+// One thread's row of a staged wave, in registers.
+template <typename S, int KM>
+struct WaveRow {
+    int nw, K, row;
+    S dia;
+    int col[KM];
+    S val[KM];
+};
+
+template <typename S, int KM>
+__device__ __forceinline__ void wave_row(const unsigned* swv, const int* srow, const S* sdia, const int* scol,
+                                         const S* sval, int w, int poff, int eoff, int tid, WaveRow<S, KM>& r)
+{
+    const unsigned m = swv[w];
+    r.nw = int(m & 0xFFFFu);
+    r.K = int(m >> 16);
+    r.row = -1;
+    if (tid < r.nw) {
+        r.row = srow[poff + tid];
+        r.dia = sdia[poff + tid];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            r.col[k] = -1;
+            if (k < r.K) {
+                r.col[k] = scol[eoff + k * r.nw + tid];
+                r.val[k] = sval[eoff + k * r.nw + tid];
+            }
+        }
+    }
+}
+
+// ---- thread-block cluster helpers (distributed shared memory)
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_size()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// shared::cluster address of `p` (own shared memory) in the CTA of rank `rank`
+__device__ __forceinline__ unsigned map_rank(const void* p, unsigned rank)
+{
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, unsigned v)
+{
+    asm volatile("st.relaxed.cluster.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, float v)
+{
+    asm volatile("st.relaxed.cluster.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v));
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, double v)
+{
+    asm volatile("st.relaxed.cluster.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v));
+}
+__device__ __forceinline__ float ld_inbox(const float* p)
+{
+    float v;
+    asm volatile("ld.relaxed.cluster.shared::cta.f32 %0, [%1];" : "=f"(v) : "r"(smem_u32(p)));
+    return v;
+}
+__device__ __forceinline__ double ld_inbox(const double* p)
+{
+    double v;
+    asm volatile("ld.relaxed.cluster.shared::cta.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
+    return v;
+}
+
+// Polls an inbox entry (written by the previous CTA of the cluster); same
+// bound and drain rule as poll_value.
+template <typename T>
+__device__ __noinline__ T poll_inbox(const T* p, int* err)
+{
+    T w = ld_inbox(p);
+    long long spins = 0;
+    while (is_sentinel(w)) {
+        if ((++spins & 255) == 0 && *(volatile int*)err) return T(0);
+        if (spins > kSpinLimit) {
+            atomicExch(err, 1);
+            return T(0);
+        }
+        w = ld_inbox(p);
+    }
+    return w;
+}
+
+// Launched in clusters of C CTAs (C = 1: plain launch).  A cluster takes a
+// group of up to C consecutive chunks of one system; rank r works on chunk
+// pos0 + r.  With op.inbox, rank r pushes each of its results into rank
+// r + 1's inbox (a sentinel-filled shared vector indexed like the producer's
+// rows), so the dependencies of a chunk on its predecessor are read from the
+// CTA's own shared memory; all other dependencies on earlier chunks are
+// polled in global memory.  Cluster barriers: after the group is handed out
+// (all ranks see it), and after the inboxes are filled (no push lands before
+// its inbox is reset); the next group's first barrier also ends this one, so
+// no rank resets its inbox while the previous rank still pushes into it.
+template <typename T, typename S, int NT, int KM>
+__global__ void __launch_bounds__(NT) k_sweep_chunk(SetView sv, ChunkSweepOp op)
+{
+    extern __shared__ __align__(128) unsigned char chunk_smem[];
+    __shared__ __align__(8) unsigned long long bars[kStageBufs];
+    __shared__ unsigned s_task, s_go;
+    __shared__ int s_nw[kStageBufs];
+    typedef typename std::conditional<(sizeof(S) > sizeof(T)), S, T>::type W;   // promoted type
+    T* yl = reinterpret_cast<T*>(chunk_smem);
+    T* inbox = reinterpret_cast<T*>(chunk_smem + op.vec_bytes);
+    unsigned char* stage = chunk_smem + op.vec_bytes * (op.inbox ? 2 : 1);
+    const int sbytes = stage_bytes<S>(op.rows_cap, op.ents_cap);
+    const int tid = threadIdx.x;
+    const unsigned cr = cluster_rank(), C = cluster_size();
+    const int nclusters = int(gridDim.x / C);
+    if (tid == 0) {
+        for (int b = 0; b < kStageBufs; ++b) mbar_init(&bars[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    unsigned consumed = 0;   // segments this CTA has consumed (uniform)
+    for (;;) {
+        if (cr == 0 && tid == 0) {
+            const int t = atomicAdd(op.ticket, 1);
+            if (t == op.ntasks + nclusters - 1) atomicExch(op.ticket, 0);
+            unsigned go = 0;
+            if (t < op.ntasks) {
+                const GroupTask gt = op.tasks[t];
+                go = !skip_system(sv.st[gt.sys], op.skip) && !*(volatile int*)sv.err;
+            }
+            for (unsigned q = 0; q < C; ++q) {
+                st_cluster(map_rank(&s_task, q), unsigned(t));
+                st_cluster(map_rank(&s_go, q), go);
+            }
+        }
+        if (C > 1) cluster_sync(); else __syncthreads();
+        const int t = int(s_task);
+        const bool go = s_go != 0;
+        GroupTask gt = {0, 0, 0, 0};
+        if (t < op.ntasks && go) gt = op.tasks[t];
+        const bool mine = int(cr) < gt.count;
+        const SysDesc& d = sv.desc[gt.sys];
+        const TriFactor& F = op.which == 0 ? d.L : d.U;
+        const int pos = gt.pos0 + int(cr);
+        const int B = F.chunk_rows;
+        const int r0 = mine ? (op.which == 0 ? pos : F.nch - 1 - pos) * B : 0;
+        const int nr = mine ? min(d.n - r0, B) : 0;
+        const bool has_pred = op.inbox && mine && cr >= 1;
+        const bool push = op.inbox && int(cr) + 1 < gt.count;
+        const int r0p = op.which == 0 ? r0 - B : r0 + B;       // predecessor chunk's rows
+        const int nrp = has_pred ? min(d.n - r0p, B) : 0;
+        const int s0 = mine ? F.cseg[pos] : 0, nseg = mine ? F.cseg[pos + 1] - s0 : 0;
+        SegRec ahead;   // thread 0: the next segment to stage
+        if (tid == 0) {
+            for (int i = 0; i < kStageBufs - 1 && i < nseg; ++i) {
+                const SegRec sg = F.segs[s0 + i];
+                const unsigned b = (consumed + i) % kStageBufs;
+                s_nw[b] = sg.nw;
+                stage_segment<S>(F, sg, stage + b * sbytes, op.rows_cap, op.ents_cap, &bars[b]);
+            }
+            if (kStageBufs - 1 < nseg) ahead = F.segs[s0 + kStageBufs - 1];
+        }
+        T* y = mine ? vptr<T>(d, op.out) : nullptr;
+        T* R = mine && op.reset != SLOT_NONE ? vptr<T>(d, op.reset) : nullptr;
+        if (mine) {
+            const T* v = vptr<T>(d, op.in);
+            for (int i = tid; i < nr; i += NT) yl[i] = v[r0 + i];
+        }
+        if (op.inbox)
+            for (int i = tid; i < B; i += NT) inbox[i] = sentinel_value<T>();
+        if (C > 1) cluster_sync(); else __syncthreads();
+        if (t >= op.ntasks) break;
+        if (!mine) continue;
+        const unsigned rpush = push ? map_rank(inbox, cr + 1) : 0u;
+        for (int i = 0; i < nseg; ++i) {
+            const unsigned g = consumed + i, b = g % kStageBufs;
+            if (tid == 0 && i + kStageBufs - 1 < nseg) {
+                // buffer of segment i - 1, released by the barrier that ended it
+                const unsigned bn = (g + kStageBufs - 1) % kStageBufs;
+                s_nw[bn] = ahead.nw;
+                stage_segment<S>(F, ahead, stage + bn * sbytes, op.rows_cap, op.ents_cap, &bars[bn]);
+                if (i + kStageBufs < nseg) ahead = F.segs[s0 + i + kStageBufs];
+            }
+            mbar_wait(&bars[b], (g / kStageBufs) & 1u, sv.err);
+            const unsigned char* buf = stage + b * sbytes;
+            const unsigned* swv = reinterpret_cast<const unsigned*>(buf);
+            const int* srow = reinterpret_cast<const int*>(buf + op.rows_cap * 4);
+            const S* sdia = reinterpret_cast<const S*>(buf + op.rows_cap * 8);
+            const int* scol = reinterpret_cast<const int*>(buf + op.rows_cap * (8 + int(sizeof(S))));
+            const S* sval = reinterpret_cast<const S*>(buf + op.rows_cap * (8 + int(sizeof(S))) + op.ents_cap * 4);
+            const int nwaves = s_nw[b];
+            int poff = 0, eoff = 0;
+            WaveRow<S, KM> cur, nxt;
+            wave_row<S, KM>(swv, srow, sdia, scol, sval, 0, 0, 0, tid, cur);
+            for (int w = 0; w < nwaves; ++w) {
+                if (cur.row >= 0) {
+                    // all in-chunk reads at once, then the waits on earlier chunks
+                    T rr = yl[cur.row - r0];
+                    T dv[KM];
+                    bool ext = false;
+#pragma unroll
+                    for (int k = 0; k < KM; ++k) {
+                        const unsigned lc = unsigned(cur.col[k] - r0);
+                        dv[k] = T(0);
+                        if (lc < unsigned(nr)) dv[k] = yl[lc];
+                        else if (cur.col[k] >= 0) ext = true;
+                    }
+                    if (ext) {
+#pragma unroll
+                        for (int k = 0; k < KM; ++k) {
+                            const int col = cur.col[k];
+                            if (col >= 0 && unsigned(col - r0) >= unsigned(nr)) {
+                                const unsigned lp = unsigned(col - r0p);
+                                dv[k] = lp < unsigned(nrp) ? poll_inbox(inbox + lp, sv.err)
+                                                           : poll_value(y + col, sv.err, op.sleep_ns);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < KM; ++k)
+                        if (cur.col[k] >= 0) rr = sweep_step<T, S>(rr, cur.val[k], dv[k]);
+                    const T out = unsentinel(T(W(rr) * W(cur.dia)));
+                    yl[cur.row - r0] = out;
+                    if (push) st_cluster(rpush + unsigned(cur.row - r0) * unsigned(sizeof(T)), out);
+                    st_relaxed_gpu(y + cur.row, out);
+                    if (R) R[cur.row] = sentinel_value<T>();
+                }
+                poff += cur.nw;
+                eoff += cur.K * cur.nw;
+                if (w + 1 < nwaves) wave_row<S, KM>(swv, srow, sdia, scol, sval, w + 1, poff, eoff, tid, nxt);
+                __syncthreads();
+                cur = nxt;
+            }
+        }
+        consumed += unsigned(nseg);
+    }
+}
+
 // ---------------------------------------------------------------- factorization
 // Device-side ILU(0) (boost/numeric/itl/pc/ilu_0.hpp:45-82, Saad's IKJ form
 // without fill): row i, for each k < i in its pattern (ascending):

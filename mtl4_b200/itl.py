@@ -89,6 +89,15 @@ class pc:
             check(self.ctx._L.mtlg_pc_levels(self.h, C.byref(a), C.byref(b)), "levels")
             return a.value, b.value
 
+        def sweep_plan(self, dtype=np.float64) -> dict:
+            """Launch plan of the chunked sweeps for vectors of `dtype` under
+            the context's tuning (all zero: flat level-order sweeps)."""
+            out = (C.c_int * 8)()
+            dt = _lib.F32 if np.dtype(dtype) == np.float32 else _lib.F64
+            check(self.ctx._L.mtlg_pc_sweep_plan(self.ctx.h, self.h, dt, out), "sweep_plan")
+            keys = ("chunk_rows", "chunks", "cluster", "clusters_resident", "smem", "threads", "entries", "inbox")
+            return dict(zip(keys, list(out)))
+
         def factor(self, which: str):
             """Stored factor ('L' or 'U') as (row_ptr, col, val) host arrays."""
             w = 0 if which == "L" else 1
