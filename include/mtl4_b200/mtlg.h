@@ -204,11 +204,11 @@ int mtlg_pc_factor(const mtlg_pc* P, int which, int64_t* nnz, int64_t* row_ptr, 
 int mtlg_pc_levels(const mtlg_pc* P, int* levels_L, int* levels_U);
 /* Launch plan of the chunked sweeps for vectors of `dtype` under the
  * context's current tuning, as 8 integers: rows per chunk, chunks of L,
- * CTAs per cluster, clusters resident at once, shared memory per CTA
- * (bytes), CTA threads, entries per row (register bucket), inbox (1: the
- * predecessor chunk's results are pushed into shared memory).  All zero
- * when the flat level-order sweeps run instead.  Not part of the reference's
- * interface (introspection for tuning). */
+ * CTAs resident at once, shared memory per CTA (bytes), compute threads per
+ * CTA (one receiver warp more), entries per row (register bucket), rows and
+ * entries per staged segment.  All zero when the flat level-order sweeps
+ * run instead.  Not part of the reference's interface (introspection for
+ * tuning). */
 int mtlg_pc_sweep_plan(mtlg_ctx* ctx, mtlg_pc* P, int dtype, int32_t* out8);
 
 /* ---- solvers ---------------------------------------------------------------- */

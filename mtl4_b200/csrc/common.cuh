@@ -82,10 +82,12 @@ struct SweepTask {
 };
 
 // One segment of a chunked triangular factor: waves [w0, w0 + nw), positions
-// [p0, p0 + np), entries [e0, e0 + ne); w0, p0 and e0 are multiples of 4.
+// [p0, p0 + np), entries [e0, e0 + ne); the starts are multiples of 4.
 struct __align__(16) SegRec {
     int w0, nw, p0, np, e0, ne, pad0, pad1;
 };
+
+constexpr unsigned kWaveOverflow = 0x8000u;   // wave reads rows of earlier chunks beyond the receive slots
 
 // Level-ordered triangular factor (device pointers).  Row k of the factor is
 // original row `row_of[k]` (-1 marks padding that aligns levels to warps);
@@ -103,17 +105,29 @@ struct TriFactor {
     // one dependency level (at most the launch's thread count rows each),
     // consecutive waves in segments that one bulk copy per array stages in
     // shared memory.  A wave's entries are column-major: entry k of its t-th
-    // row sits at k * rows + t after the wave's first entry (column -1 past
-    // the row's own entries).  Every segment starts 16-byte aligned in every
-    // array.
+    // row sits at k * rows + t after the wave's first entry.  Columns are
+    // coded as cells of the chunk's shared vector (B = chunk_rows): c < B a
+    // row of the chunk, c == B a cell holding +0 (entries past a row's own,
+    // with value +0: exactly neutral in the row's arithmetic), c > B receive
+    // slot c - B - 1, filled by the receiver warp with a row of an earlier
+    // chunk (cext lists those rows' positions per chunk, in slot order);
+    // c < 0 a row of an earlier chunk at position -c - 2, read directly (its
+    // wave carries kWaveOverflow).  Results cross chunks through ypos, in
+    // position order (a wave's results are contiguous).  Every segment starts
+    // 16-byte aligned in every array.
     int chunk_rows;    // 0: no chunked layout
     int nch;
     int seg_rows;      // rows per segment, at most
     int pad1;
     const int* cseg;   // [nch + 1] segment range of each chunk
     const SegRec* segs;          // [segments]
-    const unsigned* wv;// [waves] rows | entries per row << 16
+    const unsigned* wv;// [waves] rows | kWaveOverflow | entries per row << 16
     const int* crow;   // row at each position
+    const int* cxr;    // [nch + 1] receive-slot range of each chunk in cext
+    const int* cext;   // positions of earlier chunks' rows, per chunk in slot order
+    void* ypos;        // results by position (T), all sentinel before the sweep
+    void* ypos_reset;  // the other factor's results by position: reset to the sentinel by this sweep
+    int npos, npos_reset;
     const int* ccol;   // entries' columns
     const void* cval;  // entries' values (S)
     const void* cdia;  // multiplier per position (S)

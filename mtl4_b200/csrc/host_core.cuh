@@ -25,7 +25,6 @@ struct mtlg_ctx {
     int spmv_kernel = 0;        // tuning: 0 auto (row-length statistics), 1 stream tiles, 2 warp tasks
     int chunk_rows = 0;         // tuning: rows per sweep chunk of new preconditioners (0: by size)
     int sweep_kernel = 0;       // tuning: 0 chunked waves, 1 flat level order
-    int sweep_cluster = 0;      // tuning: chunks per cluster of the chunked sweeps (0: 8, 1: no cluster)
     int* d_scratch_err = nullptr;
     int sweep_blocks() const
     {

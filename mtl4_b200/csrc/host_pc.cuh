@@ -30,26 +30,36 @@ struct TriDev {
     int threads = 0;    // rows per wave, at most (the launch's CTA size)
     int seg_rows = 0;   // rows per segment, at most
     int seg_ents = 0;   // entries per segment, at most
-    DBuf<int> cseg, crow, ccol, csrc, cmul;
+    int max_slots = 0;  // receive slots of a chunk, at most
+    DBuf<int> cseg, cxr, cext, crow, ccol, csrc, cmul;
     DBuf<SegRec> segs;
     DBuf<unsigned> wv;
     DBuf<unsigned char> cval, cdia;    // storage type S
+    DBuf<unsigned char> ypos[2];       // results by position for FP64 [0] / FP32 [1] vectors (all sentinel between sweeps)
 };
 
 constexpr int kChunkMaxEntries = 16;   // longer factor rows: flat sweeps only
 
 inline int round4(int v) { return (v + 3) & ~3; }
-inline int entries_bucket(int k) { return k <= 4 ? 4 : k <= 8 ? 8 : 16; }
+inline int entries_bucket(int k) { return k <= 2 ? 2 : k <= 3 ? 3 : k <= 4 ? 4 : k <= 8 ? 8 : 16; }
 
 // Chunked layout of a triangular factor: chunks of B contiguous rows in
 // processing order; inside a chunk the rows are grouped by dependency level
 // (waves, split to at most `threads` rows), a wave's rows in the order of
 // the flat layout; consecutive waves form segments of at most seg_rows rows
-// and seg_ents entries; entries wave-major as described at TriFactor.
+// and seg_ents entries; entries wave-major as described at TriFactor.  The
+// columns are coded as cells of the chunk's shared vector: a row of the
+// chunk as its index in the chunk, B (a cell holding +0, with value 0) past a
+// row's entries, B + 1 + slot for the first B entries of a chunk whose row
+// lies in an earlier chunk (in wave order; that row's position listed in
+// cext, where the chunk's receiver warp fetches it from the position-ordered
+// results); any further ones as -(position + 2), polled directly, their wave
+// flagged with kWaveOverflow.
 inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& lev, int n, bool lower, int B,
                         TriDev& T)
 {
     T.nch = 0;
+    T.max_slots = 0;
     int kmax = 0;
     for (int i = 0; i < n; ++i) kmax = std::max(kmax, F.rp[i + 1] - F.rp[i]);
     if (n == 0 || B <= 0 || kmax > kChunkMaxEntries) return MTLG_OK;
@@ -77,9 +87,11 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     }
     const int NT = std::min(256, std::max(32, (maxw + 31) / 32 * 32));
     const int KB = entries_bucket(kmax);
-    const int SR = std::max(NT, 2048 / KB);
+    // segment capacity: a multiple of 32 rows, so every staged array (and
+    // every staging buffer) starts 16-byte aligned in shared memory
+    const int SR = std::max(NT, (1024 / KB + 31) / 32 * 32);
     const int SE = SR * KB;
-    std::vector<int> cseg(1, 0), crow, ccol, csrc, cmul;
+    std::vector<int> cseg(1, 0), cxr(1, 0), cext, crow, ccol, csrc, cmul;
     std::vector<unsigned> wv;
     std::vector<SegRec> segs;
     SegRec cur{};
@@ -102,9 +114,12 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         cur = SegRec{int(wv.size()), 0, int(crow.size()), 0, int(ccol.size()), 0, 0, 0};
         open = true;
     };
+    std::vector<int> pos_of(n, -1);   // position of each row in this layout
     for (int p = 0; p < nch; ++p) {
-        int q = cbeg[p];
-        while (q < cbeg[p + 1]) {
+        const int ch = lower ? p : nch - 1 - p;
+        const int r0 = ch * B, r1 = std::min(n, r0 + B);
+        int nslot = 0;
+        for (int q = cbeg[p]; q < cbeg[p + 1];) {
             int qe = q + 1;
             while (qe < cbeg[p + 1] && qe - q < NT && lev[order[qe]] == lev[order[q]]) ++qe;
             const int nw = qe - q;
@@ -112,29 +127,50 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
             for (int j = q; j < qe; ++j) K = std::max(K, F.rp[order[j] + 1] - F.rp[order[j]]);
             if (open && (int(crow.size()) - cur.p0 + nw > SR || int(ccol.size()) - cur.e0 + K * nw > SE)) close_seg();
             if (!open) open_seg();
+            const size_t wvi = wv.size();
             wv.push_back(unsigned(nw) | (unsigned(K) << 16));
+            bool ovf = false;
             const size_t ent = ccol.size();
-            for (int j = q; j < qe; ++j) crow.push_back(order[j]);
-            ccol.resize(ent + size_t(K) * nw, -1);
-            csrc.resize(ent + size_t(K) * nw, 0);
+            for (int j = q; j < qe; ++j) {
+                pos_of[order[j]] = int(crow.size());
+                crow.push_back(order[j]);
+            }
+            ccol.resize(ent + size_t(K) * nw, B);     // padding: the zero cell, value 0
+            csrc.resize(ent + size_t(K) * nw, -1);
             cmul.resize(ent + size_t(K) * nw, -1);
             for (int t = 0; t < nw; ++t) {
                 const int r = order[q + t];
                 for (int k = 0; k < F.rp[r + 1] - F.rp[r]; ++k) {
                     const size_t e = ent + size_t(k) * nw + t;
-                    ccol[e] = F.col[F.rp[r] + k];
+                    const int col = F.col[F.rp[r] + k];
+                    int code;
+                    if (col >= r0 && col < r1) {
+                        code = col - r0;                 // row of this chunk
+                    } else if (nslot < B) {
+                        cext.push_back(pos_of[col]);     // earlier chunk: receive slot
+                        code = B + 1 + nslot;
+                        ++nslot;
+                    } else {
+                        code = -(pos_of[col] + 2);       // earlier chunk beyond the slots: polled directly
+                        ovf = true;
+                    }
+                    ccol[e] = code;
                     csrc[e] = F.src[F.rp[r] + k];
                     cmul[e] = F.mul[F.rp[r] + k];
                 }
             }
+            if (ovf) wv[wvi] |= kWaveOverflow;
             q = qe;
         }
         close_seg();
         cseg.push_back(int(segs.size()));
+        cxr.push_back(int(cext.size()));
+        T.max_slots = std::max(T.max_slots, nslot);
     }
     // tails: a staged copy rounds each array's segment up to 16 bytes
     wv.resize(round4(int(wv.size())) + 4, 0u);
     crow.resize(round4(int(crow.size())) + 4, -1);
+    cext.resize(cext.size() + 4, 0);
     const int e = round4(int(ccol.size())) + 4;
     ccol.resize(e, -1);
     csrc.resize(e, 0);
@@ -150,6 +186,8 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     T.seg_rows = SR;
     T.seg_ents = SE;
     MTLG_TRY(T.cseg.upload(c, cseg.data(), cseg.size()));
+    MTLG_TRY(T.cxr.upload(c, cxr.data(), cxr.size()));
+    MTLG_TRY(T.cext.upload(c, cext.data(), cext.size()));
     MTLG_TRY(T.segs.upload(c, segs.data(), segs.size()));
     MTLG_TRY(T.wv.upload(c, wv.data(), wv.size()));
     MTLG_TRY(T.crow.upload(c, crow.data(), crow.size()));
@@ -163,17 +201,17 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
 constexpr int kChunkSmemMax = 225 * 1024;   // dynamic shared memory of one chunk CTA, at most
 
 // Launch plan of the chunked sweeps of a set of factors (computed outside
-// any stream capture: it queries the occupancy of clusters).
+// any stream capture: it queries the occupancy).
 struct ChunkPlan {
     bool ok = false;
-    int nt = 0, km = 0;          // CTA size, entries per row
+    int nt = 0, km = 0;          // compute threads per CTA, entries per row
     int rows = 0;                // rows of the largest chunk
+    int slots = 0;               // receive slots of the largest chunk
     int seg_rows = 0, seg_ents = 0;
-    int cluster = 1;             // CTAs per cluster (chunks per group)
-    int inbox = 0;               // predecessor results pushed into shared memory
     int smem = 0;                // dynamic shared memory per CTA
-    int max_clusters = 1;        // clusters resident at once
+    int resident = 1;            // CTAs resident at once
     int vec_bytes = 0;
+    int cells = 0;               // shared cells of the largest chunk (rows, +0 cell, slots)
     DBuf<GroupTask> tl, tu;
     int ntl = 0, ntu = 0;
     void add(const TriDev& T)
@@ -181,6 +219,8 @@ struct ChunkPlan {
         nt = std::max(nt, T.threads);
         km = std::max(km, T.kmax);
         rows = std::max(rows, T.chunk_rows);
+        slots = std::max(slots, T.max_slots);
+        cells = std::max(cells, T.chunk_rows + 1 + T.max_slots);
         seg_rows = std::max(seg_rows, T.seg_rows);
         seg_ents = std::max(seg_ents, T.seg_ents);
     }
@@ -196,29 +236,11 @@ struct ChunkShape {
                                        kChunkSmemMax));
         return MTLG_OK;
     }
-    static cudaLaunchConfig_t config(dim3 grid, int smem, cudaStream_t st, cudaLaunchAttribute* attr, int cluster)
+    static int occupancy(int smem)
     {
-        cudaLaunchConfig_t cfg;
-        memset(&cfg, 0, sizeof cfg);
-        cfg.gridDim = grid;
-        cfg.blockDim = dim3(NT, 1, 1);
-        cfg.dynamicSmemBytes = size_t(smem);
-        cfg.stream = st;
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = unsigned(cluster);
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        return cfg;
-    }
-    // clusters of `cluster` CTAs resident at once (0: the shape does not fit)
-    static int max_clusters(int smem, int cluster)
-    {
-        cudaLaunchAttribute attr[1];
-        cudaLaunchConfig_t cfg = config(dim3(unsigned(cluster) * 64u, 1, 1), smem, nullptr, attr, cluster);
         int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, k_sweep_chunk<T, S, NT, KM>, &cfg) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_chunk<T, S, NT, KM>, NT + 32 * kChunkExtraWarps, size_t(smem)) !=
+            cudaSuccess) {
             cudaGetLastError();
             return 0;
         }
@@ -226,20 +248,19 @@ struct ChunkShape {
     }
     static int launch(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const ChunkSweepOp& op, const ChunkPlan& pl)
     {
-        const int groups = std::max(1, std::min(op.ntasks, pl.max_clusters));
-        cudaLaunchAttribute attr[1];
-        cudaLaunchConfig_t cfg = config(dim3(unsigned(groups * pl.cluster), 1, 1), pl.smem, st, attr, pl.cluster);
-        MTLG_CUDA(cudaLaunchKernelEx(&cfg, k_sweep_chunk<T, S, NT, KM>, sv, op));
+        const int grid = std::max(1, std::min(op.ntasks, pl.resident));
+        k_sweep_chunk<T, S, NT, KM><<<grid, kChunkExtraWarps * 32 + NT, pl.smem, st>>>(sv, op);
         c->launches++;
+        MTLG_CUDA(cudaGetLastError());
         return MTLG_OK;
     }
 };
 
 #define MTLG_CHUNK_SHAPES(M, T, S) \
-    M(T, S, 32, 4) M(T, S, 32, 8) M(T, S, 32, 16) \
-    M(T, S, 64, 4) M(T, S, 64, 8) M(T, S, 64, 16) \
-    M(T, S, 128, 4) M(T, S, 128, 8) M(T, S, 128, 16) \
-    M(T, S, 256, 4) M(T, S, 256, 8) M(T, S, 256, 16)
+    M(T, S, 32, 2) M(T, S, 32, 3) M(T, S, 32, 4) M(T, S, 32, 8) M(T, S, 32, 16) \
+    M(T, S, 64, 2) M(T, S, 64, 3) M(T, S, 64, 4) M(T, S, 64, 8) M(T, S, 64, 16) \
+    M(T, S, 128, 2) M(T, S, 128, 3) M(T, S, 128, 4) M(T, S, 128, 8) M(T, S, 128, 16) \
+    M(T, S, 256, 2) M(T, S, 256, 3) M(T, S, 256, 4) M(T, S, 256, 8) M(T, S, 256, 16)
 
 inline int init_chunk_shapes()
 {
@@ -253,24 +274,24 @@ inline int init_chunk_shapes()
 }
 
 template <typename T, typename S>
-inline int chunk_max_clusters(const ChunkPlan& pl, int smem, int cluster)
+inline int chunk_occupancy(const ChunkPlan& pl, int smem)
 {
     const int nt = pl.threads(), km = pl.entries();
 #define MTLG_CHUNK_Q(TT, SS, NT, KM) \
-    if (nt == NT && km == KM) return ChunkShape<TT, SS, NT, KM>::max_clusters(smem, cluster);
+    if (nt == NT && km == KM) return ChunkShape<TT, SS, NT, KM>::occupancy(smem);
     MTLG_CHUNK_SHAPES(MTLG_CHUNK_Q, T, S)
 #undef MTLG_CHUNK_Q
     return 0;
 }
 
-// Shape, cluster size and group lists of a set of systems' factors (pcs[s]:
-// the system's factors or null for an unused slot).  Groups of up to
-// `cluster` consecutive chunks of one system, interleaved across systems.
+// Shape and task list of a set of systems' factors (f[s]: the system's L and
+// U, or nulls for an unused slot); chunks of all systems interleaved by
+// processing position.
 template <typename T, typename S>
 inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, const TriDev*>>& f, ChunkPlan& pl)
 {
     pl.ok = false;
-    pl.nt = pl.km = pl.rows = pl.seg_rows = pl.seg_ents = 0;
+    pl.nt = pl.km = pl.rows = pl.slots = pl.cells = pl.seg_rows = pl.seg_ents = 0;
     pl.ntl = pl.ntu = 0;
     bool any = false;
     for (const auto& lu : f) {
@@ -281,39 +302,25 @@ inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, c
         pl.add(*lu.second);
     }
     if (!any || c->sweep_kernel != 0) return MTLG_OK;
-    pl.vec_bytes = int((size_t(pl.rows) * sizeof(T) + 15) / 16 * 16);
-    const int stage = kStageBufs * stage_bytes<S>(pl.seg_rows, pl.seg_ents);
-    // largest cluster (8, 4, 2) whose CTAs fit with the inbox; else no cluster
-    pl.cluster = 1;
-    pl.inbox = 0;
-    pl.smem = pl.vec_bytes + stage;
+    if (pl.seg_rows % 4 || pl.seg_ents % 4) {
+        set_error("chunked sweep: staging capacity %d/%d is not a multiple of 4", pl.seg_rows, pl.seg_ents);
+        return MTLG_ERR_NOT_SUPPORTED;
+    }
+    pl.vec_bytes = int((size_t(pl.cells) * sizeof(T) + 15) / 16 * 16);
+    pl.smem = pl.vec_bytes + kStageBufs * stage_bytes<S>(pl.seg_rows, pl.seg_ents);
     if (pl.smem > kChunkSmemMax) return MTLG_OK;
-    const int want = c->sweep_cluster > 0 ? c->sweep_cluster : 8;
-    if (2 * pl.vec_bytes + stage <= kChunkSmemMax) {
-        for (int cl = want; cl >= 2; cl /= 2) {
-            const int n = chunk_max_clusters<T, S>(pl, 2 * pl.vec_bytes + stage, cl);
-            if (n >= 1) {
-                pl.cluster = cl;
-                pl.inbox = 1;
-                pl.smem = 2 * pl.vec_bytes + stage;
-                pl.max_clusters = n;
-                break;
-            }
-        }
-    }
-    if (pl.cluster == 1) {
-        pl.max_clusters = std::max(1, chunk_max_clusters<T, S>(pl, pl.smem, 1));
-    }
+    const int occ = chunk_occupancy<T, S>(pl, pl.smem);
+    if (occ < 1) return MTLG_OK;
+    pl.resident = c->sm_count * occ;
     std::vector<GroupTask> tl, tu;
     int maxch = 0;
     for (const auto& lu : f)
         if (lu.first) maxch = std::max({maxch, lu.first->nch, lu.second->nch});
-    for (int p0 = 0; p0 < maxch; p0 += pl.cluster) {
+    for (int p = 0; p < maxch; ++p) {
         for (size_t s = 0; s < f.size(); ++s) {
             if (!f[s].first) continue;
-            const int nl = f[s].first->nch, nu = f[s].second->nch;
-            if (p0 < nl) tl.push_back({int(s), p0, std::min(pl.cluster, nl - p0), 0});
-            if (p0 < nu) tu.push_back({int(s), p0, std::min(pl.cluster, nu - p0), 0});
+            if (p < f[s].first->nch) tl.push_back({int(s), p, 1, 0});
+            if (p < f[s].second->nch) tu.push_back({int(s), p, 1, 0});
         }
     }
     pl.ntl = int(tl.size());
@@ -331,7 +338,6 @@ inline int launch_chunk_sweep(mtlg_ctx* c, cudaStream_t st, const SetView& sv, C
     op.vec_bytes = pl.vec_bytes;
     op.rows_cap = pl.seg_rows;
     op.ents_cap = pl.seg_ents;
-    op.inbox = pl.inbox;
     const int nt = pl.threads(), km = pl.entries();
 #define MTLG_CHUNK_CASE(TT, SS, NT, KM) \
     if (nt == NT && km == KM) return ChunkShape<TT, SS, NT, KM>::launch(c, st, sv, op, pl);
@@ -359,6 +365,8 @@ inline TriFactor tri_view(const TriDev& T)
         f.segs = T.segs.p;
         f.wv = T.wv.p;
         f.crow = T.crow.p;
+        f.cxr = T.cxr.p;
+        f.cext = T.cext.p;
         f.ccol = T.ccol.p;
         f.cval = T.cval.p;
         f.cdia = T.cdia.p;
@@ -485,6 +493,49 @@ inline int fill_sentinel(mtlg_ctx* c, void* p, size_t bytes)
 }
 
 inline int sweep_grid(mtlg_ctx* c) { return c->sweep_grid; }
+
+// Position-ordered results of a chunked factor for vectors of one type,
+// allocated on first use and filled with the sentinel.
+inline int ensure_ypos(mtlg_ctx* c, TriDev& T, int f32)
+{
+    if (T.nch == 0 || T.ypos[f32].p) return MTLG_OK;
+    const size_t bytes = size_t(std::max(T.cnpos, 4)) * (f32 ? 4 : 8);
+    MTLG_TRY(T.ypos[f32].alloc(c, bytes));
+    return fill_sentinel(c, T.ypos[f32].p, bytes);
+}
+
+// Device views of a preconditioner's factors for vectors of one type: each
+// sweep publishes into its own position-ordered results and resets the
+// other factor's (the next sweep of the other kind reads them sentinel).
+inline int pc_views(mtlg_pc* P, int f32, TriFactor& L, TriFactor& U)
+{
+    L = tri_view(P->L);
+    U = tri_view(P->U);
+    if (L.chunk_rows > 0 && U.chunk_rows > 0) {
+        MTLG_TRY(ensure_ypos(P->ctx, P->L, f32));
+        MTLG_TRY(ensure_ypos(P->ctx, P->U, f32));
+        L.ypos = P->L.ypos[f32].p;
+        L.npos = P->L.cnpos;
+        L.ypos_reset = P->U.ypos[f32].p;
+        L.npos_reset = P->U.cnpos;
+        U.ypos = P->U.ypos[f32].p;
+        U.npos = P->U.cnpos;
+        U.ypos_reset = P->L.ypos[f32].p;
+        U.npos_reset = P->L.cnpos;
+    }
+    return MTLG_OK;
+}
+
+// After an expired device wait: back to all-sentinel sweep buffers.
+inline int pc_reset_sweep_state(mtlg_pc* P)
+{
+    if (!P) return MTLG_OK;
+    for (TriDev* T : {&P->L, &P->U})
+        for (int k = 0; k < 2; ++k)
+            if (T->ypos[k].p) MTLG_TRY(fill_sentinel(P->ctx, T->ypos[k].p, T->ypos[k].n));
+    if (P->tmp.p) MTLG_TRY(fill_sentinel(P->ctx, P->tmp.p, size_t(P->n) * 8));
+    return MTLG_OK;
+}
 
 inline int pc_setup_single_set(mtlg_pc* P)
 {

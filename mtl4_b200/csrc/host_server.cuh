@@ -159,8 +159,7 @@ inline int srv_admit(mtlg_server* S, mtlg_server::Req& R, int e, int slot)
     d.ws_stride = stride;
     d.pc = R.P->kind;
     if (R.P->kind == MTLG_PC_DIAGONAL) d.inv_diag = R.P->inv_diag.p;
-    d.L = tri_view(R.P->L);
-    d.U = tri_view(R.P->U);
+    MTLG_TRY(pc_views(R.P, ss.f32, d.L, d.U));
     if (S->refine) {
         d.x = R.ws.p + size_t(V_W1) * stride * vb;
         d.b = R.ws.p + size_t(V_W0) * stride * vb;

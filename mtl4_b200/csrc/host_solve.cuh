@@ -166,8 +166,7 @@ inline int build_set(mtlg_ctx* c, SolveSet& ss)
         d.pc = si.P ? si.P->kind : MTLG_PC_IDENTITY;
         if (si.P && si.P->kind == MTLG_PC_DIAGONAL) d.inv_diag = si.P->inv_diag.p;
         if (si.P && (si.P->kind == MTLG_PC_DIAGONAL || si.P->has_factors())) {
-            d.L = tri_view(si.P->L);
-            d.U = tri_view(si.P->U);
+            MTLG_TRY(pc_views(si.P, ss.f32, d.L, d.U));
         }
         if (ss.mixed) {
             // inner problem: x = d (slot V_W1), b = float(r / ||r||) (slot V_W0)

@@ -122,12 +122,11 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
     d.b = y->p;
     d.ws = P->tmp.p;
     d.ws_stride = 0;
-    d.L = tri_view(P->L);
-    d.U = tri_view(P->U);
+    MTLG_TRY(pc_views(P, sizeof(T) == 4 ? 1 : 0, d.L, d.U));
     MTLG_CUDA(cudaMemcpyAsync(P->desc.p, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
     ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
     int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
-    const int setting = c->sweep_kernel * 64 + c->sweep_cluster;
+    const int setting = c->sweep_kernel;
     if (made != setting) {
         std::vector<std::pair<const TriDev*, const TriDev*>> f(1, {&P->L, &P->U});
         MTLG_TRY((plan_chunks<T, S>(c, f, pl)));
@@ -168,7 +167,7 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
         int z = 0;
         MTLG_CUDA(cudaMemcpy(P->misc.p + 1, &z, sizeof z, cudaMemcpyHostToDevice));
         MTLG_CUDA(cudaMemset(P->tickets.p, 0, 8 * sizeof(int)));
-        MTLG_TRY(fill_sentinel(c, P->tmp.p, size_t(P->n) * 8));
+        MTLG_TRY(pc_reset_sweep_state(P));
         set_error("triangular sweep dependency wait expired");
         return MTLG_ERR_TIMEOUT;
     }
@@ -349,7 +348,6 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "spmv_kernel") c->spmv_kernel = int(std::max<int64_t>(0, std::min<int64_t>(value, 3)));
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
     else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
-    else if (k == "sweep_cluster") c->sweep_cluster = int(std::max<int64_t>(0, std::min<int64_t>(value, 8)));
     else if (k == "chunk_rows") c->chunk_rows = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 15)));
     else {
         set_error("unknown tuning key '%s'", key);
@@ -370,7 +368,6 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     else if (k == "sweep_sleep_ns") *value = c->sweep_sleep_ns;
     else if (k == "sm_count") *value = c->sm_count;
     else if (k == "sweep_kernel") *value = c->sweep_kernel;
-    else if (k == "sweep_cluster") *value = c->sweep_cluster;
     else if (k == "chunk_rows") *value = c->chunk_rows;
     else {
         set_error("unknown tuning key '%s'", key);
@@ -810,7 +807,7 @@ static int sweep_plan_of(mtlg_ctx* c, mtlg_pc* P, int32_t* out)
 {
     ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
     int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
-    const int setting = c->sweep_kernel * 64 + c->sweep_cluster;
+    const int setting = c->sweep_kernel;
     if (made != setting) {
         std::vector<std::pair<const TriDev*, const TriDev*>> f(1, {&P->L, &P->U});
         MTLG_TRY((plan_chunks<T, S>(c, f, pl)));
@@ -820,12 +817,12 @@ static int sweep_plan_of(mtlg_ctx* c, mtlg_pc* P, int32_t* out)
     if (!pl.ok) return MTLG_OK;
     out[0] = pl.rows;
     out[1] = P->L.nch;
-    out[2] = pl.cluster;
-    out[3] = pl.max_clusters;
-    out[4] = pl.smem;
-    out[5] = pl.threads();
-    out[6] = pl.entries();
-    out[7] = pl.inbox;
+    out[2] = pl.resident;
+    out[3] = pl.smem;
+    out[4] = pl.threads();
+    out[5] = pl.entries();
+    out[6] = pl.seg_rows;
+    out[7] = pl.seg_ents;
     return MTLG_OK;
 }
 }
@@ -880,6 +877,7 @@ static int timed_result(mtlg_ctx* c, SolveSet& ss, cudaEvent_t e0, cudaEvent_t e
         int z = 0;
         MTLG_CUDA(cudaMemcpy(ss.misc.p + 1, &z, sizeof z, cudaMemcpyHostToDevice));
         MTLG_CUDA(cudaMemset(ss.tickets.p, 0, 8 * sizeof(int)));
+        for (auto& si : ss.in) MTLG_TRY(pc_reset_sweep_state(si.P));
         set_error("a device-side wait expired during the solve");
         return MTLG_ERR_TIMEOUT;
     }

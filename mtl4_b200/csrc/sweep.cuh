@@ -148,22 +148,29 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
 
 // ------------------------------------------------------------ chunked sweep
 // One CTA per chunk of contiguous rows (TriFactor's chunked layout), taken
-// in processing order through one ticket.  The chunk's inputs are loaded
-// into shared memory, then its waves run one after the other: a row reads
-// the rows of its own chunk from shared memory (finished in earlier waves,
-// made visible by the barrier between waves) and polls only rows of earlier
-// chunks in global memory.  Every result is also published to global memory
-// with a relaxed store for later chunks.  Chunks depend on earlier chunks
-// only and waves on earlier waves, and a chunk is held by a running CTA, so
-// the waits end; they are bounded all the same (wait_value).
-//
-// The chunk's structure (wave sizes, rows, multipliers, entries) streams
-// through kStageBufs shared-memory buffers, one segment of waves per buffer,
-// each segment brought in by one bulk copy per array (TMA, completion on an
-// mbarrier) issued kStageBufs - 1 segments ahead of its use, so a wave's
-// critical path is shared-memory reads, the arithmetic and the barrier.  The
-// arithmetic per row is k_sweep's (same entry order, same roundings).
+// in processing order through one ticket.  Warp roles:
+//  - NT compute threads run the chunk's waves one after the other: a row
+//    reads the rows of its own chunk from a shared vector (finished in
+//    earlier waves, made visible by a named barrier between waves), and its
+//    result is published in position order (one coalesced store per warp and
+//    wave) for later chunks;
+//  - the receiver warp fetches the results of earlier chunks this chunk
+//    needs, in the order the waves consume them, many requests in flight,
+//    into receive slots in shared memory, so a compute thread waits on the
+//    value itself, never on an L2 round trip of its own;
+//  - the producer warp streams the chunk's structure (wave sizes, rows,
+//    multipliers, entries) through kStageBufs shared buffers, one segment of
+//    waves per buffer, one bulk copy (TMA) per array, with full / empty
+//    mbarrier pairs between it and the compute threads.
+// The chunk's right-hand sides are loaded into the shared vector up front
+// and the chunk's outputs written back at its end, both coalesced.  Chunks
+// depend on earlier chunks only and waves on earlier waves, and a chunk is
+// held by a running CTA, so the waits end; they are bounded all the same
+// (kSpinLimit polls, then a timeout flag and a drain).  The arithmetic per
+// row is k_sweep's (same entry order, same roundings).
 constexpr int kStageBufs = 3;
+constexpr int kRecvDepth = 4;         // receive requests in flight per receiver lane
+constexpr int kChunkExtraWarps = 2;   // receiver and producer warps after the NT compute threads
 
 struct ChunkSweepOp {
     const GroupTask* tasks;
@@ -173,10 +180,9 @@ struct ChunkSweepOp {
     int in, out, reset; // vector slots (reset: SLOT_NONE or cleared to the sentinel)
     int skip;
     int sleep_ns;
-    int vec_bytes;      // shared vector: rows of the largest chunk x sizeof(T), 16-byte multiple
+    int vec_bytes;      // shared cells (chunk rows, the +0 cell, receive slots) of the largest chunk, 16-byte multiple
     int rows_cap;       // staging buffer capacity in rows (multiple of 4)
     int ents_cap;       // ... and in entries (multiple of 4)
-    int inbox;          // 1: a second shared vector receives the predecessor chunk's results
 };
 
 // Staging buffer layout: [wave sizes: rows_cap u32][rows: rows_cap int]
@@ -199,6 +205,11 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
 {
     unsigned ok;
@@ -212,8 +223,8 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
     return ok != 0;
 }
 
-// Bounded wait for a staged segment: after kSpinLimit polls it records a
-// timeout and keeps waiting up to the same bound again for the copy itself.
+// Bounded mbarrier wait: after kSpinLimit polls it records a timeout and
+// keeps waiting up to the same bound again (a staged copy always completes).
 __device__ __forceinline__ void mbar_wait(unsigned long long* bar, unsigned parity, int* err)
 {
     long long spins = 0;
@@ -234,9 +245,21 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 
 __device__ __forceinline__ unsigned round16u(unsigned v) { return (v + 15u) & ~15u; }
 
+// A factor's chunked-layout arrays, copied into registers once per chunk
+// (fields read through the system descriptor would be reloaded from global
+// memory after every barrier).
+struct ChunkArrays {
+    const SegRec* segs;
+    const unsigned* wv;
+    const int* crow;
+    const void* cdia;
+    const int* ccol;
+    const void* cval;
+};
+
 // Issues the copies of segment `sg` into staging buffer `buf` (one thread).
 template <typename S>
-__device__ __forceinline__ void stage_segment(const TriFactor& F, const SegRec& sg, unsigned char* buf, int rows_cap,
+__device__ __forceinline__ void stage_segment(const ChunkArrays& F, const SegRec& sg, unsigned char* buf, int rows_cap,
                                               int ents_cap, unsigned long long* bar)
 {
     const unsigned bw = round16u(unsigned(sg.nw) * 4u), br = round16u(unsigned(sg.np) * 4u);
@@ -278,8 +301,29 @@ __device__ __forceinline__ void st_relaxed_gpu(double* p, double v)
 {
     asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v));
 }
+// receive slots: written by the receiver warp, polled by the compute threads
+__device__ __forceinline__ float ld_slot(const float* p)
+{
+    float v;
+    asm volatile("ld.volatile.shared.f32 %0, [%1];" : "=f"(v) : "r"(smem_u32(p)));
+    return v;
+}
+__device__ __forceinline__ double ld_slot(const double* p)
+{
+    double v;
+    asm volatile("ld.volatile.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
+    return v;
+}
+__device__ __forceinline__ void st_slot(float* p, float v)
+{
+    asm volatile("st.volatile.shared.f32 [%0], %1;" ::"r"(smem_u32(p)), "f"(v));
+}
+__device__ __forceinline__ void st_slot(double* p, double v)
+{
+    asm volatile("st.volatile.shared.f64 [%0], %1;" ::"r"(smem_u32(p)), "d"(v));
+}
 
-// wait_value without the clobber (same bound and drain rule)
+// A result of an earlier chunk read directly (same bound and drain rule as wait_value).
 template <typename T>
 __device__ __noinline__ T poll_value(const T* p, int* err, int sleep_ns)
 {
@@ -297,92 +341,11 @@ __device__ __noinline__ T poll_value(const T* p, int* err, int sleep_ns)
     return w;
 }
 
-// One thread's row of a staged wave, in registers.
-template <typename S, int KM>
-struct WaveRow {
-    int nw, K, row;
-    S dia;
-    int col[KM];
-    S val[KM];
-};
-
-template <typename S, int KM>
-__device__ __forceinline__ void wave_row(const unsigned* swv, const int* srow, const S* sdia, const int* scol,
-                                         const S* sval, int w, int poff, int eoff, int tid, WaveRow<S, KM>& r)
-{
-    const unsigned m = swv[w];
-    r.nw = int(m & 0xFFFFu);
-    r.K = int(m >> 16);
-    r.row = -1;
-    if (tid < r.nw) {
-        r.row = srow[poff + tid];
-        r.dia = sdia[poff + tid];
-#pragma unroll
-        for (int k = 0; k < KM; ++k) {
-            r.col[k] = -1;
-            if (k < r.K) {
-                r.col[k] = scol[eoff + k * r.nw + tid];
-                r.val[k] = sval[eoff + k * r.nw + tid];
-            }
-        }
-    }
-}
-
-// ---- thread-block cluster helpers (distributed shared memory)
-__device__ __forceinline__ unsigned cluster_rank()
-{
-    unsigned r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ unsigned cluster_size()
-{
-    unsigned r;
-    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ void cluster_sync()
-{
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-// shared::cluster address of `p` (own shared memory) in the CTA of rank `rank`
-__device__ __forceinline__ unsigned map_rank(const void* p, unsigned rank)
-{
-    unsigned r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
-    return r;
-}
-__device__ __forceinline__ void st_cluster(unsigned addr, unsigned v)
-{
-    asm volatile("st.relaxed.cluster.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
-}
-__device__ __forceinline__ void st_cluster(unsigned addr, float v)
-{
-    asm volatile("st.relaxed.cluster.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v));
-}
-__device__ __forceinline__ void st_cluster(unsigned addr, double v)
-{
-    asm volatile("st.relaxed.cluster.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v));
-}
-__device__ __forceinline__ float ld_inbox(const float* p)
-{
-    float v;
-    asm volatile("ld.relaxed.cluster.shared::cta.f32 %0, [%1];" : "=f"(v) : "r"(smem_u32(p)));
-    return v;
-}
-__device__ __forceinline__ double ld_inbox(const double* p)
-{
-    double v;
-    asm volatile("ld.relaxed.cluster.shared::cta.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
-    return v;
-}
-
-// Polls an inbox entry (written by the previous CTA of the cluster); same
-// bound and drain rule as poll_value.
+// A receive slot not filled yet: wait for the receiver (same bound and drain rule).
 template <typename T>
-__device__ __noinline__ T poll_inbox(const T* p, int* err)
+__device__ __noinline__ T poll_slot(const T* p, int* err)
 {
-    T w = ld_inbox(p);
+    T w = ld_slot(p);
     long long spins = 0;
     while (is_sentinel(w)) {
         if ((++spins & 255) == 0 && *(volatile int*)err) return T(0);
@@ -390,156 +353,300 @@ __device__ __noinline__ T poll_inbox(const T* p, int* err)
             atomicExch(err, 1);
             return T(0);
         }
-        w = ld_inbox(p);
+        w = ld_slot(p);
     }
     return w;
 }
 
-// Launched in clusters of C CTAs (C = 1: plain launch).  A cluster takes a
-// group of up to C consecutive chunks of one system; rank r works on chunk
-// pos0 + r.  With op.inbox, rank r pushes each of its results into rank
-// r + 1's inbox (a sentinel-filled shared vector indexed like the producer's
-// rows), so the dependencies of a chunk on its predecessor are read from the
-// CTA's own shared memory; all other dependencies on earlier chunks are
-// polled in global memory.  Cluster barriers: after the group is handed out
-// (all ranks see it), and after the inboxes are filled (no push lands before
-// its inbox is reset); the next group's first barrier also ends this one, so
-// no rank resets its inbox while the previous rank still pushes into it.
-template <typename T, typename S, int NT, int KM>
-__global__ void __launch_bounds__(NT) k_sweep_chunk(SetView sv, ChunkSweepOp op)
+// Receiver warp: fetches ypos[cext[x0 + e]] into slot[e] for e < nx, in slot
+// order, kRecvDepth requests in flight per lane.  A value that is still the
+// sentinel is requested again; the wait is bounded like the others (on
+// expiry the slot gets a zero so the compute threads drain).
+template <typename T>
+__device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, int x0, int nx, const T* ypos, T* slot,
+                                              int lane, int* err, int sleep_ns)
 {
+    for (int base = lane; base < nx; base += 32 * kRecvDepth) {
+        int src[kRecvDepth];
+        bool pending[kRecvDepth];
+#pragma unroll
+        for (int j = 0; j < kRecvDepth; ++j) {
+            const int e = base + 32 * j;
+            pending[j] = e < nx;
+            src[j] = pending[j] ? __ldg(cext + x0 + e) : 0;
+        }
+        long long spins = 0;
+        for (;;) {
+            T v[kRecvDepth];
+#pragma unroll
+            for (int j = 0; j < kRecvDepth; ++j)
+                if (pending[j]) v[j] = ld_relaxed_gpu(ypos + src[j]);
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < kRecvDepth; ++j) {
+                if (pending[j]) {
+                    if (!is_sentinel(v[j])) {
+                        st_slot(slot + base + 32 * j, v[j]);
+                        pending[j] = false;
+                    } else {
+                        any = true;
+                    }
+                }
+            }
+            if (!any) break;
+            if ((++spins & 255) == 0 && *(volatile int*)err) break;
+            if (spins > kSpinLimit) {
+                atomicExch(err, 1);
+                break;
+            }
+            if (sleep_ns > 0) __nanosleep(sleep_ns);
+        }
+#pragma unroll
+        for (int j = 0; j < kRecvDepth; ++j)
+            if (pending[j]) st_slot(slot + base + 32 * j, T(0));
+    }
+}
+
+// One thread's row of a staged wave, in registers.
+template <typename T, typename S, int KM>
+struct WaveRow {
+    int row;
+    T rhs;
+    S dia;
+    int col[KM];
+    S val[KM];
+};
+
+template <typename T, typename S, int KM>
+__device__ __forceinline__ void wave_row(unsigned m, const int* srow, const S* sdia, const int* scol, const S* sval,
+                                         const T* vec, int B, int r0, int poff, int eoff, int tid,
+                                         WaveRow<T, S, KM>& r)
+{
+    const int nw = int(m & 0x7FFFu), K = int(m >> 16);
+    r.row = -1;
+    if (tid < nw) {
+        r.row = srow[poff + tid];
+        r.dia = sdia[poff + tid];
+        r.rhs = vec[r.row - r0];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            r.col[k] = B;      // the +0 cell, value +0: neutral
+            r.val[k] = S(0);
+            if (k < K) {
+                r.col[k] = scol[eoff + k * nw + tid];
+                r.val[k] = sval[eoff + k * nw + tid];
+            }
+        }
+    }
+}
+
+// Staging buffer views of segment buffer b.
+template <typename S>
+struct StageView {
+    const unsigned* wv;
+    const int* row;
+    const S* dia;
+    const int* col;
+    const S* val;
+    __device__ __forceinline__ StageView(const unsigned char* buf, int rows_cap, int ents_cap)
+        : wv(reinterpret_cast<const unsigned*>(buf)),
+          row(reinterpret_cast<const int*>(buf + rows_cap * 4)),
+          dia(reinterpret_cast<const S*>(buf + rows_cap * 8)),
+          col(reinterpret_cast<const int*>(buf + rows_cap * (8 + int(sizeof(S))))),
+          val(reinterpret_cast<const S*>(buf + rows_cap * (8 + int(sizeof(S))) + ents_cap * 4))
+    {
+    }
+};
+
+__device__ __forceinline__ void compute_barrier(int nt)
+{
+    asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+}
+
+template <typename T, typename S, int NT, int KM>
+__global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetView sv, ChunkSweepOp op)
+{
+    if (blockDim.x != unsigned(NT + 32 * kChunkExtraWarps)) {   // launch shape mismatch: report, never wait
+        if (threadIdx.x == 0) atomicExch(sv.err, 1);
+        return;
+    }
     extern __shared__ __align__(128) unsigned char chunk_smem[];
-    __shared__ __align__(8) unsigned long long bars[kStageBufs];
-    __shared__ unsigned s_task, s_go;
-    __shared__ int s_nw[kStageBufs];
+    __shared__ __align__(8) unsigned long long full[kStageBufs], empty[kStageBufs];
+    __shared__ int s_task, s_go;
+    __shared__ int s_nw[kStageBufs], s_p0[kStageBufs];
     typedef typename std::conditional<(sizeof(S) > sizeof(T)), S, T>::type W;   // promoted type
-    T* yl = reinterpret_cast<T*>(chunk_smem);
-    T* inbox = reinterpret_cast<T*>(chunk_smem + op.vec_bytes);
-    unsigned char* stage = chunk_smem + op.vec_bytes * (op.inbox ? 2 : 1);
+    T* vec = reinterpret_cast<T*>(chunk_smem);   // [chunk rows | +0 cell | receive slots]
+    unsigned char* stage = chunk_smem + op.vec_bytes;
     const int sbytes = stage_bytes<S>(op.rows_cap, op.ents_cap);
     const int tid = threadIdx.x;
-    const unsigned cr = cluster_rank(), C = cluster_size();
-    const int nclusters = int(gridDim.x / C);
+    constexpr int NTH = NT + 32 * kChunkExtraWarps;
     if (tid == 0) {
-        for (int b = 0; b < kStageBufs; ++b) mbar_init(&bars[b], 1);
+        for (int b = 0; b < kStageBufs; ++b) {
+            mbar_init(&full[b], 1);
+            mbar_init(&empty[b], 1);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    unsigned consumed = 0;   // segments this CTA has consumed (uniform)
+    unsigned gseg = 0;   // segments staged and consumed by this CTA so far (uniform)
     for (;;) {
-        if (cr == 0 && tid == 0) {
+        if (tid == 0) {
             const int t = atomicAdd(op.ticket, 1);
-            if (t == op.ntasks + nclusters - 1) atomicExch(op.ticket, 0);
-            unsigned go = 0;
+            if (t == op.ntasks + int(gridDim.x) - 1) atomicExch(op.ticket, 0);
+            int go = 0;
             if (t < op.ntasks) {
                 const GroupTask gt = op.tasks[t];
                 go = !skip_system(sv.st[gt.sys], op.skip) && !*(volatile int*)sv.err;
             }
-            for (unsigned q = 0; q < C; ++q) {
-                st_cluster(map_rank(&s_task, q), unsigned(t));
-                st_cluster(map_rank(&s_go, q), go);
-            }
+            s_task = t;
+            s_go = go;
         }
-        if (C > 1) cluster_sync(); else __syncthreads();
-        const int t = int(s_task);
-        const bool go = s_go != 0;
-        GroupTask gt = {0, 0, 0, 0};
-        if (t < op.ntasks && go) gt = op.tasks[t];
-        const bool mine = int(cr) < gt.count;
-        const SysDesc& d = sv.desc[gt.sys];
-        const TriFactor& F = op.which == 0 ? d.L : d.U;
-        const int pos = gt.pos0 + int(cr);
-        const int B = F.chunk_rows;
-        const int r0 = mine ? (op.which == 0 ? pos : F.nch - 1 - pos) * B : 0;
-        const int nr = mine ? min(d.n - r0, B) : 0;
-        const bool has_pred = op.inbox && mine && cr >= 1;
-        const bool push = op.inbox && int(cr) + 1 < gt.count;
-        const int r0p = op.which == 0 ? r0 - B : r0 + B;       // predecessor chunk's rows
-        const int nrp = has_pred ? min(d.n - r0p, B) : 0;
-        const int s0 = mine ? F.cseg[pos] : 0, nseg = mine ? F.cseg[pos + 1] - s0 : 0;
-        SegRec ahead;   // thread 0: the next segment to stage
-        if (tid == 0) {
-            for (int i = 0; i < kStageBufs - 1 && i < nseg; ++i) {
-                const SegRec sg = F.segs[s0 + i];
-                const unsigned b = (consumed + i) % kStageBufs;
-                s_nw[b] = sg.nw;
-                stage_segment<S>(F, sg, stage + b * sbytes, op.rows_cap, op.ents_cap, &bars[b]);
-            }
-            if (kStageBufs - 1 < nseg) ahead = F.segs[s0 + kStageBufs - 1];
-        }
-        T* y = mine ? vptr<T>(d, op.out) : nullptr;
-        T* R = mine && op.reset != SLOT_NONE ? vptr<T>(d, op.reset) : nullptr;
-        if (mine) {
-            const T* v = vptr<T>(d, op.in);
-            for (int i = tid; i < nr; i += NT) yl[i] = v[r0 + i];
-        }
-        if (op.inbox)
-            for (int i = tid; i < B; i += NT) inbox[i] = sentinel_value<T>();
-        if (C > 1) cluster_sync(); else __syncthreads();
+        __syncthreads();
+        const int t = s_task, go = s_go;
+        __syncthreads();
         if (t >= op.ntasks) break;
-        if (!mine) continue;
-        const unsigned rpush = push ? map_rank(inbox, cr + 1) : 0u;
-        for (int i = 0; i < nseg; ++i) {
-            const unsigned g = consumed + i, b = g % kStageBufs;
-            if (tid == 0 && i + kStageBufs - 1 < nseg) {
-                // buffer of segment i - 1, released by the barrier that ended it
-                const unsigned bn = (g + kStageBufs - 1) % kStageBufs;
-                s_nw[bn] = ahead.nw;
-                stage_segment<S>(F, ahead, stage + bn * sbytes, op.rows_cap, op.ents_cap, &bars[bn]);
-                if (i + kStageBufs < nseg) ahead = F.segs[s0 + i + kStageBufs];
+        if (!go) continue;
+        const GroupTask gt = op.tasks[t];
+        const SysDesc& d = sv.desc[gt.sys];
+        const TriFactor& TF = op.which == 0 ? d.L : d.U;
+        const ChunkArrays F = {TF.segs, TF.wv, TF.crow, TF.cdia, TF.ccol, TF.cval};
+        const int pos = gt.pos0;
+        const int B = TF.chunk_rows;
+        const int r0 = (op.which == 0 ? pos : TF.nch - 1 - pos) * B;
+        const int nr = min(d.n - r0, B);
+        const int s0 = TF.cseg[pos], nseg = TF.cseg[pos + 1] - s0;
+        const int x0 = TF.cxr[pos], nx = TF.cxr[pos + 1] - x0;
+        const int* cext = TF.cext;
+        T* ypos = static_cast<T*>(TF.ypos);
+        // chunk prologue (all threads): right-hand sides, empty receive slots,
+        // this chunk's share of the other factor's result reset
+        {
+            const T* v = vptr<T>(d, op.in);
+            for (int i = tid; i < nr; i += NTH) vec[i] = v[r0 + i];
+            if (tid == 0) vec[B] = T(0);
+            for (int i = tid; i < nx; i += NTH) vec[B + 1 + i] = sentinel_value<T>();
+            T* yr = static_cast<T*>(TF.ypos_reset);
+            const long long a = (long long)TF.npos_reset * pos / TF.nch, e = (long long)TF.npos_reset * (pos + 1) / TF.nch;
+            for (long long i = a + tid; i < e; i += NTH) yr[i] = sentinel_value<T>();
+        }
+        __syncthreads();
+        if (tid >= NT + 32) {
+            // producer warp: stage the chunk's segments (lane 0)
+            if (tid == NT + 32) {
+                for (int i = 0; i < nseg; ++i) {
+                    const unsigned g = gseg + i, b = g % kStageBufs;
+                    const SegRec sg = F.segs[s0 + i];
+                    if (g >= unsigned(kStageBufs)) mbar_wait(&empty[b], ((g / kStageBufs) + 1) & 1u, sv.err);
+                    s_nw[b] = sg.nw;
+                    s_p0[b] = sg.p0;
+                    stage_segment<S>(F, sg, stage + b * sbytes, op.rows_cap, op.ents_cap, &full[b]);
+                }
             }
-            mbar_wait(&bars[b], (g / kStageBufs) & 1u, sv.err);
-            const unsigned char* buf = stage + b * sbytes;
-            const unsigned* swv = reinterpret_cast<const unsigned*>(buf);
-            const int* srow = reinterpret_cast<const int*>(buf + op.rows_cap * 4);
-            const S* sdia = reinterpret_cast<const S*>(buf + op.rows_cap * 8);
-            const int* scol = reinterpret_cast<const int*>(buf + op.rows_cap * (8 + int(sizeof(S))));
-            const S* sval = reinterpret_cast<const S*>(buf + op.rows_cap * (8 + int(sizeof(S))) + op.ents_cap * 4);
-            const int nwaves = s_nw[b];
-            int poff = 0, eoff = 0;
-            WaveRow<S, KM> cur, nxt;
-            wave_row<S, KM>(swv, srow, sdia, scol, sval, 0, 0, 0, tid, cur);
-            for (int w = 0; w < nwaves; ++w) {
+        } else if (tid >= NT) {
+            // receiver warp
+            receive_chunk<T>(cext, x0, nx, ypos, vec + B + 1, tid - NT, sv.err, op.sleep_ns);
+        } else {
+            // compute threads: all waves of the chunk, one cursor across segments
+            unsigned g = gseg, b = g % kStageBufs;
+            mbar_wait(&full[b], (g / kStageBufs) & 1u, sv.err);
+            StageView<S> V(stage + b * sbytes, op.rows_cap, op.ents_cap);
+            int si = 0, nws = s_nw[b], p0 = s_p0[b];
+            int w = 0, poff = 0, eoff = 0;
+            unsigned m = V.wv[0];
+            WaveRow<T, S, KM> cur, nxt;
+            wave_row<T, S, KM>(m, V.row, V.dia, V.col, V.val, vec, B, r0, 0, 0, tid, cur);
+            for (;;) {
+                // locate and load the next wave (possibly the next segment's first)
+                const int nw = int(m & 0x7FFFu);
+                const int poff_n = poff + nw, eoff_n = eoff + int(m >> 16) * nw;
+                bool has_next = true, cross = false;
+                unsigned mn = 0u;
+                StageView<S> Vn = V;
+                unsigned gn = g, bn = b;
+                int pn = poff_n, en = eoff_n;
+                if (w + 1 < nws) {
+                    mn = V.wv[w + 1];
+                } else if (si + 1 < nseg) {
+                    cross = true;
+                    gn = g + 1;
+                    bn = gn % kStageBufs;
+                    mbar_wait(&full[bn], (gn / kStageBufs) & 1u, sv.err);
+                    Vn = StageView<S>(stage + bn * sbytes, op.rows_cap, op.ents_cap);
+                    mn = Vn.wv[0];
+                    pn = en = 0;
+                } else {
+                    has_next = false;
+                }
+                if (has_next) wave_row<T, S, KM>(mn, Vn.row, Vn.dia, Vn.col, Vn.val, vec, B, r0, pn, en, tid, nxt);
                 if (cur.row >= 0) {
-                    // all in-chunk reads at once, then the waits on earlier chunks
-                    T rr = yl[cur.row - r0];
+                    // all of the row's reads at once (chunk rows, the +0 cell and
+                    // receive slots are cells of one shared vector); waits only
+                    // for slots the receiver has not filled yet
                     T dv[KM];
-                    bool ext = false;
-#pragma unroll
-                    for (int k = 0; k < KM; ++k) {
-                        const unsigned lc = unsigned(cur.col[k] - r0);
-                        dv[k] = T(0);
-                        if (lc < unsigned(nr)) dv[k] = yl[lc];
-                        else if (cur.col[k] >= 0) ext = true;
-                    }
-                    if (ext) {
+                    bool wait = false;
+                    if (!(m & kWaveOverflow)) {
 #pragma unroll
                         for (int k = 0; k < KM; ++k) {
-                            const int col = cur.col[k];
-                            if (col >= 0 && unsigned(col - r0) >= unsigned(nr)) {
-                                const unsigned lp = unsigned(col - r0p);
-                                dv[k] = lp < unsigned(nrp) ? poll_inbox(inbox + lp, sv.err)
-                                                           : poll_value(y + col, sv.err, op.sleep_ns);
+                            dv[k] = vec[cur.col[k]];
+                            wait |= is_sentinel(dv[k]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < KM; ++k) {
+                            dv[k] = cur.col[k] >= 0 ? vec[cur.col[k]] : sentinel_value<T>();
+                            wait |= is_sentinel(dv[k]);
+                        }
+                    }
+                    if (wait) {
+#pragma unroll
+                        for (int k = 0; k < KM; ++k) {
+                            if (is_sentinel(dv[k])) {
+                                const int c = cur.col[k];
+                                dv[k] = c >= 0 ? poll_slot(vec + c, sv.err) : poll_value(ypos + (-c - 2), sv.err, op.sleep_ns);
                             }
                         }
                     }
+                    T rr = cur.rhs;
 #pragma unroll
-                    for (int k = 0; k < KM; ++k)
-                        if (cur.col[k] >= 0) rr = sweep_step<T, S>(rr, cur.val[k], dv[k]);
+                    for (int k = 0; k < KM; ++k) rr = sweep_step<T, S>(rr, cur.val[k], dv[k]);
                     const T out = unsentinel(T(W(rr) * W(cur.dia)));
-                    yl[cur.row - r0] = out;
-                    if (push) st_cluster(rpush + unsigned(cur.row - r0) * unsigned(sizeof(T)), out);
-                    st_relaxed_gpu(y + cur.row, out);
-                    if (R) R[cur.row] = sentinel_value<T>();
+                    vec[cur.row - r0] = out;
+                    st_relaxed_gpu(ypos + p0 + poff + tid, out);
                 }
-                poff += cur.nw;
-                eoff += cur.K * cur.nw;
-                if (w + 1 < nwaves) wave_row<S, KM>(swv, srow, sdia, scol, sval, w + 1, poff, eoff, tid, nxt);
-                __syncthreads();
+                compute_barrier(NT);
+                if (!has_next) break;
+                if (cross) {
+                    // every compute thread has read its last row of buffer b
+                    if (tid == 0) mbar_arrive(&empty[b]);
+                    g = gn;
+                    b = bn;
+                    V = Vn;
+                    ++si;
+                    nws = s_nw[b];
+                    p0 = s_p0[b];
+                    w = 0;
+                    poff = eoff = 0;
+                } else {
+                    ++w;
+                    poff = poff_n;
+                    eoff = eoff_n;
+                }
+                m = mn;
                 cur = nxt;
             }
+            // last segment's buffer
+            if (tid == 0) mbar_arrive(&empty[b]);
+            // chunk epilogue: outputs and the reset of the buffer the other sweep fills
+            compute_barrier(NT);
+            T* y = vptr<T>(d, op.out);
+            T* R = op.reset != SLOT_NONE ? vptr<T>(d, op.reset) : nullptr;
+            for (int i = tid; i < nr; i += NT) {
+                y[r0 + i] = vec[i];
+                if (R) R[r0 + i] = sentinel_value<T>();
+            }
         }
-        consumed += unsigned(nseg);
+        gseg += unsigned(nseg);
+        __syncthreads();
     }
 }
 
@@ -647,13 +754,14 @@ __global__ void __launch_bounds__(kBlock) k_ic0_factor(FactorOp op)
 }
 
 // Level-ordered factor values: val[e] = S(src[idx[e]] * (mul[e] >= 0 ?
-// inv_dia[mul[e]] : 1)); dia[k] = S(row_of[k] >= 0 && dia_mode ? inv_dia[row] : 1).
+// inv_dia[mul[e]] : 1)) (+0 where idx[e] < 0); dia[k] = S(row_of[k] >= 0 &&
+// dia_mode ? inv_dia[row] : 1).
 __global__ void k_fill_factor(int nent, const int* __restrict__ idx, const int* __restrict__ mul,
                               const double* __restrict__ src, const double* __restrict__ inv_dia, void* val,
                               int val_f32)
 {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nent; e += gridDim.x * blockDim.x) {
-        double v = src[idx[e]];
+        double v = idx[e] >= 0 ? src[idx[e]] : 0.0;   // idx < 0: padding, value +0
         if (mul[e] >= 0) v = v * inv_dia[mul[e]];
         if (val_f32) static_cast<float*>(val)[e] = float(v);
         else static_cast<double*>(val)[e] = v;

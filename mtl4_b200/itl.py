@@ -95,7 +95,7 @@ class pc:
             out = (C.c_int * 8)()
             dt = _lib.F32 if np.dtype(dtype) == np.float32 else _lib.F64
             check(self.ctx._L.mtlg_pc_sweep_plan(self.ctx.h, self.h, dt, out), "sweep_plan")
-            keys = ("chunk_rows", "chunks", "cluster", "clusters_resident", "smem", "threads", "entries", "inbox")
+            keys = ("chunk_rows", "chunks", "resident", "smem", "threads", "entries", "seg_rows", "seg_ents")
             return dict(zip(keys, list(out)))
 
         def factor(self, which: str):
