@@ -88,6 +88,7 @@ struct __align__(16) SegRec {
 };
 
 constexpr unsigned kWaveOverflow = 0x8000u;   // wave reads rows of earlier chunks beyond the receive slots
+constexpr int kSlotBase = 4;                  // receive slots start at shared cell chunk_rows + kSlotBase (16-byte aligned)
 
 // Level-ordered triangular factor (device pointers).  Row k of the factor is
 // original row `row_of[k]` (-1 marks padding that aligns levels to warps);
@@ -108,13 +109,14 @@ struct TriFactor {
     // row sits at k * rows + t after the wave's first entry.  Columns are
     // coded as cells of the chunk's shared vector (B = chunk_rows): c < B a
     // row of the chunk, c == B a cell holding +0 (entries past a row's own,
-    // with value +0: exactly neutral in the row's arithmetic), c > B receive
-    // slot c - B - 1, filled by the receiver warp with a row of an earlier
-    // chunk (cext lists those rows' positions per chunk, in slot order);
-    // c < 0 a row of an earlier chunk at position -c - 2, read directly (its
-    // wave carries kWaveOverflow).  Results cross chunks through ypos, in
-    // position order (a wave's results are contiguous).  Every segment starts
-    // 16-byte aligned in every array.
+    // with value +0: exactly neutral in the row's arithmetic), c >= B +
+    // kSlotBase receive slot c - B - kSlotBase, filled by the receiver warps
+    // with a row of an earlier chunk (cext lists those rows' positions per
+    // chunk, in slot order, each chunk's list 4-aligned); c < 0 a row of an
+    // earlier chunk at position -c - 2, read directly (its wave carries
+    // kWaveOverflow).  Results cross chunks through ypos, in position order
+    // (a wave's results are contiguous, starting 4-aligned).  Every segment
+    // starts 16-byte aligned in every array.
     int chunk_rows;    // 0: no chunked layout
     int nch;
     int seg_rows;      // rows per segment, at most
@@ -124,7 +126,8 @@ struct TriFactor {
     const unsigned* wv;// [waves] rows | kWaveOverflow | entries per row << 16
     const int* crow;   // row at each position
     const int* cxr;    // [nch + 1] receive-slot range of each chunk in cext
-    const int* cext;   // positions of earlier chunks' rows, per chunk in slot order
+    const int* cext;   // positions of earlier chunks' rows, per chunk in slot order (-1: unused slot)
+    const int2* cquad; // per 4 slots: {first of 4 consecutive positions or -1, mask of used slots}
     void* ypos;        // results by position (T), all sentinel before the sweep
     void* ypos_reset;  // the other factor's results by position: reset to the sentinel by this sweep
     int npos, npos_reset;

@@ -32,6 +32,7 @@ struct TriDev {
     int seg_ents = 0;   // entries per segment, at most
     int max_slots = 0;  // receive slots of a chunk, at most
     DBuf<int> cseg, cxr, cext, crow, ccol, csrc, cmul;
+    DBuf<int2> cquad;
     DBuf<SegRec> segs;
     DBuf<unsigned> wv;
     DBuf<unsigned char> cval, cdia;    // storage type S
@@ -50,11 +51,12 @@ inline int entries_bucket(int k) { return k <= 2 ? 2 : k <= 3 ? 3 : k <= 4 ? 4 :
 // and seg_ents entries; entries wave-major as described at TriFactor.  The
 // columns are coded as cells of the chunk's shared vector: a row of the
 // chunk as its index in the chunk, B (a cell holding +0, with value 0) past a
-// row's entries, B + 1 + slot for the first B entries of a chunk whose row
-// lies in an earlier chunk (in wave order; that row's position listed in
-// cext, where the chunk's receiver warp fetches it from the position-ordered
-// results); any further ones as -(position + 2), polled directly, their wave
-// flagged with kWaveOverflow.
+// row's entries, B + kSlotBase + slot for entries whose row lies in an
+// earlier chunk, up to B slots per chunk (in wave order; that row's position
+// listed in cext, where the chunk's receiver warps fetch it from the
+// position-ordered results); any further ones as -(position + 2), polled
+// directly, their wave flagged with kWaveOverflow.  Waves start 4-aligned in
+// positions, and in slots when they read several earlier-chunk rows.
 inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& lev, int n, bool lower, int B,
                         TriDev& T)
 {
@@ -125,8 +127,21 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
             const int nw = qe - q;
             int K = 0;
             for (int j = q; j < qe; ++j) K = std::max(K, F.rp[order[j] + 1] - F.rp[order[j]]);
-            if (open && (int(crow.size()) - cur.p0 + nw > SR || int(ccol.size()) - cur.e0 + K * nw > SE)) close_seg();
+            // a wave's positions start 4-aligned
+            if (open && (round4(int(crow.size())) - cur.p0 + nw > SR || int(ccol.size()) - cur.e0 + K * nw > SE))
+                close_seg();
             if (!open) open_seg();
+            crow.resize(round4(int(crow.size())), -1);
+            // a wave with several earlier-chunk reads starts its receive slots
+            // 4-aligned too, so runs of consecutive positions move 4 at a time
+            int next = 0;
+            for (int j = q; j < qe; ++j)
+                for (int e = F.rp[order[j]]; e < F.rp[order[j] + 1]; ++e) next += (F.col[e] < r0 || F.col[e] >= r1);
+            if (next >= 4 && round4(nslot) < B)
+                while (nslot % 4) {
+                    cext.push_back(-1);
+                    ++nslot;
+                }
             const size_t wvi = wv.size();
             wv.push_back(unsigned(nw) | (unsigned(K) << 16));
             bool ovf = false;
@@ -148,7 +163,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
                         code = col - r0;                 // row of this chunk
                     } else if (nslot < B) {
                         cext.push_back(pos_of[col]);     // earlier chunk: receive slot
-                        code = B + 1 + nslot;
+                        code = B + kSlotBase + nslot;
                         ++nslot;
                     } else {
                         code = -(pos_of[col] + 2);       // earlier chunk beyond the slots: polled directly
@@ -163,9 +178,28 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
             q = qe;
         }
         close_seg();
+        while (cext.size() % 4) cext.push_back(-1);
+        nslot = round4(nslot);
         cseg.push_back(int(segs.size()));
         cxr.push_back(int(cext.size()));
         T.max_slots = std::max(T.max_slots, nslot);
+    }
+    // receive quads (slots 4q .. 4q+3): {first position, mask of used slots};
+    // first position -1 where the used slots are not four consecutive
+    // positions starting 4-aligned (fetched one by one)
+    std::vector<int2> cquad(cext.size() / 4 + 1, make_int2(-1, 0));
+    for (size_t q = 0; q < cext.size() / 4; ++q) {
+        int mask = 0, p = -2;
+        bool vec = true;
+        for (int j = 0; j < 4; ++j) {
+            const int x = cext[4 * q + j];
+            if (x < 0) continue;
+            mask |= 1 << j;
+            if (p == -2) p = x - j;
+            if (x != p + j) vec = false;
+        }
+        if (p < 0 || p % 4) vec = false;
+        cquad[q] = make_int2(vec && mask ? p : -1, mask);
     }
     // tails: a staged copy rounds each array's segment up to 16 bytes
     wv.resize(round4(int(wv.size())) + 4, 0u);
@@ -188,6 +222,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     MTLG_TRY(T.cseg.upload(c, cseg.data(), cseg.size()));
     MTLG_TRY(T.cxr.upload(c, cxr.data(), cxr.size()));
     MTLG_TRY(T.cext.upload(c, cext.data(), cext.size()));
+    MTLG_TRY(T.cquad.upload(c, cquad.data(), cquad.size()));
     MTLG_TRY(T.segs.upload(c, segs.data(), segs.size()));
     MTLG_TRY(T.wv.upload(c, wv.data(), wv.size()));
     MTLG_TRY(T.crow.upload(c, crow.data(), crow.size()));
@@ -220,7 +255,7 @@ struct ChunkPlan {
         km = std::max(km, T.kmax);
         rows = std::max(rows, T.chunk_rows);
         slots = std::max(slots, T.max_slots);
-        cells = std::max(cells, T.chunk_rows + 1 + T.max_slots);
+        cells = std::max(cells, T.chunk_rows + kSlotBase + T.max_slots);
         seg_rows = std::max(seg_rows, T.seg_rows);
         seg_ents = std::max(seg_ents, T.seg_ents);
     }
@@ -367,6 +402,7 @@ inline TriFactor tri_view(const TriDev& T)
         f.crow = T.crow.p;
         f.cxr = T.cxr.p;
         f.cext = T.cext.p;
+        f.cquad = T.cquad.p;
         f.ccol = T.ccol.p;
         f.cval = T.cval.p;
         f.cdia = T.cdia.p;

@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
 //    earlier waves, made visible by a named barrier between waves), and its
 //    result is published in position order (one coalesced store per warp and
 //    wave) for later chunks;
-//  - the receiver warp fetches the results of earlier chunks this chunk
+//  - kRecvWarps receiver warps fetch the results of earlier chunks this chunk
 //    needs, in the order the waves consume them, many requests in flight,
 //    into receive slots in shared memory, so a compute thread waits on the
 //    value itself, never on an L2 round trip of its own;
@@ -169,8 +169,9 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
 // (kSpinLimit polls, then a timeout flag and a drain).  The arithmetic per
 // row is k_sweep's (same entry order, same roundings).
 constexpr int kStageBufs = 3;
-constexpr int kRecvDepth = 4;         // receive requests in flight per receiver lane
-constexpr int kChunkExtraWarps = 2;   // receiver and producer warps after the NT compute threads
+constexpr int kRecvDepth = 2;                       // receive quads in flight per receiver lane
+constexpr int kRecvWarps = 4;                       // receiver warps
+constexpr int kChunkExtraWarps = kRecvWarps + 1;    // receiver warps and the producer warp after the NT compute threads
 
 struct ChunkSweepOp {
     const GroupTask* tasks;
@@ -301,7 +302,7 @@ __device__ __forceinline__ void st_relaxed_gpu(double* p, double v)
 {
     asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v));
 }
-// receive slots: written by the receiver warp, polled by the compute threads
+// receive slots: written by the receiver warps, polled by the compute threads
 __device__ __forceinline__ float ld_slot(const float* p)
 {
     float v;
@@ -358,42 +359,93 @@ __device__ __noinline__ T poll_slot(const T* p, int* err)
     return w;
 }
 
-// Receiver warp: fetches ypos[cext[x0 + e]] into slot[e] for e < nx, in slot
-// order, kRecvDepth requests in flight per lane.  A value that is still the
-// sentinel is requested again; the wait is bounded like the others (on
-// expiry the slot gets a zero so the compute threads drain).
-template <typename T>
-__device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, int x0, int nx, const T* ypos, T* slot,
-                                              int lane, int* err, int sleep_ns)
+// 4 consecutive results (16-byte aligned for float, 32 for double), relaxed.
+__device__ __forceinline__ void ld_relaxed_gpu4(const float* p, float* v)
 {
-    for (int base = lane; base < nx; base += 32 * kRecvDepth) {
-        int src[kRecvDepth];
-        bool pending[kRecvDepth];
+    asm volatile("ld.relaxed.gpu.global.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+                 : "l"(p));
+}
+__device__ __forceinline__ void ld_relaxed_gpu4(const double* p, double* v)
+{
+    asm volatile("ld.relaxed.gpu.global.v2.f64 {%0, %1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "l"(p));
+    asm volatile("ld.relaxed.gpu.global.v2.f64 {%0, %1}, [%2];" : "=d"(v[2]), "=d"(v[3]) : "l"(p + 2));
+}
+__device__ __forceinline__ void st_slot4(float* p, const float* v)
+{
+    asm volatile("st.volatile.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(smem_u32(p)), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+                 "f"(v[3]));
+}
+__device__ __forceinline__ void st_slot4(double* p, const double* v)
+{
+    asm volatile("st.volatile.shared.v2.f64 [%0], {%1, %2};" ::"r"(smem_u32(p)), "d"(v[0]), "d"(v[1]));
+    asm volatile("st.volatile.shared.v2.f64 [%0], {%1, %2};" ::"r"(smem_u32(p + 2)), "d"(v[2]), "d"(v[3]));
+}
+
+// Receiver warps: fill slot[e] = ypos[cext[x0 + e]] for the chunk's nx slots
+// (x0, nx multiples of 4), four slots (a quad) at a time, in slot order.
+// Quads go in rows of 32 (lane l holds quad l of a row, so a row's loads
+// coalesce); receiver warp rw of kRecvWarps takes rows rw, rw + kRecvWarps,
+// ..., kRecvDepth of them at a time, and moves to its next batch when the
+// batch is complete.  A quad whose used slots are 4 consecutive aligned
+// positions moves with one vector load; the others slot by slot.  A value
+// that is still the sentinel is requested again (the slot keeps the sentinel
+// meanwhile); the wait is bounded like the others (on expiry the remaining
+// slots get a zero so the compute threads drain).
+template <typename T>
+__device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, const int2* __restrict__ cquad, int x0,
+                                              int nx, const T* ypos, T* slot, int rw, int lane, int* err,
+                                              int sleep_ns)
+{
+    const int q0 = x0 >> 2, nq = nx >> 2;
+    for (int row0 = rw; 32 * row0 < nq; row0 += kRecvWarps * kRecvDepth) {
+        int qd[kRecvDepth];
+        int2 qi[kRecvDepth];
+        unsigned pend[kRecvDepth];
 #pragma unroll
         for (int j = 0; j < kRecvDepth; ++j) {
-            const int e = base + 32 * j;
-            pending[j] = e < nx;
-            src[j] = pending[j] ? __ldg(cext + x0 + e) : 0;
+            qd[j] = 32 * (row0 + kRecvWarps * j) + lane;
+            pend[j] = 0;
+            if (qd[j] < nq) {
+                qi[j] = __ldg(cquad + q0 + qd[j]);
+                pend[j] = unsigned(qi[j].y);
+            }
         }
         long long spins = 0;
         for (;;) {
-            T v[kRecvDepth];
-#pragma unroll
-            for (int j = 0; j < kRecvDepth; ++j)
-                if (pending[j]) v[j] = ld_relaxed_gpu(ypos + src[j]);
-            bool any = false;
+            T v[kRecvDepth][4];
 #pragma unroll
             for (int j = 0; j < kRecvDepth; ++j) {
-                if (pending[j]) {
-                    if (!is_sentinel(v[j])) {
-                        st_slot(slot + base + 32 * j, v[j]);
-                        pending[j] = false;
-                    } else {
-                        any = true;
-                    }
+                if (!pend[j]) continue;
+                if (qi[j].x >= 0) {
+                    ld_relaxed_gpu4(ypos + qi[j].x, v[j]);
+                } else {
+                    const int e = x0 + 4 * qd[j];
+#pragma unroll
+                    for (int l = 0; l < 4; ++l)
+                        v[j][l] = (pend[j] >> l) & 1u ? ld_relaxed_gpu(ypos + __ldg(cext + e + l)) : sentinel_value<T>();
                 }
             }
-            if (!any) break;
+            unsigned left = 0;
+#pragma unroll
+            for (int j = 0; j < kRecvDepth; ++j) {
+                if (!pend[j]) continue;
+                T* dst = slot + 4 * qd[j];
+                unsigned ready = 0;
+#pragma unroll
+                for (int l = 0; l < 4; ++l)
+                    if (((pend[j] >> l) & 1u) && !is_sentinel(v[j][l])) ready |= 1u << l;
+                if (qi[j].x >= 0) {
+                    if (ready) st_slot4(dst, v[j]);   // not-ready lanes store the sentinel they hold
+                } else {
+#pragma unroll
+                    for (int l = 0; l < 4; ++l)
+                        if ((ready >> l) & 1u) st_slot(dst + l, v[j][l]);
+                }
+                pend[j] &= ~ready;
+                left |= pend[j];
+            }
+            if (!left) break;
             if ((++spins & 255) == 0 && *(volatile int*)err) break;
             if (spins > kSpinLimit) {
                 atomicExch(err, 1);
@@ -403,7 +455,9 @@ __device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, int 
         }
 #pragma unroll
         for (int j = 0; j < kRecvDepth; ++j)
-            if (pending[j]) st_slot(slot + base + 32 * j, T(0));
+#pragma unroll
+            for (int l = 0; l < 4; ++l)
+                if ((pend[j] >> l) & 1u) st_slot(slot + 4 * qd[j] + l, T(0));
     }
 }
 
@@ -475,7 +529,7 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
     __shared__ int s_task, s_go;
     __shared__ int s_nw[kStageBufs], s_p0[kStageBufs];
     typedef typename std::conditional<(sizeof(S) > sizeof(T)), S, T>::type W;   // promoted type
-    T* vec = reinterpret_cast<T*>(chunk_smem);   // [chunk rows | +0 cell | receive slots]
+    T* vec = reinterpret_cast<T*>(chunk_smem);   // [chunk rows | +0 cell, kSlotBase - 1 unused | receive slots]
     unsigned char* stage = chunk_smem + op.vec_bytes;
     const int sbytes = stage_bytes<S>(op.rows_cap, op.ents_cap);
     const int tid = threadIdx.x;
@@ -524,15 +578,15 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
             const T* v = vptr<T>(d, op.in);
             for (int i = tid; i < nr; i += NTH) vec[i] = v[r0 + i];
             if (tid == 0) vec[B] = T(0);
-            for (int i = tid; i < nx; i += NTH) vec[B + 1 + i] = sentinel_value<T>();
+            for (int i = tid; i < nx; i += NTH) vec[B + kSlotBase + i] = sentinel_value<T>();
             T* yr = static_cast<T*>(TF.ypos_reset);
             const long long a = (long long)TF.npos_reset * pos / TF.nch, e = (long long)TF.npos_reset * (pos + 1) / TF.nch;
             for (long long i = a + tid; i < e; i += NTH) yr[i] = sentinel_value<T>();
         }
         __syncthreads();
-        if (tid >= NT + 32) {
+        if (tid >= NT + 32 * kRecvWarps) {
             // producer warp: stage the chunk's segments (lane 0)
-            if (tid == NT + 32) {
+            if (tid == NT + 32 * kRecvWarps) {
                 for (int i = 0; i < nseg; ++i) {
                     const unsigned g = gseg + i, b = g % kStageBufs;
                     const SegRec sg = F.segs[s0 + i];
@@ -543,8 +597,9 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
                 }
             }
         } else if (tid >= NT) {
-            // receiver warp
-            receive_chunk<T>(cext, x0, nx, ypos, vec + B + 1, tid - NT, sv.err, op.sleep_ns);
+            // receiver warps
+            receive_chunk<T>(cext, TF.cquad, x0, nx, ypos, vec + B + kSlotBase, (tid - NT) >> 5, tid & 31, sv.err,
+                             op.sleep_ns);
         } else {
             // compute threads: all waves of the chunk, one cursor across segments
             unsigned g = gseg, b = g % kStageBufs;
@@ -558,7 +613,7 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
             for (;;) {
                 // locate and load the next wave (possibly the next segment's first)
                 const int nw = int(m & 0x7FFFu);
-                const int poff_n = poff + nw, eoff_n = eoff + int(m >> 16) * nw;
+                const int poff_n = (poff + nw + 3) & ~3, eoff_n = eoff + int(m >> 16) * nw;   // waves start 4-aligned
                 bool has_next = true, cross = false;
                 unsigned mn = 0u;
                 StageView<S> Vn = V;
