@@ -39,6 +39,9 @@ METRIC = "solves/s at relres<=1e-8, mixed vs plain FP64 on B200; SpMV %HBM; p99 
 WORKLOAD = ("BiCGSTAB+ILU(0) on 128^3 7-point convection-diffusion (2,097,152 unknowns, 14,581,760 nnz, "
             "beta=(0.5,0.3,0.2), h=1/129), b=A*x_true seed 1, relres<=1e-8")
 PEAKS = ROOT / "MEASURED_PEAKS.json"
+# DRAM bytes (read + write) of one FP32 ILU(0) apply (L and U k_sweep_chunk
+# launches) from ncu on this workload; see profiles/k_sweep_chunk_ilu0_convdiff128_f32.md
+TRAFFIC_PER_APPLY = 203_350_000   # 101.0 MB (L) + 102.3 MB (U)
 FALLBACK_HBM = 6650.0
 
 
@@ -301,8 +304,10 @@ def main():
     x_tight = xd.numpy()
     err_vs_fp64 = float(np.abs(x_mixed - x_tight).max() / np.abs(x_tight).max())
 
-    # dominant kernel: the level-scheduled sweeps of the FP32 ILU(0) apply,
-    # timed with events on the launching stream
+    # dominant kernel: the chunked triangular sweeps of the FP32 ILU(0)
+    # apply (k_sweep_chunk, L then U), timed with events on the launching
+    # stream; the applies are queued back to back (pc_apply_sync = 0), then
+    # one synchronous apply reports any expired device wait
     bf = mtl.dense_vector(b.astype(np.float32), np.float32, ctx)
     yf = mtl.dense_vector(n, np.float32, ctx)
     for _ in range(3):
@@ -310,12 +315,17 @@ def main():
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = 20
+    ctx.set_tuning("pc_apply_sync", 0)
     e0.record(stream)
     for _ in range(reps):
         itl.solve(P32, bf, yf)
     e1.record(stream)
     torch.cuda.synchronize()
+    ctx.set_tuning("pc_apply_sync", 1)
+    itl.solve(P32, bf, yf)
     apply_s = e0.elapsed_time(e1) * 1e-3 / reps
+    lev_L, lev_U = P32.levels()
+    plan = P32.sweep_plan(np.float32)
     Lr, Lc, Lv = P32.factor("L")
     Ur, Uc, Uv = P32.factor("U")
     # algorithmic bytes of one apply (two sweeps), FP32 values, int32 indices:
@@ -361,10 +371,13 @@ def main():
         "mixed_over_fp64": value / v64,
         "spmv": {"matrix": f"power-law CSR {Q.n_rows} rows, {Q.nnz} nnz", "us": spmv_s * 1e6, "GBs": spmv_gbs,
                  "frac_measured_peak": spmv_gbs / peak, "frac_8TBs_nominal": spmv_gbs / 8000.0},
-        "roofline": {"kernel": "k_sweep<float,float> (ILU(0) L and U sweeps, one apply)", "bound": "hbm",
+        "roofline": {"kernel": "k_sweep_chunk<float,float> (ILU(0) L and U sweeps, one apply)", "bound": "hbm",
                      "achieved": sweep_gbs, "peak": peak, "unit": "GB/s", "frac": sweep_gbs / peak,
-                     "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_apply": bytes_apply,
-                     "apply_us": apply_s * 1e6},
+                     "peak_kind": peak_kind, "traffic": TRAFFIC_PER_APPLY,
+                     "algorithmic_bytes_per_apply": bytes_apply, "apply_us": apply_s * 1e6,
+                     "levels": lev_L + lev_U, "ns_per_level": apply_s * 1e9 / (lev_L + lev_U),
+                     "note": "dependency-latency bound: one level of the L or U chain per step",
+                     "plan": plan},
         "e2e": {"value": world * args.steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(launches),

@@ -130,7 +130,13 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * plain CUDA graphs, two in flight; 1: one graph with a WHILE conditional
  * node per solve), "spmv_kernel" (standalone SpMV: 0 chooses by row
  * lengths, 1 shared-memory stream tiles, 2 row-aligned warp tasks, 3 one
- * thread per row from global memory).
+ * thread per row from global memory), "sweep_kernel" (0: chunked sweeps,
+ * one CTA per chunk of rows, default; 1: flat level-order sweeps),
+ * "chunk_rows" (rows per chunk of preconditioners created afterwards; 0:
+ * 16384 for FP32 factors, 8192 for FP64), "pc_apply_sync" (1, default:
+ * mtlg_pc_apply waits for its sweeps and reports an expired device wait;
+ * 0: it only enqueues them, and an expired wait is reported by the next
+ * synchronous apply of the same preconditioner).
  * Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
 int mtlg_ctx_set_tuning(mtlg_ctx* ctx, const char* key, int64_t value);
 int mtlg_ctx_get_tuning(mtlg_ctx* ctx, const char* key, int64_t* value);

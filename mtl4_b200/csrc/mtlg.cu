@@ -160,6 +160,9 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
         if (op.ntasks) { k_sweep<T, S><<<grid, kBlock, 0, c->stream>>>(sv, op); c->launches++; }
     }
     MTLG_CUDA(cudaGetLastError());
+    // queued applies (pc_apply_sync = 0): an expired wait stays flagged on the
+    // device and is reported by the next synchronous apply of this preconditioner
+    if (!c->pc_apply_sync) return MTLG_OK;
     int err = 0;
     MTLG_CUDA(cudaMemcpyAsync(&err, P->misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     MTLG_CUDA(cudaStreamSynchronize(c->stream));
@@ -348,6 +351,7 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "spmv_kernel") c->spmv_kernel = int(std::max<int64_t>(0, std::min<int64_t>(value, 3)));
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
     else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
+    else if (k == "pc_apply_sync") c->pc_apply_sync = value ? 1 : 0;
     else if (k == "chunk_rows") c->chunk_rows = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 15)));
     else {
         set_error("unknown tuning key '%s'", key);
@@ -368,6 +372,7 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     else if (k == "sweep_sleep_ns") *value = c->sweep_sleep_ns;
     else if (k == "sm_count") *value = c->sm_count;
     else if (k == "sweep_kernel") *value = c->sweep_kernel;
+    else if (k == "pc_apply_sync") *value = c->pc_apply_sync;
     else if (k == "chunk_rows") *value = c->chunk_rows;
     else {
         set_error("unknown tuning key '%s'", key);
