@@ -174,6 +174,58 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ batched and served samples
+def batch_and_serve(ctx, n_batch=64, n_req=120, rate=20.0):
+    """Bounded samples of the batched and the served workloads: every 16th
+    of the 1,024 uneven systems (same size distribution) solved as one batch
+    (FP64, and FP32 inner / FP64 refinement), and the first n_req requests of
+    the 20,000-request stream under open-loop Poisson arrivals (p50 / p99 of
+    arrival -> result on the host, setup included)."""
+    import time as _t
+    from mtl4_b200 import problems as P
+    from mtl4_b200 import serve
+    out = {}
+    specs = P.batch_specs(1024)[::1024 // n_batch]
+    systems = [sp.build() for sp in specs]
+    rhs = [P.random_rhs(A.n_rows, sp.seed) for sp, A in zip(specs, systems)]
+    rows = int(sum(A.n_rows for A in systems))
+    for mixed in (False, True):
+        B = serve.batch(ctx)
+        for sp, A, b in zip(specs, systems, rhs):
+            B.add(A, b, sp.solver, sp.pc, max_iter=3000, rtol=1e-8)
+        ctx.synchronize()
+        t0 = _t.perf_counter()
+        B.solve(mixed=mixed, rtol=1e-8, inner_rtol=1e-4)
+        ctx.synchronize()
+        t1 = _t.perf_counter()
+        B.solve(mixed=mixed, rtol=1e-8, inner_rtol=1e-4)
+        ctx.synchronize()
+        t2 = _t.perf_counter()
+        res = [B.result(i) for i in range(len(systems))]
+        ok = sum(1 for r in res if r.error_code == 0)
+        worst = max(float(np.linalg.norm(A.matvec(r.x) - b) / np.linalg.norm(b))
+                    for A, b, r in zip(systems, rhs, res))
+        out["mixed" if mixed else "fp64"] = {
+            "systems": len(systems), "rows": rows, "converged": ok, "worst_relres": worst,
+            "solve_s": t2 - t1, "solves_per_s": len(systems) / (t2 - t1), "first_solve_with_setup_s": t1 - t0}
+        del B
+    rspecs = P.request_specs(20000)[:n_req]
+    reqs = []
+    for sp in rspecs:
+        A = sp.build()
+        reqs.append((A, P.random_rhs(A.n_rows, sp.seed), sp.solver, sp.pc, 3000))
+    arrivals = P.poisson_arrivals(n_req, rate)
+    srv = serve.server(ctx, max_active=64, iters_per_step=16, mixed=True, rtol=1e-8, inner_rtol=1e-4)
+    r = serve.run_open_loop(srv, reqs, arrivals, timeout_s=240.0)
+    ok = sum(1 for x in r["results"] if x is not None and x.error_code == 0)
+    out["served"] = {"requests": n_req, "rate_per_s": rate, "completed": r["completed"], "converged": ok,
+                     "rows": int(sum(q[0].n_rows for q in reqs)), "wall_s": r["wall_s"],
+                     "solves_per_s": r["solves_per_s"], "p50_s": r["p50_s"], "p99_s": r["p99_s"],
+                     "clock": "host, arrival -> result available (setup included)"}
+    del srv
+    return out
+
+
 # ------------------------------------------------------------------ profiling cases
 def run_kernel_case(args):
     """One kernel on its bench case, `reps` times (no timing output): the
@@ -216,6 +268,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mtl4_b200", choices=["mtl4_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the batched / served samples")
     ap.add_argument("--kernel", choices=["spmv_powerlaw", "spmv_stencil", "sweep_ilu0", "solve_mixed"],
                     help="run one kernel on its bench case a few times and exit (for profilers)")
     ap.add_argument("--reps", type=int, default=3)
@@ -383,6 +436,8 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    if not args.no_serve:
+        line["batched_and_served"] = batch_and_serve(ctx)
     if not args.no_cpu_baseline and world == 1:
         try:
             from oracle import oracle as O

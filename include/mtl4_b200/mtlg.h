@@ -70,7 +70,10 @@ enum {
     MTLG_ST_CONVERGED = 1,   /* resid <= rtol*norm_r0 or resid <= atol   error_code 0 */
     MTLG_ST_MAXIT = 2,       /* "Too many iterations."                    error_code 1 */
     MTLG_ST_BREAKDOWN = 3,   /* zero rho/gamma/omega (BiCGSTAB) or NaN    */
-    MTLG_ST_NO_DIRECTION = 4 /* GMRES found no direction                  error_code 2 */
+    MTLG_ST_NO_DIRECTION = 4, /* GMRES found no direction                 error_code 2 */
+    MTLG_ST_STALLED = 5       /* refinement: an FP64 outer step failed to halve the
+                                 residual (operator too ill-conditioned for the FP32
+                                 inner solve); no counterpart in the reference */
 };
 
 typedef struct mtlg_ctx mtlg_ctx;
@@ -100,6 +103,10 @@ typedef struct {
     double relresid;    /* iter.relresid() = resid / norm_r0 */
     double norm_r0;
     double seconds;     /* device time of the solve (CUDA events) */
+    int fp64_fallback;  /* refinement: 1 when the system was finished by a plain
+                           FP64 solve after the FP32-inner refinement stalled or
+                           broke down (iterations then include that solve's) */
+    int reserved;
 } mtlg_iter_result;
 
 /* FP64 iterative refinement around an FP32 inner Krylov solve. */

@@ -34,7 +34,7 @@ F64, F32 = 0, 1
 ASSIGN, PLUS, MINUS = 0, 1, 2
 PC_IDENTITY, PC_DIAGONAL, PC_ILU0, PC_IC0 = 0, 1, 2, 3
 CG, BICGSTAB, GMRES = 0, 1, 2
-ST_RUNNING, ST_CONVERGED, ST_MAXIT, ST_BREAKDOWN, ST_NO_DIRECTION = 0, 1, 2, 3, 4
+ST_RUNNING, ST_CONVERGED, ST_MAXIT, ST_BREAKDOWN, ST_NO_DIRECTION, ST_STALLED = 0, 1, 2, 3, 4, 5
 
 
 class IterParams(C.Structure):
@@ -45,7 +45,8 @@ class IterParams(C.Structure):
 class IterResult(C.Structure):
     _fields_ = [("iterations", C.c_int), ("error_code", C.c_int), ("status", C.c_int),
                 ("outer_iterations", C.c_int), ("resid", C.c_double), ("relresid", C.c_double),
-                ("norm_r0", C.c_double), ("seconds", C.c_double)]
+                ("norm_r0", C.c_double), ("seconds", C.c_double), ("fp64_fallback", C.c_int),
+                ("reserved", C.c_int)]
 
 
 class RefineParams(C.Structure):

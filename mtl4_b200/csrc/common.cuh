@@ -59,6 +59,7 @@ constexpr int kBlock = 256;
 constexpr int kSweepRows = 32;        // rows per sweep task (one warp, one row per lane)
 constexpr int kMaxDots = 4;           // dots a fused pass can reduce at once
 constexpr int kNumVec = 16;           // workspace vectors per system
+constexpr double kRefMinGain = 0.5;  // refinement: an outer step must at least halve the FP64 residual
 constexpr int kScalarMeanRow = 12;   // SpMV auto choice: thread per row up to this mean row length
 constexpr long long kSpinLimit = 1LL << 20;  // polls before a device wait gives up (~0.5 s)
 

@@ -135,6 +135,16 @@ int mtlg_batch_solve(mtlg_batch* B, int precision, const mtlg_refine_params* ref
             fill_result(h[k], mixed, &B->sys[members[k]]->result);
             B->sys[members[k]]->result.seconds = ms * 1e-3;
         }
+        // systems whose FP32-inner refinement stalled or broke down: finished in FP64
+        if (mixed) {
+            for (size_t k = 0; k < members.size(); ++k) {
+                auto& s = B->sys[members[k]];
+                if (!needs_fp64_finish(s->result)) continue;
+                const int st = fp64_finish(c, solver, s->A, s->P32, s->x.p, s->b.p,
+                                           fp64_budget(rp, s->result.iterations), rp.rtol, s->result);
+                if (st != MTLG_OK && st != MTLG_ERR_BREAKDOWN) return st;
+            }
+        }
         int flag = 0;
         MTLG_CUDA(cudaMemcpy(&flag, ss.misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost));
         if (flag) {

@@ -511,6 +511,8 @@ struct mtlg_pc {
     DBuf<SysDesc> desc;
     DBuf<SysState> st;
     DBuf<int> misc;
+    mtlg_pc* fallback64 = nullptr;  // FP32 storage: the FP64 preconditioner of the same kind a stalled
+                                    // refinement finishes with (made on first need)
     ChunkPlan plan[2];              // chunked sweeps with FP64 [0] / FP32 [1] vectors
     int plan_kernel[2] = {-1, -1};  // context's sweep_kernel / cluster setting the plan was made for
     RowLists lt;                    // IC(0): transposed upper pattern (natural order)

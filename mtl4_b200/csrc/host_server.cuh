@@ -370,10 +370,19 @@ int mtlg_server_step(mtlg_server* S)
             if (E.slot_req[s] < 0 || st[s].phase != PH_DONE) continue;
             auto& R = *S->reqs[E.slot_req[s]];
             if (R.state == 1) {
-                R.xh.resize(size_t(R.n));
-                MTLG_CUDA(cudaMemcpy(R.xh.data(), R.x.p, size_t(R.n) * 8, cudaMemcpyDeviceToHost));
                 fill_result(st[s], S->refine, &R.res);
                 if (!S->refine) R.res.norm_r0 = R.nb, R.res.relresid = R.nb ? st[s].resid / R.nb : st[s].resid;
+                if (S->refine && needs_fp64_finish(R.res) && !flag) {
+                    // the FP32-inner refinement stalled or broke down: finish in FP64
+                    mtlg_refine_params rp{};
+                    rp.max_outer = 20;
+                    rp.max_inner = R.max_iter;
+                    rp.rtol = S->o.rtol;
+                    MTLG_TRY(fp64_finish(c, R.solver, R.A, R.P, R.x.p, R.bd.p, fp64_budget(rp, R.res.iterations),
+                                         S->o.rtol, R.res));
+                }
+                R.xh.resize(size_t(R.n));
+                MTLG_CUDA(cudaMemcpy(R.xh.data(), R.x.p, size_t(R.n) * 8, cudaMemcpyDeviceToHost));
                 R.res.seconds = 0;
                 R.state = 2;
                 R.status_code = flag ? MTLG_ERR_TIMEOUT : MTLG_OK;

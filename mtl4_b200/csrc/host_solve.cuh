@@ -684,6 +684,8 @@ inline void fill_result(const SysState& s, bool mixed, mtlg_iter_result* r)
     r->resid = s.resid;
     r->norm_r0 = mixed ? s.nb : s.norm_r0;
     r->relresid = r->norm_r0 != 0.0 ? s.resid / r->norm_r0 : s.resid;
+    r->fp64_fallback = 0;
+    r->reserved = 0;
 }
 
 }  // namespace mtlg

@@ -158,6 +158,8 @@ __device__ void finalize(const SetView& sv, int fin, int sys, const double* dots
         s.gamma = dots[0];
         if (s.gamma == 0.0) { retire(sv, s, MTLG_ST_BREAKDOWN, 1); break; }
         s.alpha = s.rho / s.gamma;
+        // a non-finite step would spoil the iterate: stop before the update
+        if (!isfinite(s.alpha)) retire(sv, s, MTLG_ST_BREAKDOWN, 1);
         break;
     case FIN_BI_S: {
         // iter.finished(s) (bicgstab.hpp:64): on true, x += alpha*phat is
@@ -172,10 +174,13 @@ __device__ void finalize(const SetView& sv, int fin, int sys, const double* dots
     }
     case FIN_BI_OMEGA:
         s.omega = dots[0] / dots[1];
+        // t.t == 0 or an overflow: stop before x and r take a non-finite step
+        if (!isfinite(s.omega)) retire(sv, s, MTLG_ST_BREAKDOWN, 1);
         break;
     case FIN_REF_OUTER: {
         // Refinement stop test on the FP64 residual: ||b - A x|| <= rtol*||b||.
         const double rn = sqrt(fabs(dots[0]));
+        const double prev = s.scale;   // the previous outer residual (outer >= 1)
         s.inner_total += s.iter;
         s.iter = 0;
         s.scale = rn;
@@ -185,6 +190,11 @@ __device__ void finalize(const SetView& sv, int fin, int sys, const double* dots
             s.ostatus = MTLG_ST_CONVERGED; s.status = MTLG_ST_CONVERGED; s.error = 0; s.phase = PH_DONE;
         } else if (isnan(rn) || isinf(rn)) {
             s.ostatus = MTLG_ST_BREAKDOWN; s.status = MTLG_ST_BREAKDOWN; s.error = 1; s.phase = PH_DONE;
+        } else if (s.outer >= 1 && !(rn <= kRefMinGain * prev)) {
+            // the FP32 inner solves no longer reduce the FP64 residual (the
+            // operator is too ill-conditioned for FP32): stop; the host
+            // finishes the system in FP64
+            s.ostatus = MTLG_ST_STALLED; s.status = MTLG_ST_STALLED; s.error = 1; s.phase = PH_DONE;
         } else if (s.outer >= s.max_outer) {
             s.ostatus = MTLG_ST_MAXIT; s.status = MTLG_ST_MAXIT; s.error = 1; s.phase = PH_DONE;
         } else {

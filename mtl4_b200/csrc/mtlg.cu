@@ -4,6 +4,7 @@
 #include "host_solve.cuh"
 
 #include <map>
+#include <cmath>
 #include <type_traits>
 
 using namespace mtlg;
@@ -724,6 +725,7 @@ int mtlg_pc_destroy(mtlg_pc* P)
 {
     if (!P) return MTLG_OK;
     cudaStreamSynchronize(P->ctx->stream);
+    if (P->fallback64) mtlg_pc_destroy(P->fallback64);
     purge_sets(P->ctx, P);
     delete P;
     return MTLG_OK;
@@ -938,6 +940,65 @@ int mtlg_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* L, mtlg_pc* R, mtl
     return s;
 }
 
+// A refinement that stalled (the operator is too ill-conditioned for the
+// FP32 inner solve) or broke down is finished by a plain FP64 solve of the
+// same kind from its current iterate (from zero if that is not finite or
+// its residual is not below ||b||), with
+// the same stopping rule (relative to ||b||) and an iteration budget of
+// max_iter; the result adds up both and sets fp64_fallback.  x and b are
+// FP64 device vectors of A's size; P32 is the FP32 preconditioner (or null).
+extern "C++" {
+namespace mtlg {
+int fp64_finish(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* P32, double* x, const double* b, int max_iter,
+                double rtol, mtlg_iter_result& r)
+{
+    mtlg_pc* P64 = nullptr;
+    if (P32 && P32->kind != MTLG_PC_IDENTITY) {
+        if (!P32->fallback64) MTLG_TRY(mtlg_pc_create(c, A, P32->kind, MTLG_F64, &P32->fallback64));
+        P64 = P32->fallback64;
+    }
+    mtlg_vec xv, bv;
+    xv.ctx = bv.ctx = c;
+    xv.n = bv.n = A->n_rows;
+    xv.dtype = bv.dtype = MTLG_F64;
+    xv.p = x;
+    bv.p = const_cast<double*>(b);
+    // an iterate no better than zero (the FP32 solves may have driven it far
+    // off before the stall showed) restarts from zero: from a huge start the
+    // FP64 recursive residual would drift from the true one
+    if (!std::isfinite(r.resid) || !(r.resid < r.norm_r0)) MTLG_CUDA(cudaMemsetAsync(x, 0, xv.bytes(), c->stream));
+    mtlg_iter_params ip{};
+    ip.max_iter = std::max(max_iter, 1);
+    ip.rtol = rtol;
+    ip.atol = 0.0;
+    ip.norm_r0 = -1.0;
+    mtlg_iter_result r2{};
+    const int s = mtlg_solve(c, solver, A, P64, nullptr, &xv, &bv, &ip, &r2);
+    r.iterations += r2.iterations;
+    r.status = r2.status;
+    r.error_code = r2.error_code;
+    r.resid = r2.resid;
+    r.relresid = r2.relresid;
+    r.norm_r0 = r2.norm_r0;
+    r.seconds += r2.seconds;
+    r.fp64_fallback = 1;
+    return s;
+}
+
+inline bool needs_fp64_finish(const mtlg_iter_result& r)
+{
+    return r.status == MTLG_ST_STALLED || r.status == MTLG_ST_BREAKDOWN;
+}
+
+// remaining refinement budget, at least one inner solve's worth
+inline int fp64_budget(const mtlg_refine_params& rp, int used)
+{
+    const int64_t total = int64_t(std::max(rp.max_inner, 1)) * std::max(rp.max_outer, 1) - used;
+    return int(std::max<int64_t>(std::max(rp.max_inner, 1), total));
+}
+}  // namespace mtlg
+}
+
 int mtlg_refine_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* P, mtlg_vec* x, const mtlg_vec* b,
                       const mtlg_refine_params* rp, mtlg_iter_result* res)
 {
@@ -979,10 +1040,15 @@ int mtlg_refine_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* P, mtlg_vec
     MTLG_CUDA(cudaEventCreate(&e0));
     MTLG_CUDA(cudaEventCreate(&e1));
     MTLG_CUDA(cudaEventRecord(e0, c->stream));
+    mtlg_iter_result r{};
     int s = run_refine(ss, *rp);
-    if (s == MTLG_OK) s = timed_result(c, ss, e0, e1, res);
+    if (s == MTLG_OK) s = timed_result(c, ss, e0, e1, &r);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if ((s == MTLG_OK || s == MTLG_ERR_BREAKDOWN) && needs_fp64_finish(r))
+        s = fp64_finish(c, solver, A, P, static_cast<double*>(x->p), static_cast<const double*>(b->p),
+                        fp64_budget(*rp, r.iterations), rp->rtol, r);
+    if (res) *res = r;
     return s;
 }
 

@@ -42,6 +42,7 @@ class basic_iteration:
         self.status = _lib.ST_RUNNING
         self.seconds = 0.0
         self.outer = 0
+        self.fp64_fallback = False   # refinement finished by a plain FP64 solve
 
     # reference accessors
     def iterations(self) -> int: return self.i
@@ -65,6 +66,7 @@ class basic_iteration:
         self.status = r.status
         self.seconds = r.seconds
         self.outer = r.outer_iterations
+        self.fp64_fallback = bool(r.fp64_fallback)
         if r.norm_r0 > 0 or self._norm_r0 == 0:
             self._norm_r0 = r.norm_r0
 
@@ -175,7 +177,10 @@ def gmres(A, x, b, L, R, it: basic_iteration, restart: int) -> int:
 def refine(solver: str, A: compressed2D, x: dense_vector, b: dense_vector, P, rtol: float = 1e-8,
            inner_rtol: float = 1e-4, max_outer: int = 20, max_inner: int = 2000) -> basic_iteration:
     """FP64 iterative refinement around an FP32 inner solve (no reference
-    counterpart).  x, b: FP64; P: preconditioner stored in FP32."""
+    counterpart).  x, b: FP64; P: preconditioner stored in FP32.  When an
+    outer step fails to halve the FP64 residual (an operator too
+    ill-conditioned for FP32) or the inner solve breaks down, the system is
+    finished by a plain FP64 solve (it.fp64_fallback is then True)."""
     kind = {"cg": _lib.CG, "bicgstab": _lib.BICGSTAB}[solver]
     rp = _lib.RefineParams(int(max_outer), int(max_inner), 0, 0, float(rtol), float(inner_rtol))
     res = _lib.IterResult()

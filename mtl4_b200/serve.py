@@ -36,10 +36,12 @@ class Result:
     resid: float
     relresid: float
     seconds: float = 0.0
+    fp64_fallback: bool = False   # mixed precision finished by a plain FP64 solve
 
 
 def _result(x, r: _lib.IterResult) -> Result:
-    return Result(x, r.iterations, r.error_code, r.status, r.outer_iterations, r.resid, r.relresid, r.seconds)
+    return Result(x, r.iterations, r.error_code, r.status, r.outer_iterations, r.resid, r.relresid, r.seconds,
+                  bool(r.fp64_fallback))
 
 
 class batch:

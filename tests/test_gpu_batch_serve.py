@@ -121,3 +121,21 @@ def test_server_admission_and_cancel(ctx):
         if all(srv2.poll(i) is not None for i in ids[1:] if i in srv2.n):
             break
     assert srv2.stats()["cancelled"] == 1
+
+
+def test_batch_and_server_finish_stalled_refinement_in_fp64(ctx):
+    # the served stream's request 33 is too ill-conditioned for the FP32 inner
+    # solve; batch and server finish it in FP64 and report that they did
+    from mtl4_b200 import serve
+    sp = P.request_specs(20000)[33]
+    A = sp.build()
+    b = P.random_rhs(A.n_rows, sp.seed)
+    B = serve.batch(ctx)
+    B.add(A, b, "bicgstab", "ilu_0", max_iter=2000, rtol=1e-8)
+    B.solve(mixed=True, rtol=1e-8, inner_rtol=1e-4)
+    r = B.result(0)
+    assert r.error_code == 0 and r.fp64_fallback and relres(A, r.x, b) <= 1.05e-8
+    srv = serve.server(ctx, max_active=4, iters_per_step=16, mixed=True, rtol=1e-8, inner_rtol=1e-4)
+    out = serve.run_open_loop(srv, [(A, b, "bicgstab", "ilu_0", 2000)], np.zeros(1), timeout_s=120.0)
+    r = out["results"][0]
+    assert r is not None and r.error_code == 0 and r.fp64_fallback and relres(A, r.x, b) <= 1.05e-8

@@ -286,6 +286,29 @@ def test_refinement_fp32_inner_fp64_outer(ctx, solver, pc):
     assert rel <= 1e-10
     x64 = O.port_solve(A, b, solver, pc, max_iter=5000, rtol=1e-13)["x"]
     assert np.abs(xs - x64).max() <= 1e-6 * np.abs(x64).max()
+    assert not it.fp64_fallback
+
+
+def ill_conditioned_request():
+    """A request of the served stream whose operator is too ill-conditioned
+    for an FP32 inner solve (2D, 552^2, log-normal coefficients sigma = 1,
+    weak convection): the FP32 BiCGSTAB + ILU(0) refinement does not reduce
+    the FP64 residual."""
+    sp = P.request_specs(20000)[33]
+    assert (sp.dims, sp.m, sp.solver, sp.pc) == (2, 552, "bicgstab", "ilu_0")
+    A = sp.build()
+    return sp, A, P.random_rhs(A.n_rows, sp.seed)
+
+
+def test_refinement_stall_finishes_in_fp64(ctx):
+    from mtl4_b200 import itl, mtl
+    sp, A, b = ill_conditioned_request()
+    Ad = dev(A, ctx)
+    x = mtl.dense_vector(A.n_rows, np.float64, ctx)
+    it = itl.refine("bicgstab", Ad, x, vec(b, ctx), itl.pc.ilu_0(Ad, np.float32), rtol=1e-8, inner_rtol=1e-4)
+    assert it.fp64_fallback and it.is_converged()
+    rel = np.linalg.norm(A.matvec(x.numpy()) - b) / np.linalg.norm(b)
+    assert rel <= 1e-8
 
 
 # ---------------------------------------------------------------- GMRES
