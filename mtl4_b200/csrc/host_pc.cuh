@@ -44,6 +44,13 @@ constexpr int kChunkMaxEntries = 16;   // longer factor rows: flat sweeps only
 inline int round4(int v) { return (v + 3) & ~3; }
 inline int entries_bucket(int k) { return k <= 2 ? 2 : k <= 3 ? 3 : k <= 4 ? 4 : k <= 8 ? 8 : 16; }
 
+// Wave cap (rows) of a factor whose rows hold up to kb entries (bucket),
+// stored in ssz-byte values: the largest shape built for it.
+inline int chunk_wave_cap(int kb, int ssz)
+{
+    return ssz == 8 && kb > 8 ? 128 : 256;
+}
+
 // Chunked layout of a triangular factor: chunks of B contiguous rows in
 // processing order; inside a chunk the rows are grouped by dependency level
 // (waves, split to at most `threads` rows), a wave's rows in the order of
@@ -58,7 +65,7 @@ inline int entries_bucket(int k) { return k <= 2 ? 2 : k <= 3 ? 3 : k <= 4 ? 4 :
 // directly, their wave flagged with kWaveOverflow.  Waves start 4-aligned in
 // positions, and in slots when they read several earlier-chunk rows.
 inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& lev, int n, bool lower, int B,
-                        TriDev& T)
+                        int ssz, TriDev& T)
 {
     T.nch = 0;
     T.max_slots = 0;
@@ -87,8 +94,8 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         }
         cbeg[p + 1] = int(order.size());
     }
-    const int NT = std::min(256, std::max(32, (maxw + 31) / 32 * 32));
     const int KB = entries_bucket(kmax);
+    const int NT = std::min(chunk_wave_cap(KB, ssz), std::max(32, (maxw + 31) / 32 * 32));
     // segment capacity: a multiple of 32 rows, so every staged array (and
     // every staging buffer) starts 16-byte aligned in shared memory
     const int SR = std::max(NT, (1024 / KB + 31) / 32 * 32);
@@ -235,11 +242,10 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
 // ------------------------------------------------------------ chunked sweeps
 constexpr int kChunkSmemMax = 225 * 1024;   // dynamic shared memory of one chunk CTA, at most
 
-// Launch plan of the chunked sweeps of a set of factors (computed outside
-// any stream capture: it queries the occupancy).
-struct ChunkPlan {
-    bool ok = false;
-    int nt = 0, km = 0;          // compute threads per CTA, entries per row
+// Launch shape of the chunked sweeps of one side (the L or the U factors)
+// of a set of systems.
+struct ChunkSide {
+    int nt = 0, km = 0;          // wave cap (rows), entries per row
     int rows = 0;                // rows of the largest chunk
     int slots = 0;               // receive slots of the largest chunk
     int seg_rows = 0, seg_ents = 0;
@@ -247,8 +253,6 @@ struct ChunkPlan {
     int resident = 1;            // CTAs resident at once
     int vec_bytes = 0;
     int cells = 0;               // shared cells of the largest chunk (rows, +0 cell, slots)
-    DBuf<GroupTask> tl, tu;
-    int ntl = 0, ntu = 0;
     void add(const TriDev& T)
     {
         nt = std::max(nt, T.threads);
@@ -263,90 +267,125 @@ struct ChunkPlan {
     int entries() const { return entries_bucket(km); }
 };
 
+// Launch plan of the chunked sweeps of a set of factors (computed outside
+// any stream capture: it queries the occupancy): a shape per side and the
+// task lists.
+struct ChunkPlan {
+    bool ok = false;
+    ChunkSide side[2];           // L [0], U [1]
+    DBuf<GroupTask> tl, tu;
+    int ntl = 0, ntu = 0;
+};
+
+// Kernel shape of a wave cap of NT rows and KM entries per row: up to four
+// compute warps, two rows per thread beyond 128 rows.
 template <typename T, typename S, int NT, int KM>
 struct ChunkShape {
+    static constexpr int CW = NT >= 128 ? 4 : NT / 32;
+    static constexpr int RPT = NT / (32 * CW);
+    static constexpr int THREADS = 32 * (CW + kChunkExtraWarps);
     static int init()
     {
-        MTLG_CUDA(cudaFuncSetAttribute(k_sweep_chunk<T, S, NT, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        MTLG_CUDA(cudaFuncSetAttribute(k_sweep_chunk<T, S, CW, RPT, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kChunkSmemMax));
         return MTLG_OK;
     }
     static int occupancy(int smem)
     {
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_chunk<T, S, NT, KM>, NT + 32 * kChunkExtraWarps, size_t(smem)) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_chunk<T, S, CW, RPT, KM>, THREADS, size_t(smem)) !=
             cudaSuccess) {
             cudaGetLastError();
             return 0;
         }
         return n;
     }
-    static int launch(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const ChunkSweepOp& op, const ChunkPlan& pl)
+    static int launch(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const ChunkSweepOp& op, const ChunkSide& pl)
     {
         const int grid = std::max(1, std::min(op.ntasks, pl.resident));
-        k_sweep_chunk<T, S, NT, KM><<<grid, kChunkExtraWarps * 32 + NT, pl.smem, st>>>(sv, op);
+        k_sweep_chunk<T, S, CW, RPT, KM><<<grid, THREADS, pl.smem, st>>>(sv, op);
         c->launches++;
         MTLG_CUDA(cudaGetLastError());
         return MTLG_OK;
     }
 };
 
-#define MTLG_CHUNK_SHAPES(M, T, S) \
+// The shapes built, by stored type: with FP64 values, rows of 16 entries
+// stay at one row per thread (the rows of a wave, the next wave's and their
+// reads stay in registers).
+#define MTLG_CHUNK_SHAPES_F32(M, T, S) \
     M(T, S, 32, 2) M(T, S, 32, 3) M(T, S, 32, 4) M(T, S, 32, 8) M(T, S, 32, 16) \
     M(T, S, 64, 2) M(T, S, 64, 3) M(T, S, 64, 4) M(T, S, 64, 8) M(T, S, 64, 16) \
     M(T, S, 128, 2) M(T, S, 128, 3) M(T, S, 128, 4) M(T, S, 128, 8) M(T, S, 128, 16) \
     M(T, S, 256, 2) M(T, S, 256, 3) M(T, S, 256, 4) M(T, S, 256, 8) M(T, S, 256, 16)
+#define MTLG_CHUNK_SHAPES_F64(M, T, S) \
+    M(T, S, 32, 2) M(T, S, 32, 3) M(T, S, 32, 4) M(T, S, 32, 8) M(T, S, 32, 16) \
+    M(T, S, 64, 2) M(T, S, 64, 3) M(T, S, 64, 4) M(T, S, 64, 8) M(T, S, 64, 16) \
+    M(T, S, 128, 2) M(T, S, 128, 3) M(T, S, 128, 4) M(T, S, 128, 8) M(T, S, 128, 16) \
+    M(T, S, 256, 2) M(T, S, 256, 3) M(T, S, 256, 4) M(T, S, 256, 8)
 
 inline int init_chunk_shapes()
 {
 #define MTLG_CHUNK_INIT(T, S, NT, KM) MTLG_TRY((ChunkShape<T, S, NT, KM>::init()));
-    MTLG_CHUNK_SHAPES(MTLG_CHUNK_INIT, double, double)
-    MTLG_CHUNK_SHAPES(MTLG_CHUNK_INIT, double, float)
-    MTLG_CHUNK_SHAPES(MTLG_CHUNK_INIT, float, float)
-    MTLG_CHUNK_SHAPES(MTLG_CHUNK_INIT, float, double)
+    MTLG_CHUNK_SHAPES_F64(MTLG_CHUNK_INIT, double, double)
+    MTLG_CHUNK_SHAPES_F32(MTLG_CHUNK_INIT, double, float)
+    MTLG_CHUNK_SHAPES_F32(MTLG_CHUNK_INIT, float, float)
+    MTLG_CHUNK_SHAPES_F64(MTLG_CHUNK_INIT, float, double)
 #undef MTLG_CHUNK_INIT
     return MTLG_OK;
 }
 
-template <typename T, typename S>
-inline int chunk_occupancy(const ChunkPlan& pl, int smem)
+// Calls fn(ChunkShape<T, S, NT, KM>()) for the built shape of (nt, km);
+// false if none is built.
+template <typename T, typename S, typename Fn>
+inline bool with_chunk_shape(int nt, int km, Fn&& fn)
 {
-    const int nt = pl.threads(), km = pl.entries();
-#define MTLG_CHUNK_Q(TT, SS, NT, KM) \
-    if (nt == NT && km == KM) return ChunkShape<TT, SS, NT, KM>::occupancy(smem);
-    MTLG_CHUNK_SHAPES(MTLG_CHUNK_Q, T, S)
-#undef MTLG_CHUNK_Q
-    return 0;
+    bool found = false;
+#define MTLG_CHUNK_WITH(TT, SS, NT, KM) \
+    if (!found && nt == NT && km == KM) { fn(ChunkShape<TT, SS, NT, KM>()); found = true; }
+    if constexpr (sizeof(S) == 4) {
+        MTLG_CHUNK_SHAPES_F32(MTLG_CHUNK_WITH, T, S)
+    } else {
+        MTLG_CHUNK_SHAPES_F64(MTLG_CHUNK_WITH, T, S)
+    }
+#undef MTLG_CHUNK_WITH
+    return found;
 }
 
 // Shape and task list of a set of systems' factors (f[s]: the system's L and
 // U, or nulls for an unused slot); chunks of all systems interleaved by
-// processing position.
+// processing position.  Not ok (flat sweeps) when a side's shape is not
+// built or its shared memory does not fit.
 template <typename T, typename S>
 inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, const TriDev*>>& f, ChunkPlan& pl)
 {
     pl.ok = false;
-    pl.nt = pl.km = pl.rows = pl.slots = pl.cells = pl.seg_rows = pl.seg_ents = 0;
+    pl.side[0] = pl.side[1] = ChunkSide();
     pl.ntl = pl.ntu = 0;
     bool any = false;
     for (const auto& lu : f) {
         if (!lu.first) continue;
         any = true;
         if (lu.first->nch == 0 || lu.second->nch == 0 || !lu.first->cval.p || !lu.second->cval.p) return MTLG_OK;
-        pl.add(*lu.first);
-        pl.add(*lu.second);
+        pl.side[0].add(*lu.first);
+        pl.side[1].add(*lu.second);
     }
     if (!any || c->sweep_kernel != 0) return MTLG_OK;
-    if (pl.seg_rows % 4 || pl.seg_ents % 4) {
-        set_error("chunked sweep: staging capacity %d/%d is not a multiple of 4", pl.seg_rows, pl.seg_ents);
-        return MTLG_ERR_NOT_SUPPORTED;
+    for (ChunkSide& sd : pl.side) {
+        if (sd.seg_rows % 4 || sd.seg_ents % 4) {
+            set_error("chunked sweep: staging capacity %d/%d is not a multiple of 4", sd.seg_rows, sd.seg_ents);
+            return MTLG_ERR_NOT_SUPPORTED;
+        }
+        sd.vec_bytes = int((size_t(sd.cells) * sizeof(T) + 15) / 16 * 16);
+        sd.smem = sd.vec_bytes + kStageBufs * stage_bytes<S>(sd.seg_rows, sd.seg_ents);
+        if (sd.smem > kChunkSmemMax) return MTLG_OK;
+        int occ = 0;
+        const int smem = sd.smem;
+        if (!with_chunk_shape<T, S>(sd.threads(), sd.entries(), [&](auto shape) { occ = decltype(shape)::occupancy(smem); }))
+            return MTLG_OK;
+        if (occ < 1) return MTLG_OK;
+        sd.resident = c->sm_count * occ;
     }
-    pl.vec_bytes = int((size_t(pl.cells) * sizeof(T) + 15) / 16 * 16);
-    pl.smem = pl.vec_bytes + kStageBufs * stage_bytes<S>(pl.seg_rows, pl.seg_ents);
-    if (pl.smem > kChunkSmemMax) return MTLG_OK;
-    const int occ = chunk_occupancy<T, S>(pl, pl.smem);
-    if (occ < 1) return MTLG_OK;
-    pl.resident = c->sm_count * occ;
     std::vector<GroupTask> tl, tu;
     int maxch = 0;
     for (const auto& lu : f)
@@ -367,19 +406,20 @@ inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, c
 }
 
 template <typename T, typename S>
-inline int launch_chunk_sweep(mtlg_ctx* c, cudaStream_t st, const SetView& sv, ChunkSweepOp op, const ChunkPlan& pl)
+inline int launch_chunk_sweep(mtlg_ctx* c, cudaStream_t st, const SetView& sv, ChunkSweepOp op, const ChunkPlan& plan)
 {
     if (op.ntasks == 0) return MTLG_OK;
+    const ChunkSide& pl = plan.side[op.which];
     op.vec_bytes = pl.vec_bytes;
     op.rows_cap = pl.seg_rows;
     op.ents_cap = pl.seg_ents;
-    const int nt = pl.threads(), km = pl.entries();
-#define MTLG_CHUNK_CASE(TT, SS, NT, KM) \
-    if (nt == NT && km == KM) return ChunkShape<TT, SS, NT, KM>::launch(c, st, sv, op, pl);
-    MTLG_CHUNK_SHAPES(MTLG_CHUNK_CASE, T, S)
-#undef MTLG_CHUNK_CASE
-    set_error("chunk sweep shape %d/%d", nt, km);
-    return MTLG_ERR_NOT_SUPPORTED;
+    int rc = MTLG_OK;
+    if (!with_chunk_shape<T, S>(pl.threads(), pl.entries(),
+                                [&](auto shape) { rc = decltype(shape)::launch(c, st, sv, op, pl); })) {
+        set_error("chunk sweep shape %d/%d", pl.threads(), pl.entries());
+        return MTLG_ERR_NOT_SUPPORTED;
+    }
+    return rc;
 }
 
 // Device view of a factor (both layouts).
@@ -440,7 +480,7 @@ inline int default_chunk_rows(const mtlg_ctx* c, int storage)
     return storage == MTLG_F32 ? 16384 : 8192;
 }
 
-inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& T, int chunk_rows)
+inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& T, int chunk_rows, int ssz)
 {
     T.n = n;
     T.lower = lower;
@@ -492,7 +532,7 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
     MTLG_TRY(T.src.upload(c, T.h_src.data(), T.h_src.size()));
     MTLG_TRY(T.mul.upload(c, T.h_mul.data(), T.h_mul.size()));
     MTLG_TRY(T.tasks.upload(c, tasks.data(), tasks.size()));
-    return build_chunks(c, F, lev, n, lower, chunk_rows, T);
+    return build_chunks(c, F, lev, n, lower, chunk_rows, ssz, T);
 }
 
 }  // namespace mtlg
@@ -634,8 +674,8 @@ inline int pc_build(mtlg_pc* P)
         RowLists E;
         E.rp.assign(n + 1, 0);
         const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
-        MTLG_TRY(build_tri(c, E, n, true, P->L, B));
-        MTLG_TRY(build_tri(c, E, n, false, P->U, B));
+        MTLG_TRY(build_tri(c, E, n, true, P->L, B, int(P->ssize())));
+        MTLG_TRY(build_tri(c, E, n, false, P->U, B, int(P->ssize())));
         MTLG_TRY(P->L.val.alloc(c, 16));
         MTLG_TRY(P->U.val.alloc(c, 16));
         MTLG_TRY(P->L.dia.alloc(c, size_t(P->L.npad) * P->ssize()));
@@ -704,8 +744,8 @@ inline int pc_build(mtlg_pc* P)
         MTLG_TRY(P->lt_src.upload(c, Lr.src.data(), std::max<size_t>(1, Lr.src.size())));
     }
     const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
-    MTLG_TRY(build_tri(c, Lr, n, true, P->L, B));
-    MTLG_TRY(build_tri(c, Ur, n, false, P->U, B));
+    MTLG_TRY(build_tri(c, Lr, n, true, P->L, B, int(P->ssize())));
+    MTLG_TRY(build_tri(c, Ur, n, false, P->U, B, int(P->ssize())));
     MTLG_TRY(pc_setup_single_set(P));
 
     // ---- numeric factorization on the device (FP64)

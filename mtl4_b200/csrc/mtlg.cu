@@ -822,14 +822,15 @@ static int sweep_plan_of(mtlg_ctx* c, mtlg_pc* P, int32_t* out)
     }
     for (int i = 0; i < 8; ++i) out[i] = 0;
     if (!pl.ok) return MTLG_OK;
-    out[0] = pl.rows;
+    const ChunkSide& sl = pl.side[0];
+    out[0] = sl.rows;
     out[1] = P->L.nch;
-    out[2] = pl.resident;
-    out[3] = pl.smem;
-    out[4] = pl.threads();
-    out[5] = pl.entries();
-    out[6] = pl.seg_rows;
-    out[7] = pl.seg_ents;
+    out[2] = sl.resident;
+    out[3] = sl.smem;
+    out[4] = sl.threads();
+    out[5] = sl.entries();
+    out[6] = sl.seg_rows;
+    out[7] = sl.seg_ents;
     return MTLG_OK;
 }
 }

@@ -149,11 +149,14 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
 // ------------------------------------------------------------ chunked sweep
 // One CTA per chunk of contiguous rows (TriFactor's chunked layout), taken
 // in processing order through one ticket.  Warp roles:
-//  - NT compute threads run the chunk's waves one after the other: a row
-//    reads the rows of its own chunk from a shared vector (finished in
-//    earlier waves, made visible by a named barrier between waves), and its
-//    result is published in position order (one coalesced store per warp and
-//    wave) for later chunks;
+//  - CW compute warps (CT = 32 CW threads) run the chunk's waves one after
+//    the other, RPT rows per thread (thread i holds rows i, i + CT, ... of a
+//    wave of at most CT RPT rows; slots past the wave's rows repeat its last
+//    row, so the rows need no branches), with a barrier among the compute
+//    warps between waves: a row reads the rows of its own chunk from a
+//    shared vector (finished in earlier waves), and its result is published
+//    in position order (one coalesced store per warp, row group and wave)
+//    for later chunks;
 //  - kRecvWarps receiver warps fetch the results of earlier chunks this chunk
 //    needs, in the order the waves consume them, many requests in flight,
 //    into receive slots in shared memory, so a compute thread waits on the
@@ -163,15 +166,15 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
 //    waves per buffer, one bulk copy (TMA) per array, with full / empty
 //    mbarrier pairs between it and the compute threads.
 // The chunk's right-hand sides are loaded into the shared vector up front
-// and the chunk's outputs written back at its end, both coalesced.  Chunks
+// and the chunk's outputs written back at its end by all warps, coalesced.  Chunks
 // depend on earlier chunks only and waves on earlier waves, and a chunk is
 // held by a running CTA, so the waits end; they are bounded all the same
 // (kSpinLimit polls, then a timeout flag and a drain).  The arithmetic per
 // row is k_sweep's (same entry order, same roundings).
 constexpr int kStageBufs = 3;
 constexpr int kRecvDepth = 2;                       // receive quads in flight per receiver lane
-constexpr int kRecvWarps = 4;                       // receiver warps
-constexpr int kChunkExtraWarps = kRecvWarps + 1;    // receiver warps and the producer warp after the NT compute threads
+constexpr int kRecvWarps = 3;                       // receiver warps
+constexpr int kChunkExtraWarps = kRecvWarps + 1;    // receiver warps and the producer warp after the compute warps
 
 struct ChunkSweepOp {
     const GroupTask* tasks;
@@ -461,37 +464,47 @@ __device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, cons
     }
 }
 
-// One thread's row of a staged wave, in registers.
-template <typename T, typename S, int KM>
-struct WaveRow {
-    int row;
-    T rhs;
-    S dia;
-    int col[KM];
-    S val[KM];
+// One compute thread's rows of a staged wave, in registers (RPT rows: i, i + CT, ...).
+template <typename T, typename S, int RPT, int KM>
+struct WaveRows {
+    int row[RPT];     // chunk-local index
+    int pos[RPT];     // position in the wave
+    T rhs[RPT];
+    S dia[RPT];
+    int col[RPT][KM];
+    S val[RPT][KM];
 };
 
-template <typename T, typename S, int KM>
-__device__ __forceinline__ void wave_row(unsigned m, const int* srow, const S* sdia, const int* scol, const S* sval,
-                                         const T* vec, int B, int r0, int poff, int eoff, int tid,
-                                         WaveRow<T, S, KM>& r)
+// Loads compute thread i's rows of staged wave m (positions from poff,
+// entries from eoff).  Row slots past the wave's rows repeat its last row (same reads,
+// same result, same stores), and entries past the wave's K are the +0 cell
+// with value 0, so the sweep needs no per-row branches; every index stays
+// inside the staged segment.
+template <typename T, typename S, int CT, int RPT, int KM>
+__device__ __forceinline__ void wave_rows(unsigned m, const int* srow, const S* sdia, const int* scol, const S* sval,
+                                          const T* vec, int B, int r0, int poff, int eoff, int ents_cap, int lane,
+                                          WaveRows<T, S, RPT, KM>& r)
 {
     const int nw = int(m & 0x7FFFu), K = int(m >> 16);
-    r.row = -1;
-    if (tid < nw) {
-        r.row = srow[poff + tid];
-        r.dia = sdia[poff + tid];
-        r.rhs = vec[r.row - r0];
+    const int kl = max(K - 1, 0);
+    const int elast = ents_cap - 1;   // a wave without entries (K = 0) may start at the end of the staged entries
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+        const int t = min(lane + CT * q, nw - 1);
+        r.pos[q] = poff + t;
+        r.row[q] = srow[poff + t] - r0;
+        r.dia[q] = sdia[poff + t];
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
-            r.col[k] = B;      // the +0 cell, value +0: neutral
-            r.val[k] = S(0);
-            if (k < K) {
-                r.col[k] = scol[eoff + k * nw + tid];
-                r.val[k] = sval[eoff + k * nw + tid];
-            }
+            const int e = min(eoff + min(k, kl) * nw + t, elast);   // inside the wave's entries (K > 0)
+            const int c = scol[e];
+            const S v = sval[e];
+            r.col[q][k] = k < K ? c : B;   // the +0 cell, value +0: neutral
+            r.val[q][k] = k < K ? v : S(0);
         }
     }
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) r.rhs[q] = vec[r.row[q]];
 }
 
 // Staging buffer views of segment buffer b.
@@ -512,15 +525,22 @@ struct StageView {
     }
 };
 
-__device__ __forceinline__ void compute_barrier(int nt)
+// Barrier among the CT compute threads (a warp barrier for one warp).
+template <int CW>
+__device__ __forceinline__ void compute_barrier()
 {
-    asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+    if constexpr (CW == 1)
+        __syncwarp();
+    else
+        asm volatile("bar.sync 1, %0;" ::"n"(32 * CW) : "memory");
 }
 
-template <typename T, typename S, int NT, int KM>
-__global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetView sv, ChunkSweepOp op)
+template <typename T, typename S, int CW, int RPT, int KM>
+__global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(SetView sv, ChunkSweepOp op)
 {
-    if (blockDim.x != unsigned(NT + 32 * kChunkExtraWarps)) {   // launch shape mismatch: report, never wait
+    constexpr int CT = 32 * CW;
+    constexpr int NTH = 32 * (CW + kChunkExtraWarps);
+    if (blockDim.x != unsigned(NTH)) {   // launch shape mismatch: report, never wait
         if (threadIdx.x == 0) atomicExch(sv.err, 1);
         return;
     }
@@ -533,7 +553,6 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
     unsigned char* stage = chunk_smem + op.vec_bytes;
     const int sbytes = stage_bytes<S>(op.rows_cap, op.ents_cap);
     const int tid = threadIdx.x;
-    constexpr int NTH = NT + 32 * kChunkExtraWarps;
     if (tid == 0) {
         for (int b = 0; b < kStageBufs; ++b) {
             mbar_init(&full[b], 1);
@@ -584,9 +603,9 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
             for (long long i = a + tid; i < e; i += NTH) yr[i] = sentinel_value<T>();
         }
         __syncthreads();
-        if (tid >= NT + 32 * kRecvWarps) {
+        if (tid >= CT + 32 * kRecvWarps) {
             // producer warp: stage the chunk's segments (lane 0)
-            if (tid == NT + 32 * kRecvWarps) {
+            if (tid == CT + 32 * kRecvWarps) {
                 for (int i = 0; i < nseg; ++i) {
                     const unsigned g = gseg + i, b = g % kStageBufs;
                     const SegRec sg = F.segs[s0 + i];
@@ -596,20 +615,22 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
                     stage_segment<S>(F, sg, stage + b * sbytes, op.rows_cap, op.ents_cap, &full[b]);
                 }
             }
-        } else if (tid >= NT) {
+        } else if (tid >= CT) {
             // receiver warps
-            receive_chunk<T>(cext, TF.cquad, x0, nx, ypos, vec + B + kSlotBase, (tid - NT) >> 5, tid & 31, sv.err,
+            receive_chunk<T>(cext, TF.cquad, x0, nx, ypos, vec + B + kSlotBase, (tid - CT) >> 5, tid & 31, sv.err,
                              op.sleep_ns);
         } else {
-            // compute threads: all waves of the chunk, one cursor across segments
+            // compute warps: all waves of the chunk, one cursor across
+            // segments; the next wave's rows load while this one computes
+            const int lane = tid;
             unsigned g = gseg, b = g % kStageBufs;
             mbar_wait(&full[b], (g / kStageBufs) & 1u, sv.err);
             StageView<S> V(stage + b * sbytes, op.rows_cap, op.ents_cap);
             int si = 0, nws = s_nw[b], p0 = s_p0[b];
             int w = 0, poff = 0, eoff = 0;
             unsigned m = V.wv[0];
-            WaveRow<T, S, KM> cur, nxt;
-            wave_row<T, S, KM>(m, V.row, V.dia, V.col, V.val, vec, B, r0, 0, 0, tid, cur);
+            WaveRows<T, S, RPT, KM> cur, nxt;
+            wave_rows<T, S, CT, RPT, KM>(m, V.row, V.dia, V.col, V.val, vec, B, r0, 0, 0, op.ents_cap, lane, cur);
             for (;;) {
                 // locate and load the next wave (possibly the next segment's first)
                 const int nw = int(m & 0x7FFFu);
@@ -632,47 +653,47 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
                 } else {
                     has_next = false;
                 }
-                if (has_next) wave_row<T, S, KM>(mn, Vn.row, Vn.dia, Vn.col, Vn.val, vec, B, r0, pn, en, tid, nxt);
-                if (cur.row >= 0) {
-                    // all of the row's reads at once (chunk rows, the +0 cell and
-                    // receive slots are cells of one shared vector); waits only
-                    // for slots the receiver has not filled yet
-                    T dv[KM];
-                    bool wait = false;
-                    if (!(m & kWaveOverflow)) {
+                // all of the wave's reads at once (chunk rows, the +0 cell and
+                // receive slots are cells of one shared vector; an entry coded
+                // below zero is an earlier chunk's result read from global
+                // memory); waits only for values not there yet
+                T dv[RPT][KM];
+                bool wait = false;
 #pragma unroll
-                        for (int k = 0; k < KM; ++k) {
-                            dv[k] = vec[cur.col[k]];
-                            wait |= is_sentinel(dv[k]);
-                        }
-                    } else {
+                for (int q = 0; q < RPT; ++q)
 #pragma unroll
-                        for (int k = 0; k < KM; ++k) {
-                            dv[k] = cur.col[k] >= 0 ? vec[cur.col[k]] : sentinel_value<T>();
-                            wait |= is_sentinel(dv[k]);
-                        }
+                    for (int k = 0; k < KM; ++k) {
+                        const int c = cur.col[q][k];
+                        const T x = vec[c >= 0 ? c : B];
+                        dv[q][k] = c >= 0 ? x : sentinel_value<T>();
+                        wait |= is_sentinel(dv[q][k]);
                     }
-                    if (wait) {
+                if (has_next) wave_rows<T, S, CT, RPT, KM>(mn, Vn.row, Vn.dia, Vn.col, Vn.val, vec, B, r0, pn, en, op.ents_cap, lane, nxt);
+                if (wait) {
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q)
 #pragma unroll
                         for (int k = 0; k < KM; ++k) {
-                            if (is_sentinel(dv[k])) {
-                                const int c = cur.col[k];
-                                dv[k] = c >= 0 ? poll_slot(vec + c, sv.err) : poll_value(ypos + (-c - 2), sv.err, op.sleep_ns);
+                            if (is_sentinel(dv[q][k])) {
+                                const int c = cur.col[q][k];
+                                dv[q][k] = c >= 0 ? poll_slot(vec + c, sv.err) : poll_value(ypos + (-c - 2), sv.err, op.sleep_ns);
                             }
                         }
-                    }
-                    T rr = cur.rhs;
-#pragma unroll
-                    for (int k = 0; k < KM; ++k) rr = sweep_step<T, S>(rr, cur.val[k], dv[k]);
-                    const T out = unsentinel(T(W(rr) * W(cur.dia)));
-                    vec[cur.row - r0] = out;
-                    st_relaxed_gpu(ypos + p0 + poff + tid, out);
                 }
-                compute_barrier(NT);
+#pragma unroll
+                for (int q = 0; q < RPT; ++q) {
+                    T rr = cur.rhs[q];
+#pragma unroll
+                    for (int k = 0; k < KM; ++k) rr = sweep_step<T, S>(rr, cur.val[q][k], dv[q][k]);
+                    const T out = unsentinel(T(W(rr) * W(cur.dia[q])));
+                    vec[cur.row[q]] = out;
+                    st_relaxed_gpu(ypos + p0 + cur.pos[q], out);
+                }
+                compute_barrier<CW>();
                 if (!has_next) break;
                 if (cross) {
-                    // every compute thread has read its last row of buffer b
-                    if (tid == 0) mbar_arrive(&empty[b]);
+                    // every compute thread has read its last rows of buffer b
+                    if (lane == 0) mbar_arrive(&empty[b]);
                     g = gn;
                     b = bn;
                     V = Vn;
@@ -690,18 +711,20 @@ __global__ void __launch_bounds__(NT + 32 * kChunkExtraWarps) k_sweep_chunk(SetV
                 cur = nxt;
             }
             // last segment's buffer
-            if (tid == 0) mbar_arrive(&empty[b]);
-            // chunk epilogue: outputs and the reset of the buffer the other sweep fills
-            compute_barrier(NT);
+            if (lane == 0) mbar_arrive(&empty[b]);
+        }
+        gseg += unsigned(nseg);
+        __syncthreads();
+        // chunk epilogue (all warps): outputs and the reset of the buffer the
+        // other sweep fills
+        {
             T* y = vptr<T>(d, op.out);
             T* R = op.reset != SLOT_NONE ? vptr<T>(d, op.reset) : nullptr;
-            for (int i = tid; i < nr; i += NT) {
+            for (int i = tid; i < nr; i += NTH) {
                 y[r0 + i] = vec[i];
                 if (R) R[r0 + i] = sentinel_value<T>();
             }
         }
-        gseg += unsigned(nseg);
-        __syncthreads();
     }
 }
 
