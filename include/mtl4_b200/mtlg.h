@@ -140,7 +140,10 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * thread per row from global memory), "sweep_kernel" (0: chunked sweeps,
  * one CTA per chunk of rows, default; 1: flat level-order sweeps),
  * "chunk_rows" (rows per chunk of preconditioners created afterwards; 0:
- * 16384 for FP32 factors, 8192 for FP64), "pc_apply_sync" (1, default:
+ * 16384 for FP32 factors, 8192 for FP64), "sweep_cluster" (CTAs per
+ * thread-block cluster of the chunked sweeps, whose neighbouring chunks
+ * hand results over through shared memory: 1, 2, 4 or 8; 0, default:
+ * chosen per plan), "pc_apply_sync" (1, default:
  * mtlg_pc_apply waits for its sweeps and reports an expired device wait;
  * 0: it only enqueues them, and an expired wait is reported by the next
  * synchronous apply of the same preconditioner).

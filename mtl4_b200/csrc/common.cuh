@@ -129,6 +129,8 @@ struct TriFactor {
     const int* cxr;    // [nch + 1] receive-slot range of each chunk in cext
     const int* cext;   // positions of earlier chunks' rows, per chunk in slot order (-1: unused slot)
     const int2* cquad; // per 4 slots: {first of 4 consecutive positions or -1, mask of used slots}
+    const int* cqpull; // per 4 slots: mask of the used slots the previous chunk does not push
+    const int* cpush;  // per position: receive slot of the next chunk the row's result fills, or -1
     void* ypos;        // results by position (T), all sentinel before the sweep
     void* ypos_reset;  // the other factor's results by position: reset to the sentinel by this sweep
     int npos, npos_reset;
@@ -137,15 +139,17 @@ struct TriFactor {
     const void* cdia;  // multiplier per position (S)
 };
 
-// A group of consecutive chunks of one system's triangular factor, by
-// processing position: chunks pos0 .. pos0 + count - 1, one per CTA of a
-// thread-block cluster.
+// One CTA's chunk in a group of chunks run by one thread-block cluster:
+// chunk pos0 of system sys's factor; count holds the kGroup flags.
 struct GroupTask {
     int sys;
     int pos0;
     int count;
     int pad;
 };
+constexpr int kGroupActive = 1;     // the CTA has a chunk in this group
+constexpr int kGroupPushNext = 2;   // the next CTA of the cluster holds the next chunk: push results into it
+constexpr int kGroupPushedIn = 4;   // the previous CTA holds the previous chunk and pushes into this one
 
 // Workspace vector slots.
 enum Vec : int {

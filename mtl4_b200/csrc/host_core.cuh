@@ -24,6 +24,7 @@ struct mtlg_ctx {
     int loop_mode = 0;          // tuning: 0 chunked plain graphs, 1 WHILE conditional graph
     int spmv_kernel = 0;        // tuning: 0 auto (row-length statistics), 1 stream tiles, 2 warp tasks
     int chunk_rows = 0;         // tuning: rows per sweep chunk of new preconditioners (0: by size)
+    int sweep_cluster = 0;      // tuning: CTAs per cluster of the chunked sweeps (0: automatic)
     int sweep_kernel = 0;       // tuning: 0 chunked waves, 1 flat level order
     int pc_apply_sync = 1;      // tuning: 1 each preconditioner apply checks its device waits (synchronizes), 0 queued
     int* d_scratch_err = nullptr;

@@ -33,6 +33,7 @@ struct TriDev {
     int max_slots = 0;  // receive slots of a chunk, at most
     DBuf<int> cseg, cxr, cext, crow, ccol, csrc, cmul;
     DBuf<int2> cquad;
+    DBuf<int> cqpull, cpush;
     DBuf<SegRec> segs;
     DBuf<unsigned> wv;
     DBuf<unsigned char> cval, cdia;    // storage type S
@@ -124,10 +125,12 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         open = true;
     };
     std::vector<int> pos_of(n, -1);   // position of each row in this layout
+    std::vector<int> cpbeg;            // first position of each chunk (and the end)
     for (int p = 0; p < nch; ++p) {
         const int ch = lower ? p : nch - 1 - p;
         const int r0 = ch * B, r1 = std::min(n, r0 + B);
         int nslot = 0;
+        cpbeg.push_back(int(crow.size()));
         for (int q = cbeg[p]; q < cbeg[p + 1];) {
             int qe = q + 1;
             while (qe < cbeg[p + 1] && qe - q < NT && lev[order[qe]] == lev[order[q]]) ++qe;
@@ -191,6 +194,23 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         cxr.push_back(int(cext.size()));
         T.max_slots = std::max(T.max_slots, nslot);
     }
+    cpbeg.push_back(int(crow.size()));
+    // pushes: a row of chunk p - 1 fills the first slot of chunk p that reads
+    // it (when the two chunks run in neighbouring CTAs of a cluster); the
+    // receivers fetch the other slots
+    std::vector<int> cpush(crow.size(), -1);
+    std::vector<char> pushed(cext.size(), 0);
+    for (int p = 1; p < nch; ++p)
+        for (int e = cxr[p]; e < cxr[p + 1]; ++e) {
+            const int x = cext[e];
+            if (x < cpbeg[p - 1] || x >= cpbeg[p] || cpush[x] >= 0) continue;
+            cpush[x] = e - cxr[p];
+            pushed[e] = 1;
+        }
+    std::vector<int> cqpull(cext.size() / 4 + 1, 0);
+    for (size_t q = 0; q < cext.size() / 4; ++q)
+        for (int j = 0; j < 4; ++j)
+            if (cext[4 * q + j] >= 0 && !pushed[4 * q + j]) cqpull[q] |= 1 << j;
     // receive quads (slots 4q .. 4q+3): {first position, mask of used slots};
     // first position -1 where the used slots are not four consecutive
     // positions starting 4-aligned (fetched one by one)
@@ -211,6 +231,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     // tails: a staged copy rounds each array's segment up to 16 bytes
     wv.resize(round4(int(wv.size())) + 4, 0u);
     crow.resize(round4(int(crow.size())) + 4, -1);
+    cpush.resize(crow.size(), -1);
     cext.resize(cext.size() + 4, 0);
     const int e = round4(int(ccol.size())) + 4;
     ccol.resize(e, -1);
@@ -230,6 +251,8 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     MTLG_TRY(T.cxr.upload(c, cxr.data(), cxr.size()));
     MTLG_TRY(T.cext.upload(c, cext.data(), cext.size()));
     MTLG_TRY(T.cquad.upload(c, cquad.data(), cquad.size()));
+    MTLG_TRY(T.cqpull.upload(c, cqpull.data(), cqpull.size()));
+    MTLG_TRY(T.cpush.upload(c, cpush.data(), cpush.size()));
     MTLG_TRY(T.segs.upload(c, segs.data(), segs.size()));
     MTLG_TRY(T.wv.upload(c, wv.data(), wv.size()));
     MTLG_TRY(T.crow.upload(c, crow.data(), crow.size()));
@@ -250,7 +273,8 @@ struct ChunkSide {
     int slots = 0;               // receive slots of the largest chunk
     int seg_rows = 0, seg_ents = 0;
     int smem = 0;                // dynamic shared memory per CTA
-    int resident = 1;            // CTAs resident at once
+    int resident = 1;            // CTAs resident at once (whole clusters)
+    int cl = 1;                  // CTAs per cluster
     int vec_bytes = 0;
     int cells = 0;               // shared cells of the largest chunk (rows, +0 cell, slots)
     void add(const TriDev& T)
@@ -269,7 +293,8 @@ struct ChunkSide {
 
 // Launch plan of the chunked sweeps of a set of factors (computed outside
 // any stream capture: it queries the occupancy): a shape per side and the
-// task lists.
+// task lists (ntl / ntu groups of cl GroupTask entries, one per CTA of a
+// cluster).
 struct ChunkPlan {
     bool ok = false;
     ChunkSide side[2];           // L [0], U [1]
@@ -290,22 +315,59 @@ struct ChunkShape {
                                        kChunkSmemMax));
         return MTLG_OK;
     }
-    static int occupancy(int smem)
+    // CTAs resident at once, in whole clusters of cl CTAs (0: does not fit)
+    static int resident(mtlg_ctx* c, int smem, int cl)
     {
+        if (cl == 1) {
+            int n = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_chunk<T, S, CW, RPT, KM>, THREADS,
+                                                              size_t(smem)) != cudaSuccess) {
+                cudaGetLastError();
+                return 0;
+            }
+            return n * c->sm_count;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = unsigned(cl);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(unsigned(cl * c->sm_count));
+        cfg.blockDim = dim3(THREADS);
+        cfg.dynamicSmemBytes = size_t(smem);
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_chunk<T, S, CW, RPT, KM>, THREADS, size_t(smem)) !=
-            cudaSuccess) {
+        if (cudaOccupancyMaxActiveClusters(&n, (const void*)k_sweep_chunk<T, S, CW, RPT, KM>, &cfg) != cudaSuccess) {
             cudaGetLastError();
             return 0;
         }
-        return n;
+        return n * cl;
     }
     static int launch(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const ChunkSweepOp& op, const ChunkSide& pl)
     {
-        const int grid = std::max(1, std::min(op.ntasks, pl.resident));
-        k_sweep_chunk<T, S, CW, RPT, KM><<<grid, THREADS, pl.smem, st>>>(sv, op);
+        const int grid = std::max(1, std::min(op.ntasks, pl.resident / pl.cl)) * pl.cl;
+        if (pl.cl == 1) {
+            k_sweep_chunk<T, S, CW, RPT, KM><<<grid, THREADS, pl.smem, st>>>(sv, op);
+            c->launches++;
+            MTLG_CUDA(cudaGetLastError());
+            return MTLG_OK;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = unsigned(pl.cl);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(unsigned(grid));
+        cfg.blockDim = dim3(THREADS);
+        cfg.dynamicSmemBytes = size_t(pl.smem);
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        MTLG_CUDA(cudaLaunchKernelEx(&cfg, k_sweep_chunk<T, S, CW, RPT, KM>, sv, op));
         c->launches++;
-        MTLG_CUDA(cudaGetLastError());
         return MTLG_OK;
     }
 };
@@ -352,10 +414,39 @@ inline bool with_chunk_shape(int nt, int km, Fn&& fn)
     return found;
 }
 
-// Shape and task list of a set of systems' factors (f[s]: the system's L and
-// U, or nulls for an unused slot); chunks of all systems interleaved by
-// processing position.  Not ok (flat sweeps) when a side's shape is not
-// built or its shared memory does not fit.
+// Groups of chunks, one per cluster of cl CTAs (cl GroupTask entries each):
+// each factor's chunks (nch[s] of system s, in processing order) in runs of
+// cl consecutive chunks, run by run (all systems' first runs, then their
+// second runs, ...), runs packed into groups while they fit; the chunks of a
+// run sit in neighbouring CTAs and push to each other.  Returns the number
+// of groups.
+inline int chunk_groups(const std::vector<int>& nch, int cl, std::vector<GroupTask>& g)
+{
+    g.clear();
+    int ng = 0, used = cl, maxch = 0;
+    for (int n : nch) maxch = std::max(maxch, n);
+    for (int a = 0; a < maxch; a += cl)
+        for (size_t s = 0; s < nch.size(); ++s) {
+            const int len = std::min(cl, nch[s] - a);
+            if (len <= 0) continue;
+            if (used + len > cl) {
+                g.resize(g.size() + size_t(cl), GroupTask{0, 0, 0, 0});
+                ++ng;
+                used = 0;
+            }
+            GroupTask* t = g.data() + size_t(ng - 1) * size_t(cl) + used;
+            for (int i = 0; i < len; ++i)
+                t[i] = GroupTask{int(s), a + i,
+                                 kGroupActive | (i + 1 < len ? kGroupPushNext : 0) | (i > 0 ? kGroupPushedIn : 0), 0};
+            used += len;
+        }
+    return ng;
+}
+
+// Shape and task lists of a set of systems' factors (f[s]: the system's L
+// and U, or nulls for an unused slot), in groups (chunk_groups) of the
+// side's cluster size.  Not ok (flat sweeps) when a side's shape is not built
+// or its shared memory does not fit.
 template <typename T, typename S>
 inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, const TriDev*>>& f, ChunkPlan& pl)
 {
@@ -379,28 +470,45 @@ inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, c
         sd.vec_bytes = int((size_t(sd.cells) * sizeof(T) + 15) / 16 * 16);
         sd.smem = sd.vec_bytes + kStageBufs * stage_bytes<S>(sd.seg_rows, sd.seg_ents);
         if (sd.smem > kChunkSmemMax) return MTLG_OK;
-        int occ = 0;
-        const int smem = sd.smem;
-        if (!with_chunk_shape<T, S>(sd.threads(), sd.entries(), [&](auto shape) { occ = decltype(shape)::occupancy(smem); }))
-            return MTLG_OK;
-        if (occ < 1) return MTLG_OK;
-        sd.resident = c->sm_count * occ;
     }
-    std::vector<GroupTask> tl, tu;
-    int maxch = 0;
-    for (const auto& lu : f)
-        if (lu.first) maxch = std::max({maxch, lu.first->nch, lu.second->nch});
-    for (int p = 0; p < maxch; ++p) {
-        for (size_t s = 0; s < f.size(); ++s) {
-            if (!f[s].first) continue;
-            if (p < f[s].first->nch) tl.push_back({int(s), p, 1, 0});
-            if (p < f[s].second->nch) tu.push_back({int(s), p, 1, 0});
+    for (int w = 0; w < 2; ++w) {
+        ChunkSide& sd = pl.side[w];
+        std::vector<int> nch(f.size(), 0);
+        int maxch = 0;
+        for (size_t s = 0; s < f.size(); ++s)
+            if (f[s].first) {
+                nch[s] = w == 0 ? f[s].first->nch : f[s].second->nch;
+                maxch = std::max(maxch, nch[s]);
+            }
+        // clusters when some factor has several chunks: the context's size,
+        // else 4 CTAs when about all groups run at once (a cluster takes its
+        // next group only when all of its CTAs are done, so queued groups of
+        // 4 leave CTAs idle), else 2; one CTA per chunk (taken in order as
+        // CTAs free up) when clusters do not fit
+        int res = 0, ng = 0;
+        std::vector<GroupTask> g;
+        const int smem = sd.smem;
+        const int cands[3] = {c->sweep_cluster > 0 ? c->sweep_cluster : 4, c->sweep_cluster > 0 ? 1 : 2, 1};
+        for (int cl : cands) {
+            if (cl > 1 && maxch < 2) continue;
+            if (!with_chunk_shape<T, S>(sd.threads(), sd.entries(),
+                                        [&](auto shape) { res = decltype(shape)::resident(c, smem, cl); }))
+                return MTLG_OK;
+            sd.cl = cl;
+            ng = chunk_groups(nch, cl, g);
+            const int rc = res / cl;   // clusters resident at once
+            if (cl == 1 || (rc >= 1 && (c->sweep_cluster > 0 || cl == 2 || 4 * ng <= 5 * rc))) break;
+        }
+        if (res < 1) return MTLG_OK;
+        sd.resident = res;
+        if (w == 0) {
+            pl.ntl = ng;
+            MTLG_TRY(pl.tl.upload(c, g.data(), std::max<size_t>(1, g.size())));
+        } else {
+            pl.ntu = ng;
+            MTLG_TRY(pl.tu.upload(c, g.data(), std::max<size_t>(1, g.size())));
         }
     }
-    pl.ntl = int(tl.size());
-    pl.ntu = int(tu.size());
-    MTLG_TRY(pl.tl.upload(c, tl.data(), std::max<size_t>(1, tl.size())));
-    MTLG_TRY(pl.tu.upload(c, tu.data(), std::max<size_t>(1, tu.size())));
     pl.ok = true;
     return MTLG_OK;
 }
@@ -413,6 +521,7 @@ inline int launch_chunk_sweep(mtlg_ctx* c, cudaStream_t st, const SetView& sv, C
     op.vec_bytes = pl.vec_bytes;
     op.rows_cap = pl.seg_rows;
     op.ents_cap = pl.seg_ents;
+    op.cl = pl.cl;
     int rc = MTLG_OK;
     if (!with_chunk_shape<T, S>(pl.threads(), pl.entries(),
                                 [&](auto shape) { rc = decltype(shape)::launch(c, st, sv, op, pl); })) {
@@ -443,6 +552,8 @@ inline TriFactor tri_view(const TriDev& T)
         f.cxr = T.cxr.p;
         f.cext = T.cext.p;
         f.cquad = T.cquad.p;
+        f.cqpull = T.cqpull.p;
+        f.cpush = T.cpush.p;
         f.ccol = T.ccol.p;
         f.cval = T.cval.p;
         f.cdia = T.cdia.p;

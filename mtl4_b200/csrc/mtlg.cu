@@ -127,7 +127,7 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
     MTLG_CUDA(cudaMemcpyAsync(P->desc.p, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
     ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
     int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
-    const int setting = c->sweep_kernel;
+    const int setting = c->sweep_kernel | (c->sweep_cluster << 4);
     if (made != setting) {
         std::vector<std::pair<const TriDev*, const TriDev*>> f(1, {&P->L, &P->U});
         MTLG_TRY((plan_chunks<T, S>(c, f, pl)));
@@ -354,6 +354,13 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
     else if (k == "pc_apply_sync") c->pc_apply_sync = value ? 1 : 0;
     else if (k == "chunk_rows") c->chunk_rows = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 15)));
+    else if (k == "sweep_cluster") {
+        if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8) {
+            set_error("sweep_cluster must be 0, 1, 2, 4 or 8");
+            return MTLG_ERR_INVALID_ARG;
+        }
+        c->sweep_cluster = int(value);
+    }
     else {
         set_error("unknown tuning key '%s'", key);
         return MTLG_ERR_INVALID_ARG;
@@ -375,6 +382,7 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     else if (k == "sweep_kernel") *value = c->sweep_kernel;
     else if (k == "pc_apply_sync") *value = c->pc_apply_sync;
     else if (k == "chunk_rows") *value = c->chunk_rows;
+    else if (k == "sweep_cluster") *value = c->sweep_cluster;
     else {
         set_error("unknown tuning key '%s'", key);
         return MTLG_ERR_INVALID_ARG;
@@ -814,7 +822,7 @@ static int sweep_plan_of(mtlg_ctx* c, mtlg_pc* P, int32_t* out)
 {
     ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
     int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
-    const int setting = c->sweep_kernel;
+    const int setting = c->sweep_kernel | (c->sweep_cluster << 4);
     if (made != setting) {
         std::vector<std::pair<const TriDev*, const TriDev*>> f(1, {&P->L, &P->U});
         MTLG_TRY((plan_chunks<T, S>(c, f, pl)));

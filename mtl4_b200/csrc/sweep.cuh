@@ -187,14 +187,17 @@ struct ChunkSweepOp {
     int vec_bytes;      // shared cells (chunk rows, the +0 cell, receive slots) of the largest chunk, 16-byte multiple
     int rows_cap;       // staging buffer capacity in rows (multiple of 4)
     int ents_cap;       // ... and in entries (multiple of 4)
+    int cl;             // cluster size the task table is built for (tasks: ntasks groups of cl entries)
+    int pad;
 };
 
 // Staging buffer layout: [wave sizes: rows_cap u32][rows: rows_cap int]
-// [multipliers: rows_cap S][columns: ents_cap int][values: ents_cap S].
+// [push cells: rows_cap int][multipliers: rows_cap S][columns: ents_cap int]
+// [values: ents_cap S].
 template <typename S>
 __host__ __device__ __forceinline__ int stage_bytes(int rows_cap, int ents_cap)
 {
-    return rows_cap * (8 + int(sizeof(S))) + ents_cap * (4 + int(sizeof(S)));
+    return rows_cap * (12 + int(sizeof(S))) + ents_cap * (4 + int(sizeof(S)));
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return unsigned(__cvta_generic_to_shared(p)); }
@@ -256,6 +259,7 @@ struct ChunkArrays {
     const SegRec* segs;
     const unsigned* wv;
     const int* crow;
+    const int* cpush;
     const void* cdia;
     const int* ccol;
     const void* cval;
@@ -269,11 +273,13 @@ __device__ __forceinline__ void stage_segment(const ChunkArrays& F, const SegRec
     const unsigned bw = round16u(unsigned(sg.nw) * 4u), br = round16u(unsigned(sg.np) * 4u);
     const unsigned bd = round16u(unsigned(sg.np) * unsigned(sizeof(S)));
     const unsigned bc = round16u(unsigned(sg.ne) * 4u), bv = round16u(unsigned(sg.ne) * unsigned(sizeof(S)));
-    mbar_expect_tx(bar, bw + br + bd + bc + bv);
+    mbar_expect_tx(bar, bw + 2 * br + bd + bc + bv);
     unsigned char* o = buf;
     bulk_g2s(o, F.wv + sg.w0, bw, bar);
     o += rows_cap * 4;
     bulk_g2s(o, F.crow + sg.p0, br, bar);
+    o += rows_cap * 4;
+    bulk_g2s(o, F.cpush + sg.p0, br, bar);
     o += rows_cap * 4;
     bulk_g2s(o, static_cast<const S*>(F.cdia) + sg.p0, bd, bar);
     o += rows_cap * int(sizeof(S));
@@ -394,11 +400,14 @@ __device__ __forceinline__ void st_slot4(double* p, const double* v)
 // positions moves with one vector load; the others slot by slot.  A value
 // that is still the sentinel is requested again (the slot keeps the sentinel
 // meanwhile); the wait is bounded like the others (on expiry the remaining
-// slots get a zero so the compute threads drain).
-template <typename T>
-__device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, const int2* __restrict__ cquad, int x0,
-                                              int nx, const T* ypos, T* slot, int rw, int lane, int* err,
-                                              int sleep_ns)
+// slots get a zero so the compute threads drain).  With cqpull (the previous
+// chunk runs in the previous CTA of the cluster and pushes its results into
+// this chunk's slots; PULL) only the slots in cqpull's masks are fetched, one
+// by one in quads that also hold pushed slots.
+template <typename T, bool PULL>
+__device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, const int2* __restrict__ cquad,
+                                              const int* __restrict__ cqpull, int x0, int nx, const T* ypos, T* slot,
+                                              int rw, int lane, int* err, int sleep_ns)
 {
     const int q0 = x0 >> 2, nq = nx >> 2;
     for (int row0 = rw; 32 * row0 < nq; row0 += kRecvWarps * kRecvDepth) {
@@ -412,6 +421,11 @@ __device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, cons
             if (qd[j] < nq) {
                 qi[j] = __ldg(cquad + q0 + qd[j]);
                 pend[j] = unsigned(qi[j].y);
+                if constexpr (PULL) {
+                    const unsigned pm = unsigned(__ldg(cqpull + q0 + qd[j]));
+                    if (pm != pend[j]) qi[j].x = -1;   // pushed slots stay untouched
+                    pend[j] = pm;
+                }
             }
         }
         long long spins = 0;
@@ -464,11 +478,32 @@ __device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, cons
     }
 }
 
+// Staging buffer views of segment buffer b.
+template <typename S>
+struct StageView {
+    const unsigned* wv;
+    const int* row;
+    const int* push;
+    const S* dia;
+    const int* col;
+    const S* val;
+    __device__ __forceinline__ StageView(const unsigned char* buf, int rows_cap, int ents_cap)
+        : wv(reinterpret_cast<const unsigned*>(buf)),
+          row(reinterpret_cast<const int*>(buf + rows_cap * 4)),
+          push(reinterpret_cast<const int*>(buf + rows_cap * 8)),
+          dia(reinterpret_cast<const S*>(buf + rows_cap * 12)),
+          col(reinterpret_cast<const int*>(buf + rows_cap * (12 + int(sizeof(S))))),
+          val(reinterpret_cast<const S*>(buf + rows_cap * (12 + int(sizeof(S))) + ents_cap * 4))
+    {
+    }
+};
+
 // One compute thread's rows of a staged wave, in registers (RPT rows: i, i + CT, ...).
 template <typename T, typename S, int RPT, int KM>
 struct WaveRows {
     int row[RPT];     // chunk-local index
-    int pos[RPT];     // position in the wave
+    int pos[RPT];     // position in the segment
+    int push[RPT];    // receive slot of the next chunk this row's result fills, or -1
     T rhs[RPT];
     S dia[RPT];
     int col[RPT][KM];
@@ -481,9 +516,9 @@ struct WaveRows {
 // with value 0, so the sweep needs no per-row branches; every index stays
 // inside the staged segment.
 template <typename T, typename S, int CT, int RPT, int KM>
-__device__ __forceinline__ void wave_rows(unsigned m, const int* srow, const S* sdia, const int* scol, const S* sval,
+__device__ __forceinline__ void wave_rows(unsigned m, const StageView<S>& V,
                                           const T* vec, int B, int r0, int poff, int eoff, int ents_cap, int lane,
-                                          WaveRows<T, S, RPT, KM>& r)
+                                          bool push, WaveRows<T, S, RPT, KM>& r)
 {
     const int nw = int(m & 0x7FFFu), K = int(m >> 16);
     const int kl = max(K - 1, 0);
@@ -492,13 +527,14 @@ __device__ __forceinline__ void wave_rows(unsigned m, const int* srow, const S* 
     for (int q = 0; q < RPT; ++q) {
         const int t = min(lane + CT * q, nw - 1);
         r.pos[q] = poff + t;
-        r.row[q] = srow[poff + t] - r0;
-        r.dia[q] = sdia[poff + t];
+        r.row[q] = V.row[poff + t] - r0;
+        r.push[q] = push && t == lane + CT * q ? V.push[poff + t] : -1;   // a repeated row pushes nothing
+        r.dia[q] = V.dia[poff + t];
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
             const int e = min(eoff + min(k, kl) * nw + t, elast);   // inside the wave's entries (K > 0)
-            const int c = scol[e];
-            const S v = sval[e];
+            const int c = V.col[e];
+            const S v = V.val[e];
             r.col[q][k] = k < K ? c : B;   // the +0 cell, value +0: neutral
             r.val[q][k] = k < K ? v : S(0);
         }
@@ -507,23 +543,44 @@ __device__ __forceinline__ void wave_rows(unsigned m, const int* srow, const S* 
     for (int q = 0; q < RPT; ++q) r.rhs[q] = vec[r.row[q]];
 }
 
-// Staging buffer views of segment buffer b.
-template <typename S>
-struct StageView {
-    const unsigned* wv;
-    const int* row;
-    const S* dia;
-    const int* col;
-    const S* val;
-    __device__ __forceinline__ StageView(const unsigned char* buf, int rows_cap, int ents_cap)
-        : wv(reinterpret_cast<const unsigned*>(buf)),
-          row(reinterpret_cast<const int*>(buf + rows_cap * 4)),
-          dia(reinterpret_cast<const S*>(buf + rows_cap * 8)),
-          col(reinterpret_cast<const int*>(buf + rows_cap * (8 + int(sizeof(S))))),
-          val(reinterpret_cast<const S*>(buf + rows_cap * (8 + int(sizeof(S))) + ents_cap * 4))
-    {
-    }
-};
+// Thread-block cluster helpers: rank and size, a barrier over all threads of
+// the cluster (release / acquire: what a CTA wrote before it, in its own or a
+// peer's shared memory, is visible after it), a peer's address of a shared
+// variable, and stores into a peer CTA's shared memory.
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_size()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+__device__ __forceinline__ unsigned peer_addr(const void* p, unsigned rank)
+{
+    unsigned a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+    return a;
+}
+__device__ __forceinline__ void st_peer(unsigned a, int v)
+{
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_peer_relaxed(unsigned a, float v)
+{
+    asm volatile("st.relaxed.cluster.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v));
+}
+__device__ __forceinline__ void st_peer_relaxed(unsigned a, double v)
+{
+    asm volatile("st.relaxed.cluster.shared::cluster.f64 [%0], %1;" ::"r"(a), "d"(v));
+}
 
 // Barrier among the CT compute threads (a warp barrier for one warp).
 template <int CW>
@@ -561,28 +618,31 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    const unsigned crank = cluster_rank(), csize = cluster_size();
+    if (int(csize) != op.cl) {   // task table built for another cluster size: report (uniform over the cluster)
+        if (tid == 0) atomicExch(sv.err, 1);
+        return;
+    }
+    cluster_sync();      // every CTA of the cluster runs before any writes into a peer's shared memory
     unsigned gseg = 0;   // segments staged and consumed by this CTA so far (uniform)
     for (;;) {
-        if (tid == 0) {
+        // the cluster's leader takes the next group of chunks for the cluster
+        if (tid == 0 && crank == 0) {
             const int t = atomicAdd(op.ticket, 1);
-            if (t == op.ntasks + int(gridDim.x) - 1) atomicExch(op.ticket, 0);
-            int go = 0;
-            if (t < op.ntasks) {
-                const GroupTask gt = op.tasks[t];
-                go = !skip_system(sv.st[gt.sys], op.skip) && !*(volatile int*)sv.err;
-            }
-            s_task = t;
-            s_go = go;
+            if (t == op.ntasks + int(gridDim.x / csize) - 1) atomicExch(op.ticket, 0);
+            for (unsigned r = 0; r < csize; ++r) st_peer(peer_addr(&s_task, r), t);
         }
+        cluster_sync();
+        const int t = s_task;
+        if (t >= op.ntasks) break;   // the same for the whole cluster
+        const GroupTask gt = op.tasks[size_t(t) * csize + crank];
+        if (tid == 0)
+            s_go = (gt.count & kGroupActive) && !skip_system(sv.st[gt.sys], op.skip) && !*(volatile int*)sv.err;
         __syncthreads();
-        const int t = s_task, go = s_go;
-        __syncthreads();
-        if (t >= op.ntasks) break;
-        if (!go) continue;
-        const GroupTask gt = op.tasks[t];
+        const int go = s_go;
         const SysDesc& d = sv.desc[gt.sys];
         const TriFactor& TF = op.which == 0 ? d.L : d.U;
-        const ChunkArrays F = {TF.segs, TF.wv, TF.crow, TF.cdia, TF.ccol, TF.cval};
+        const ChunkArrays F = {TF.segs, TF.wv, TF.crow, TF.cpush, TF.cdia, TF.ccol, TF.cval};
         const int pos = gt.pos0;
         const int B = TF.chunk_rows;
         const int r0 = (op.which == 0 ? pos : TF.nch - 1 - pos) * B;
@@ -591,9 +651,14 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
         const int x0 = TF.cxr[pos], nx = TF.cxr[pos + 1] - x0;
         const int* cext = TF.cext;
         T* ypos = static_cast<T*>(TF.ypos);
+        // pushes: this chunk's results fill receive slots of the next chunk,
+        // held by the next CTA of the cluster; the previous CTA fills ours
+        const bool push_out = go && (gt.count & kGroupPushNext);
+        const unsigned rvec = push_out ? peer_addr(vec, crank + 1) : 0u;
+        const int* cqpull = (gt.count & kGroupPushedIn) ? TF.cqpull : nullptr;
         // chunk prologue (all threads): right-hand sides, empty receive slots,
         // this chunk's share of the other factor's result reset
-        {
+        if (go) {
             const T* v = vptr<T>(d, op.in);
             for (int i = tid; i < nr; i += NTH) vec[i] = v[r0 + i];
             if (tid == 0) vec[B] = T(0);
@@ -602,8 +667,11 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
             const long long a = (long long)TF.npos_reset * pos / TF.nch, e = (long long)TF.npos_reset * (pos + 1) / TF.nch;
             for (long long i = a + tid; i < e; i += NTH) yr[i] = sentinel_value<T>();
         }
-        __syncthreads();
-        if (tid >= CT + 32 * kRecvWarps) {
+        // every chunk of the group has empty receive slots before any push
+        cluster_sync();
+        if (!go) {
+            // no chunk for this CTA in the group: the cluster's barriers only
+        } else if (tid >= CT + 32 * kRecvWarps) {
             // producer warp: stage the chunk's segments (lane 0)
             if (tid == CT + 32 * kRecvWarps) {
                 for (int i = 0; i < nseg; ++i) {
@@ -617,8 +685,12 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
             }
         } else if (tid >= CT) {
             // receiver warps
-            receive_chunk<T>(cext, TF.cquad, x0, nx, ypos, vec + B + kSlotBase, (tid - CT) >> 5, tid & 31, sv.err,
-                             op.sleep_ns);
+            if (cqpull)
+                receive_chunk<T, true>(cext, TF.cquad, cqpull, x0, nx, ypos, vec + B + kSlotBase, (tid - CT) >> 5,
+                                       tid & 31, sv.err, op.sleep_ns);
+            else
+                receive_chunk<T, false>(cext, TF.cquad, nullptr, x0, nx, ypos, vec + B + kSlotBase, (tid - CT) >> 5,
+                                        tid & 31, sv.err, op.sleep_ns);
         } else {
             // compute warps: all waves of the chunk, one cursor across
             // segments; the next wave's rows load while this one computes
@@ -630,7 +702,7 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
             int w = 0, poff = 0, eoff = 0;
             unsigned m = V.wv[0];
             WaveRows<T, S, RPT, KM> cur, nxt;
-            wave_rows<T, S, CT, RPT, KM>(m, V.row, V.dia, V.col, V.val, vec, B, r0, 0, 0, op.ents_cap, lane, cur);
+            wave_rows<T, S, CT, RPT, KM>(m, V, vec, B, r0, 0, 0, op.ents_cap, lane, push_out, cur);
             for (;;) {
                 // locate and load the next wave (possibly the next segment's first)
                 const int nw = int(m & 0x7FFFu);
@@ -668,7 +740,7 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
                         dv[q][k] = c >= 0 ? x : sentinel_value<T>();
                         wait |= is_sentinel(dv[q][k]);
                     }
-                if (has_next) wave_rows<T, S, CT, RPT, KM>(mn, Vn.row, Vn.dia, Vn.col, Vn.val, vec, B, r0, pn, en, op.ents_cap, lane, nxt);
+                if (has_next) wave_rows<T, S, CT, RPT, KM>(mn, Vn, vec, B, r0, pn, en, op.ents_cap, lane, push_out, nxt);
                 if (wait) {
 #pragma unroll
                     for (int q = 0; q < RPT; ++q)
@@ -688,6 +760,11 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
                     const T out = unsentinel(T(W(rr) * W(cur.dia[q])));
                     vec[cur.row[q]] = out;
                     st_relaxed_gpu(ypos + p0 + cur.pos[q], out);
+                    if (push_out) {
+                        // rows the next chunk does not read go to an unused cell
+                        const int ps = cur.push[q];
+                        st_peer_relaxed(rvec + unsigned(ps >= 0 ? B + kSlotBase + ps : B + 1) * unsigned(sizeof(T)), out);
+                    }
                 }
                 compute_barrier<CW>();
                 if (!has_next) break;
@@ -713,11 +790,11 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
             // last segment's buffer
             if (lane == 0) mbar_arrive(&empty[b]);
         }
-        gseg += unsigned(nseg);
         __syncthreads();
         // chunk epilogue (all warps): outputs and the reset of the buffer the
         // other sweep fills
-        {
+        if (go) {
+            gseg += unsigned(nseg);
             T* y = vptr<T>(d, op.out);
             T* R = op.reset != SLOT_NONE ? vptr<T>(d, op.reset) : nullptr;
             for (int i = tid; i < nr; i += NTH) {
@@ -725,6 +802,8 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
                 if (R) R[r0 + i] = sentinel_value<T>();
             }
         }
+        // the group's pushes have landed and its CTAs are done with s_task
+        cluster_sync();
     }
 }
 

@@ -102,6 +102,48 @@ def test_chunked_apply_matches_oracle(ctx, name, chunk_rows):
                 assert np.array_equal(y, ref), (name, chunk_rows, kind, mode)
 
 
+@pytest.mark.parametrize("cluster", [1, 2, 4, 8])
+def test_cluster_pushes_match_oracle(ctx, cluster):
+    # neighbouring chunks in one thread-block cluster hand their results over
+    # through shared memory; runs of chunks cross cluster groups, and a group
+    # may hold more chunks than fit at once
+    from mtl4_b200 import itl
+    A = P.vardiff_3d(24, sigma=1.0, seed=5, beta=(0.05, 0.02, 0.01))
+    x = np.random.default_rng(12).standard_normal(A.n_rows)
+    for chunk_rows in (96, 576, 2304):
+        with tuning(ctx, chunk_rows=chunk_rows, sweep_kernel=0, sweep_cluster=cluster):
+            Ad = dev(A, ctx)
+            for kind, dt in (("ilu_0", np.float64), ("ic_0", np.float32)):
+                Pc = getattr(itl.pc, kind)(Ad, dt)
+                assert Pc.sweep_plan(dt)["chunks"] > 1
+                for _ in range(2):
+                    y = itl.solve(Pc, vec(x.astype(dt), ctx, dt)).numpy()
+                    assert np.array_equal(y, O.port_pc_apply(A, kind, x.astype(dt))), (chunk_rows, kind)
+
+
+@pytest.mark.parametrize("cluster", [1, 8])
+def test_batch_cluster_groups_match_standalone(ctx, cluster):
+    # chunk runs of several systems packed into the groups of one cluster
+    from mtl4_b200 import itl, mtl, serve
+    probs = [P.vardiff_3d(m, sigma=0.5, seed=m, beta=(0.05, 0.02, 0.01)) for m in (7, 9, 12, 15)]
+    rhs = [P.random_rhs(A.n_rows, 4) for A in probs]
+    with tuning(ctx, chunk_rows=256, sweep_kernel=0, sweep_cluster=cluster):
+        B = serve.batch(ctx)
+        for A, b in zip(probs, rhs):
+            B.add(A, b, "bicgstab", "ilu_0", max_iter=2000, rtol=1e-8)
+        B.solve(mixed=False)
+        for i, (A, b) in enumerate(zip(probs, rhs)):
+            Ad = mtl.compressed2D.from_problem(A, ctx)
+            x = mtl.dense_vector(A.n_rows, np.float64, ctx)
+            bd = mtl.dense_vector(b, np.float64, ctx)
+            it = itl.basic_iteration(bd, 2000, 1e-8)
+            itl.bicgstab(Ad, x, bd, itl.pc.ilu_0(Ad), it)
+            r = B.result(i)
+            assert r.error_code == 0
+            assert r.iterations == it.iterations()
+            assert np.array_equal(r.x, x.numpy())
+
+
 def test_wave_split_beyond_cta(ctx):
     from mtl4_b200 import itl
     A = paired_blocks(9001)
