@@ -143,7 +143,8 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * 16384 for FP32 factors, 8192 for FP64), "sweep_cluster" (CTAs per
  * thread-block cluster of the chunked sweeps, whose neighbouring chunks
  * hand results over through shared memory: 1, 2, 4 or 8; 0, default:
- * chosen per plan), "pc_apply_sync" (1, default:
+ * chosen per plan), "vec_ctas_per_sm" (CTAs per SM of the fused vector
+ * passes, 1-16, default 2), "pc_apply_sync" (1, default:
  * mtlg_pc_apply waits for its sweeps and reports an expired device wait;
  * 0: it only enqueues them, and an expired wait is reported by the next
  * synchronous apply of the same preconditioner).

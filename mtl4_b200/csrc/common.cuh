@@ -285,40 +285,74 @@ __device__ __forceinline__ void block_reduce(double (&v)[ND], double* smem /* [N
     }
 }
 
-// Writes this tile's partial dots and reports whether the calling CTA is the
-// last of its system to do so (then it owns the system's finalize).  The
-// counter resets itself for the next pass.
+// Writes tile `tile`'s partial dots (block_reduce results, valid in thread 0).
 template <int ND>
-__device__ __forceinline__ bool publish_partials(const SetView& sv, int tile, int sys, const double (&v)[ND])
+__device__ __forceinline__ void store_partials(const SetView& sv, int tile, const double (&v)[ND])
 {
-    __shared__ int s_last;
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int j = 0; j < ND; ++j) sv.partials[(long long)tile * kMaxDots + j] = v[j];
-        __threadfence();
-        const unsigned ntiles = unsigned(sv.sys_tile_begin[sys + 1] - sv.sys_tile_begin[sys]);
-        const unsigned prev = atomicAdd(&sv.counters[sys], 1u);
-        s_last = (prev == ntiles - 1);
+    }
+}
+
+// A CTA's count of finished tiles of one system (tiles whose partials it has
+// stored), published with one atomic when the CTA moves on to another system
+// or ends: one atomic per CTA and system instead of one per tile.
+struct TileTally {
+    int sys = -1;
+    unsigned n = 0;
+    unsigned need = 0;   // tiles that complete the system (0: all of its SpMV tiles)
+};
+
+// Publishes the tally (whole CTA, tally uniform) and reports whether it
+// completed the system's tiles: the calling CTA then owns the system's
+// finalize.  The counter resets itself for the next pass.
+__device__ __forceinline__ bool publish_tally(const SetView& sv, TileTally& tt)
+{
+    __shared__ int s_last;
+    if (tt.n == 0) return false;
+    if (threadIdx.x == 0) {
+        __threadfence();   // this CTA's partials before its count
+        const unsigned ntiles =
+            tt.need ? tt.need : unsigned(sv.sys_tile_begin[tt.sys + 1] - sv.sys_tile_begin[tt.sys]);
+        const unsigned prev = atomicAdd(&sv.counters[tt.sys], tt.n);
+        s_last = (prev + tt.n == ntiles);
         if (s_last) {
-            sv.counters[sys] = 0;
+            sv.counters[tt.sys] = 0;
             __threadfence();
         }
     }
     __syncthreads();
-    return s_last != 0;
+    const bool last = s_last != 0;
+    __syncthreads();
+    tt.n = 0;
+    return last;
 }
 
-// Sum of a system's tile partials in tile order (deterministic); called by
-// the whole last CTA, result valid in thread 0.
+// Sum of a system's tile partials (its first `count` tiles, or all of its
+// SpMV tiles) in tile order (deterministic: thread i adds tiles i,
+// i + blockDim, ... in turn, loads issued 8 tiles at a time); called by the
+// whole last CTA, result valid in thread 0.
 template <int ND>
-__device__ __forceinline__ void gather_partials(const SetView& sv, int sys, double (&out)[ND], double* smem)
+__device__ __forceinline__ void gather_partials(const SetView& sv, int sys, double (&out)[ND], double* smem,
+                                                int count = -1)
 {
-    const int t0 = sv.sys_tile_begin[sys], t1 = sv.sys_tile_begin[sys + 1];
+    const int t0 = sv.sys_tile_begin[sys], t1 = count >= 0 ? t0 + count : sv.sys_tile_begin[sys + 1];
+    const int B = blockDim.x;
 #pragma unroll
     for (int j = 0; j < ND; ++j) out[j] = 0.0;
-    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+    for (int t = t0 + threadIdx.x; t < t1; t += 8 * B) {
+        double v[8][ND];
 #pragma unroll
-        for (int j = 0; j < ND; ++j) out[j] += __ldcg(&sv.partials[(long long)t * kMaxDots + j]);
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int j = 0; j < ND; ++j)
+                v[u][j] = t + u * B < t1 ? __ldcg(&sv.partials[(long long)(t + u * B) * kMaxDots + j]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int j = 0; j < ND; ++j)
+                if (t + u * B < t1) out[j] += v[u][j];
     }
     block_reduce<ND>(out, smem);
 }

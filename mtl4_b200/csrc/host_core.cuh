@@ -25,6 +25,7 @@ struct mtlg_ctx {
     int spmv_kernel = 0;        // tuning: 0 auto (row-length statistics), 1 stream tiles, 2 warp tasks
     int chunk_rows = 0;         // tuning: rows per sweep chunk of new preconditioners (0: by size)
     int sweep_cluster = 0;      // tuning: CTAs per cluster of the chunked sweeps (0: automatic)
+    int vec_ctas_per_sm = 2;    // tuning: CTAs per SM of the vector passes
     int sweep_kernel = 0;       // tuning: 0 chunked waves, 1 flat level order
     int pc_apply_sync = 1;      // tuning: 1 each preconditioner apply checks its device waits (synchronizes), 0 queued
     int* d_scratch_err = nullptr;
@@ -342,7 +343,9 @@ template <typename T>
 inline int launch_vec(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const VecOp& op)
 {
     if (sv.n_tiles == 0) return MTLG_OK;
-    dim3 g(sv.n_tiles), b(kBlock);
+    // one CTA per run of tiles, vec_ctas_per_sm per SM at most (each CTA
+    // publishes its dot tally with one atomic on the system's counter)
+    dim3 g(std::min(sv.n_tiles, c->vec_ctas_per_sm * c->sm_count)), b(kBlock);
     switch (op.op) {
 #define MTLG_VEC_CASE(OP) \
     case OP: k_vec<T, OP><<<g, b, 0, st>>>(sv, op); break;

@@ -355,6 +355,18 @@ __device__ __forceinline__ void stage_tile(const Tile& t, const int* rp, const i
 // then sums one row sequentially; rows longer than kShortRow are summed by a
 // warp from shared memory.  A long tile (one row with more than kTileNnz
 // entries) is summed by the whole CTA straight from global memory.
+// Publishes a CTA's tally of a system's finished SpMV tiles; the CTA that
+// completes the system gathers its partials and finalizes.
+template <typename OpT>
+__device__ __forceinline__ void spmv_publish(const SetView& sv, const OpT& op, TileTally& tally, double* s_red)
+{
+    if (publish_tally(sv, tally)) {
+        double tot[kMaxDots];
+        gather_partials<kMaxDots>(sv, tally.sys, tot, s_red);
+        if (threadIdx.x == 0) finalize(sv, op.fin, tally.sys, tot);
+    }
+}
+
 template <typename T, int XF, int ASG>
 __global__ void __launch_bounds__(kBlock, 3) k_spmv(SetView sv, SpmvOp op)
 {
@@ -374,6 +386,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_spmv(SetView sv, SpmvOp op)
     const int G = gridDim.x;
     int t = blockIdx.x;
     if (t >= sv.n_tiles) return;
+    TileTally tally;   // finished tiles of the current system, published per system run
 
     Tile cur = sv.tiles[t];
     {
@@ -399,6 +412,10 @@ __global__ void __launch_bounds__(kBlock, 3) k_spmv(SetView sv, SpmvOp op)
 
         const Tile tile = cur;
         const int sys = tile.sys;
+        if (op.fin != FIN_NONE && sys != tally.sys) {
+            spmv_publish(sv, op, tally, s_red);
+            tally.sys = sys;
+        }
         const SysDesc& d = sv.desc[sys];
         const SysState& s = sv.st[sys];
         if (!skip_system(s, op.skip)) {
@@ -509,11 +526,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_spmv(SetView sv, SpmvOp op)
             if (op.fin != FIN_NONE) {
                 double dd[kMaxDots] = {d0, d1, 0.0, 0.0};
                 block_reduce<kMaxDots>(dd, s_red);
-                if (publish_partials<kMaxDots>(sv, t, sys, dd)) {
-                    double tot[kMaxDots];
-                    gather_partials<kMaxDots>(sv, sys, tot, s_red);
-                    if (threadIdx.x == 0) finalize(sv, op.fin, sys, tot);
-                }
+                store_partials<kMaxDots>(sv, t, dd);
+                ++tally.n;
             }
         }
         __syncthreads();   // the buffer is refilled two tiles later
@@ -521,6 +535,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_spmv(SetView sv, SpmvOp op)
         nxt = nn;
     }
     cp_async_wait_0();
+    if (op.fin != FIN_NONE) spmv_publish(sv, op, tally, s_red);
 }
 
 // ---------------------------------------------------------------- SpMV, warp tasks
@@ -663,93 +678,157 @@ __device__ __forceinline__ T vpick(const T* const* v, int j, int code, int i, co
     return v[j][i];
 }
 
-template <typename T, int OP>
-__global__ void __launch_bounds__(kBlock) k_vec(SetView sv, VecOp op)
+// Publishes a CTA's tally of a system's finished vector-pass tiles; the CTA
+// that completes the system gathers its partials and finalizes (or retires a
+// finishing BiCGSTAB system).
+template <int OP>
+__device__ __forceinline__ void vec_publish(const SetView& sv, const VecOp& op, TileTally& tally, double* s_red)
 {
-    __shared__ double s_red[kMaxDots * 32];
-    const int tile_id = blockIdx.x;
-    const Tile tile = sv.tiles[tile_id];
-    const int sys = tile.sys;
-    const SysDesc& d = sv.desc[sys];
-    SysState& s = sv.st[sys];
-    if (op.count_body && tile_id == 0 && threadIdx.x == 0) {
-        int runs = atomicAdd(&sv.err[1], 1) + 1;
-        if (runs > sv.err[2] || *(volatile int*)sv.running <= 0) set_cond(sv, 0u);
-    }
-    if (skip_system(s, op.skip)) return;
-
-    const T* dinv = static_cast<const T*>(d.inv_diag);
-    const T* dv[3 * kMaxDots];
-    for (int j = 0; j < kMaxDots; ++j) {
-        dv[3 * j + 0] = (j < op.ndot && names_vector(op.da[j])) ? vptr<T>(d, op.da[j]) : nullptr;
-        dv[3 * j + 1] = (j < op.ndot && names_vector(op.db[j])) ? vptr<T>(d, op.db[j]) : nullptr;
-        dv[3 * j + 2] = (j < op.ndot && names_vector(op.dc[j])) ? vptr<T>(d, op.dc[j]) : nullptr;
-    }
-    T* A = op.a != SLOT_NONE ? vptr<T>(d, op.a) : nullptr;
-    T* B = op.b != SLOT_NONE ? vptr<T>(d, op.b) : nullptr;
-    T* C = op.c != SLOT_NONE ? vptr<T>(d, op.c) : nullptr;
-    T* E = op.e != SLOT_NONE ? vptr<T>(d, op.e) : nullptr;
-    T* F = op.f != SLOT_NONE ? vptr<T>(d, op.f) : nullptr;
-    T* G = op.g != SLOT_NONE ? vptr<T>(d, op.g) : nullptr;
-    const bool finishing = (s.flags & FLAG_FINISHING) != 0;
-    const T alpha = T(s.alpha), beta = T(s.beta), omega = T(s.omega);
-    const bool first = (s.iter <= 1);
-    double dot[kMaxDots] = {0.0, 0.0, 0.0, 0.0};
-
-    for (int i = tile.row_begin + threadIdx.x; i < tile.row_end; i += blockDim.x) {
-        if (OP == VOP_AXPY) {
-            A[i] = fma(T(op.scalar), B[i], A[i]);                       // A += s B
-        } else if (OP == VOP_CG_UPDATE) {
-            A[i] = fma(alpha, B[i], A[i]);                              // x += alpha p
-            C[i] = fma(-alpha, E[i], C[i]);                             // r -= alpha q
-        } else if (OP == VOP_BI_P) {
-            // p = r + beta * (p - omega * v)     (bicgstab.hpp:49-53)
-            A[i] = first ? B[i] : fma(beta, fma(-omega, C[i], A[i]), B[i]);
-        } else if (OP == VOP_BI_S) {
-            A[i] = fma(-alpha, C[i], B[i]);                             // s = r - alpha v
-        } else if (OP == VOP_BI_XR) {
-            // A x, B phat, C shat, E s, F t, G r
-            if (finishing) {
-                A[i] = fma(alpha, B[i], A[i]);                          // x += alpha phat
-            } else {
-                A[i] = A[i] + fma(omega, C[i], alpha * B[i]);           // x += omega shat + alpha phat
-                G[i] = fma(-omega, F[i], E[i]);                         // r = s - omega t
-            }
-        } else if (OP == VOP_REF_CAST) {
-            // inner right-hand side float(r64 / ||r64||); inner x = 0, r = b
-            const T bi = T(d.r64[i] / s.scale);
-            A[i] = bi;
-            if (B) B[i] = T(0);
-            if (C) C[i] = bi;
-            if (E) E[i] = bi;
-        } else if (OP == VOP_REF_UPDATE) {
-            d.x64[i] = fma(s.scale, double(A[i]), d.x64[i]);          // x += ||r|| * d
-        } else if (OP == VOP_FILL) {
-            A[i] = T(op.scalar);
-        } else if (OP == VOP_COPY) {
-            A[i] = B[i];
-        } else if (OP == VOP_SCALE_COPY) {
-            A[i] = T(op.scalar) * B[i];
-        }
-        for (int j = 0; j < op.ndot; ++j) {
-            dot[j] += double(vpick<T>(dv, 3 * j + 0, op.da[j], i, dinv) * vpick<T>(dv, 3 * j + 1, op.db[j], i, dinv) *
-                             vpick<T>(dv, 3 * j + 2, op.dc[j], i, dinv));
-        }
-    }
-    if (op.fin == FIN_NONE && !(OP == VOP_BI_XR && finishing)) return;
-    block_reduce<kMaxDots>(dot, s_red);
-    if (publish_partials<kMaxDots>(sv, tile_id, sys, dot)) {
+    const int count = int(tally.need);
+    if (publish_tally(sv, tally)) {
         double tot[kMaxDots];
-        gather_partials<kMaxDots>(sv, sys, tot, s_red);
+        gather_partials<kMaxDots>(sv, tally.sys, tot, s_red, count);
         if (threadIdx.x == 0) {
-            if (OP == VOP_BI_XR && finishing) {
+            SysState& s = sv.st[tally.sys];
+            if (OP == VOP_BI_XR && (s.flags & FLAG_FINISHING)) {
                 s.flags &= ~FLAG_FINISHING;
                 retire(sv, s, (int)s.dots[3], s.error);
             } else {
-                finalize(sv, op.fin, sys, tot);
+                finalize(sv, op.fin, tally.sys, tot);
             }
         }
     }
+}
+
+constexpr int kVecGroup = 4;   // tiles a vector-pass CTA works on at once (one row of each per thread)
+
+// A vector pass splits each system into row tiles of kTileRows (tile v:
+// rows v kTileRows .. + kTileRows), as many as fit in the system's share of
+// the SpMV tile indices (at least that many: SpMV tiles hold at most
+// kTileRows rows), whose partial slots it uses.  One CTA per run of
+// consecutive tile indices (the launch sizes the grid to the SMs),
+// kVecGroup tiles of one system at a time (thread k takes row k of each, so
+// its loads of the group's rows are in flight together, with no tile
+// metadata to read); the system's vectors and scalars are read once per run.
+// Each tile's partial dots are block reduced on their own in a fixed order,
+// so the sums do not depend on the grid, the grouping or the batch.
+template <typename T, int OP>
+__global__ void __launch_bounds__(kBlock) k_vec(SetView sv, VecOp op)
+{
+    static_assert(kBlock == kTileRows, "a vector-pass thread takes one row of each tile");
+    constexpr int NR = kVecGroup * kMaxDots;
+    __shared__ double s_red[NR * 32];
+    if (op.count_body && blockIdx.x == 0 && threadIdx.x == 0) {
+        int runs = atomicAdd(&sv.err[1], 1) + 1;
+        if (runs > sv.err[2] || *(volatile int*)sv.running <= 0) set_cond(sv, 0u);
+    }
+    const int t_begin = int((long long)sv.n_tiles * blockIdx.x / gridDim.x);
+    const int t_end = int((long long)sv.n_tiles * (blockIdx.x + 1) / gridDim.x);
+    TileTally tally;
+    int t = t_begin;
+    while (t < t_end) {
+        const int sys = sv.tiles[t].sys;
+        const int tb = sv.sys_tile_begin[sys];
+        const int te = min(t_end, sv.sys_tile_begin[sys + 1]);   // this system's tile indices in the CTA's range
+        const SysDesc& d = sv.desc[sys];
+        const int n = sv.tiles[sv.sys_tile_begin[sys + 1] - 1].row_end;   // its rows (the last tile's end)
+        const int nvt = (n + kTileRows - 1) / kTileRows;                   // its row tiles
+        if (sys != tally.sys) {
+            vec_publish<OP>(sv, op, tally, s_red);
+            tally.sys = sys;
+            tally.need = unsigned(nvt);
+        }
+        SysState& s = sv.st[sys];
+        if (skip_system(s, op.skip)) {
+            t = te;
+            continue;
+        }
+        const T* dinv = static_cast<const T*>(d.inv_diag);
+        const T* dv[3 * kMaxDots];
+#pragma unroll
+        for (int j = 0; j < kMaxDots; ++j) {
+            dv[3 * j + 0] = (j < op.ndot && names_vector(op.da[j])) ? vptr<T>(d, op.da[j]) : nullptr;
+            dv[3 * j + 1] = (j < op.ndot && names_vector(op.db[j])) ? vptr<T>(d, op.db[j]) : nullptr;
+            dv[3 * j + 2] = (j < op.ndot && names_vector(op.dc[j])) ? vptr<T>(d, op.dc[j]) : nullptr;
+        }
+        T* A = op.a != SLOT_NONE ? vptr<T>(d, op.a) : nullptr;
+        T* B = op.b != SLOT_NONE ? vptr<T>(d, op.b) : nullptr;
+        T* C = op.c != SLOT_NONE ? vptr<T>(d, op.c) : nullptr;
+        T* E = op.e != SLOT_NONE ? vptr<T>(d, op.e) : nullptr;
+        T* F = op.f != SLOT_NONE ? vptr<T>(d, op.f) : nullptr;
+        T* G = op.g != SLOT_NONE ? vptr<T>(d, op.g) : nullptr;
+        const bool finishing = (s.flags & FLAG_FINISHING) != 0;
+        const T alpha = T(s.alpha), beta = T(s.beta), omega = T(s.omega);
+        const bool first = (s.iter <= 1);
+        const double scale = s.scale;
+        const bool reduce = op.fin != FIN_NONE || (OP == VOP_BI_XR && finishing);
+        // one row: the pass and its dot terms
+        auto row = [&](int i, double* dot) {
+            if (OP == VOP_AXPY) {
+                A[i] = fma(T(op.scalar), B[i], A[i]);                       // A += s B
+            } else if (OP == VOP_CG_UPDATE) {
+                A[i] = fma(alpha, B[i], A[i]);                              // x += alpha p
+                C[i] = fma(-alpha, E[i], C[i]);                             // r -= alpha q
+            } else if (OP == VOP_BI_P) {
+                // p = r + beta * (p - omega * v)     (bicgstab.hpp:49-53)
+                A[i] = first ? B[i] : fma(beta, fma(-omega, C[i], A[i]), B[i]);
+            } else if (OP == VOP_BI_S) {
+                A[i] = fma(-alpha, C[i], B[i]);                             // s = r - alpha v
+            } else if (OP == VOP_BI_XR) {
+                // A x, B phat, C shat, E s, F t, G r
+                if (finishing) {
+                    A[i] = fma(alpha, B[i], A[i]);                          // x += alpha phat
+                } else {
+                    A[i] = A[i] + fma(omega, C[i], alpha * B[i]);           // x += omega shat + alpha phat
+                    G[i] = fma(-omega, F[i], E[i]);                         // r = s - omega t
+                }
+            } else if (OP == VOP_REF_CAST) {
+                // inner right-hand side float(r64 / ||r64||); inner x = 0, r = b
+                const T bi = T(d.r64[i] / scale);
+                A[i] = bi;
+                if (B) B[i] = T(0);
+                if (C) C[i] = bi;
+                if (E) E[i] = bi;
+            } else if (OP == VOP_REF_UPDATE) {
+                d.x64[i] = fma(scale, double(A[i]), d.x64[i]);            // x += ||r|| * d
+            } else if (OP == VOP_FILL) {
+                A[i] = T(op.scalar);
+            } else if (OP == VOP_COPY) {
+                A[i] = B[i];
+            } else if (OP == VOP_SCALE_COPY) {
+                A[i] = T(op.scalar) * B[i];
+            }
+#pragma unroll
+            for (int j = 0; j < kMaxDots; ++j)
+                if (j < op.ndot)
+                    dot[j] += double(vpick<T>(dv, 3 * j + 0, op.da[j], i, dinv) * vpick<T>(dv, 3 * j + 1, op.db[j], i, dinv) *
+                                     vpick<T>(dv, 3 * j + 2, op.dc[j], i, dinv));
+        };
+        for (; t < te; t += kVecGroup) {
+            const int v0 = t - tb;
+            const int ng = max(0, min(min(kVecGroup, te - t), nvt - v0));   // row tiles among these indices
+            double dot[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) dot[k] = 0.0;
+#pragma unroll
+            for (int q = 0; q < kVecGroup; ++q) {
+                const int i = (v0 + q) * kTileRows + int(threadIdx.x);
+                if (q < ng && i < n) row(i, dot + q * kMaxDots);
+            }
+            if (!reduce || ng == 0) continue;
+            block_reduce<NR>(dot, s_red);
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int q = 0; q < kVecGroup; ++q)
+                    if (q < ng)
+#pragma unroll
+                        for (int j = 0; j < kMaxDots; ++j) sv.partials[(long long)(t + q) * kMaxDots + j] = dot[q * kMaxDots + j];
+            }
+            tally.n += unsigned(ng);
+        }
+        t = te;
+    }
+    vec_publish<OP>(sv, op, tally, s_red);
 }
 
 }  // namespace mtlg

@@ -354,6 +354,7 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
     else if (k == "pc_apply_sync") c->pc_apply_sync = value ? 1 : 0;
     else if (k == "chunk_rows") c->chunk_rows = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 15)));
+    else if (k == "vec_ctas_per_sm") c->vec_ctas_per_sm = int(std::max<int64_t>(1, std::min<int64_t>(value, 16)));
     else if (k == "sweep_cluster") {
         if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8) {
             set_error("sweep_cluster must be 0, 1, 2, 4 or 8");
@@ -383,6 +384,7 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     else if (k == "pc_apply_sync") *value = c->pc_apply_sync;
     else if (k == "chunk_rows") *value = c->chunk_rows;
     else if (k == "sweep_cluster") *value = c->sweep_cluster;
+    else if (k == "vec_ctas_per_sm") *value = c->vec_ctas_per_sm;
     else {
         set_error("unknown tuning key '%s'", key);
         return MTLG_ERR_INVALID_ARG;
