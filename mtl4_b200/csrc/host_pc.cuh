@@ -430,7 +430,9 @@ inline int chunk_groups(const std::vector<int>& nch, int cl, std::vector<GroupTa
             const int len = std::min(cl, nch[s] - a);
             if (len <= 0) continue;
             if (used + len > cl) {
-                g.resize(g.size() + size_t(cl), GroupTask{0, 0, 0, 0});
+                // CTAs without a chunk in the group read the descriptors of
+                // the group's first chunk (a live system) and do nothing else
+                g.resize(g.size() + size_t(cl), GroupTask{int(s), a, 0, 0});
                 ++ng;
                 used = 0;
             }

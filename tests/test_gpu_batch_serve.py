@@ -76,6 +76,24 @@ def test_batch_bicgstab_ilu0(ctx):
 
 @pytest.mark.parametrize("mixed", [True, False])
 def test_served_alone_equals_in_mix(ctx, mixed):
+    served_alone_equals_in_mix(ctx, mixed)
+
+
+def test_served_mix_in_clusters(ctx):
+    # small chunks and 4-CTA clusters: every request spans several chunks,
+    # cluster groups hold CTAs without a chunk, and slots (slot 0 among
+    # them) fall free while the others still run
+    old = {k: ctx.get_tuning(k) for k in ("chunk_rows", "sweep_cluster")}
+    try:
+        ctx.set_tuning("chunk_rows", 512)
+        ctx.set_tuning("sweep_cluster", 4)
+        served_alone_equals_in_mix(ctx, True)
+    finally:
+        for k, v in old.items():
+            ctx.set_tuning(k, v)
+
+
+def served_alone_equals_in_mix(ctx, mixed):
     from mtl4_b200 import serve
     sys_ = small_specs(10, seed=21)
     reqs = [(A, b, "cg", sp.pc, 3000) for sp, A, b in sys_]
