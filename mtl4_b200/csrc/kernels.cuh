@@ -543,6 +543,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_spmv(SetView sv, SpmvOp op)
 // either a run of consecutive rows with at most kWarpNnz entries in total
 // (and at most kWarpNnz rows), or one row with more entries.
 constexpr int kWarpNnz = 256;
+constexpr int kSeqRow = 32;   // rows of a run task summed by one lane in storage order
 
 struct WarpTask {
     int row_begin, row_end, nnz_begin, nnz_end;
@@ -550,9 +551,10 @@ struct WarpTask {
 
 // Run tasks: lanes load values and columns with coalesced loads and issue up
 // to 8 independent x gathers each; the rounded products go to shared memory
-// and every lane then sums whole rows from there, sequentially in storage
-// order (so each row's result is bitwise that of a sequential row sum).  No
-// CTA barrier: warps proceed independently.  Long-row tasks: the warp strides
+// and every lane then sums whole rows of up to kSeqRow entries from there,
+// sequentially in storage order (so such a row's result is bitwise that of a
+// sequential row sum); longer rows are summed by the whole warp.  No CTA
+// barrier: warps proceed independently.  Long-row tasks: the warp strides
 // over the row (8 gathers in flight per lane) and reduces with a fixed tree.
 template <typename T, int ASG>
 __global__ void __launch_bounds__(kBlock, 3)
@@ -604,12 +606,34 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restric
             if (k < k1) prod[lane + 32 * u] = mul_rn(av[u], xv[u]);
         }
         __syncwarp();
-        for (int r = lane; r < nr; r += 32) {
-            T acc = T(0);
-            for (int e = srp[r]; e < srp[r + 1]; ++e) acc = add_rn(acc, prod[e]);
-            const int row = task.row_begin + r;
-            const T base = (ASG == ASG_SET) ? T(0) : y[row];
-            y[row] = assign_out<T, ASG>(base, acc);
+        // rows of up to kSeqRow entries: one lane each, summed sequentially
+        // (bitwise the sequential row sum); longer rows: the whole warp,
+        // lane-strided partial sums and a fixed shuffle tree, so no lane
+        // walks a long row alone while the others wait
+        for (int base = 0; base < nr; base += 32) {
+            const int r = base + lane;
+            const bool seq = r < nr && srp[r + 1] - srp[r] <= kSeqRow;
+            if (seq) {
+                T acc = T(0);
+                for (int e = srp[r]; e < srp[r + 1]; ++e) acc = add_rn(acc, prod[e]);
+                const int row = task.row_begin + r;
+                const T yb = (ASG == ASG_SET) ? T(0) : y[row];
+                y[row] = assign_out<T, ASG>(yb, acc);
+            }
+            unsigned lng = __ballot_sync(0xffffffffu, r < nr && !seq);
+            while (lng) {
+                const int rr = base + __ffs(lng) - 1;
+                lng &= lng - 1;
+                T acc = T(0);
+                for (int e = srp[rr] + lane; e < srp[rr + 1]; e += 32) acc = add_rn(acc, prod[e]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                if (lane == 0) {
+                    const int row = task.row_begin + rr;
+                    const T yb = (ASG == ASG_SET) ? T(0) : y[row];
+                    y[row] = assign_out<T, ASG>(yb, acc);
+                }
+            }
         }
         __syncwarp();
     }

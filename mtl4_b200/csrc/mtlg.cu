@@ -216,7 +216,7 @@ int launch_spmv_rows(mtlg_ctx* c, mtlg_csr* A, const void* x, void* y, int asg)
     if (A->wtasks.empty()) return MTLG_OK;
     if (!A->d_wtasks.p) MTLG_TRY(A->d_wtasks.upload(c, A->wtasks.data(), A->wtasks.size()));
     const int ntasks = int(A->wtasks.size());
-    const int grid = std::min((ntasks + 7) / 8, c->sm_count * 4);
+    const int grid = std::min((ntasks + 7) / 8, c->sm_count * 3);   // the CTAs resident at once (80 registers)
     const T* va = std::is_same<T, float>::value ? (const T*)A->v32.p : (const T*)A->v64.p;
     switch (asg) {
     case ASG_SET: k_spmv_rows<T, ASG_SET><<<grid, kBlock, 0, c->stream>>>(A->d_wtasks.p, ntasks, A->rp.p, A->ci.p, va, (const T*)x, (T*)y); break;
