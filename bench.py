@@ -41,7 +41,7 @@ WORKLOAD = ("BiCGSTAB+ILU(0) on 128^3 7-point convection-diffusion (2,097,152 un
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 # DRAM bytes (read + write) of one FP32 ILU(0) apply (L and U k_sweep_chunk
 # launches) from ncu on this workload; see profiles/k_sweep_chunk_ilu0_convdiff128_f32.md
-TRAFFIC_PER_APPLY = 203_350_000   # 101.0 MB (L) + 102.3 MB (U)
+TRAFFIC_PER_APPLY = 210_680_000   # 105.1 MB (L) + 105.5 MB (U)
 FALLBACK_HBM = 6650.0
 
 
