@@ -142,7 +142,7 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * "chunk_rows" (rows per chunk of preconditioners created afterwards; 0:
  * 16384 for FP32 factors, 8192 for FP64), "sweep_cluster" (CTAs per
  * thread-block cluster of the chunked sweeps, whose neighbouring chunks
- * hand results over through shared memory: 1, 2, 4 or 8; 0, default:
+ * hand results over through shared memory: 1, 2, 4, 8 or 16; 0, default:
  * chosen per plan), "vec_ctas_per_sm" (CTAs per SM of the fused vector
  * passes, 1-16, default 2), "pc_apply_sync" (1, default:
  * mtlg_pc_apply waits for its sweeps and reports an expired device wait;

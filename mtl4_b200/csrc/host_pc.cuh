@@ -313,6 +313,10 @@ struct ChunkShape {
     {
         MTLG_CUDA(cudaFuncSetAttribute(k_sweep_chunk<T, S, CW, RPT, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kChunkSmemMax));
+        // clusters of 16 CTAs (beyond the portable 8) where the device has them
+        if (cudaFuncSetAttribute(k_sweep_chunk<T, S, CW, RPT, KM>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess)
+            cudaGetLastError();
         return MTLG_OK;
     }
     // CTAs resident at once, in whole clusters of cl CTAs (0: does not fit)
@@ -483,14 +487,15 @@ inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, c
                 maxch = std::max(maxch, nch[s]);
             }
         // clusters when some factor has several chunks: the context's size,
-        // else 4 CTAs when about all groups run at once (a cluster takes its
-        // next group only when all of its CTAs are done, so queued groups of
-        // 4 leave CTAs idle), else 2; one CTA per chunk (taken in order as
-        // CTAs free up) when clusters do not fit
+        // else the largest of 16, 8, 4 CTAs whose groups run at once (a
+        // cluster takes its next group only when all of its CTAs are done, so
+        // queued groups leave CTAs idle), else 2; one CTA per chunk (taken in
+        // order as CTAs free up) when clusters do not fit
         int res = 0, ng = 0;
         std::vector<GroupTask> g;
         const int smem = sd.smem;
-        const int cands[3] = {c->sweep_cluster > 0 ? c->sweep_cluster : 4, c->sweep_cluster > 0 ? 1 : 2, 1};
+        const bool forced = c->sweep_cluster > 0;
+        const int cands[5] = {forced ? c->sweep_cluster : 16, forced ? 1 : 8, forced ? 1 : 4, forced ? 1 : 2, 1};
         for (int cl : cands) {
             if (cl > 1 && maxch < 2) continue;
             if (!with_chunk_shape<T, S>(sd.threads(), sd.entries(),
@@ -499,7 +504,10 @@ inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, c
             sd.cl = cl;
             ng = chunk_groups(nch, cl, g);
             const int rc = res / cl;   // clusters resident at once
-            if (cl == 1 || (rc >= 1 && (c->sweep_cluster > 0 || cl == 2 || 4 * ng <= 5 * rc))) break;
+            // 16 and 8 only when every group is resident at once, 4 when
+            // about all are, 2 always
+            const bool fits = cl >= 8 ? ng <= rc : cl == 4 ? 4 * ng <= 5 * rc : true;
+            if (cl == 1 || (rc >= 1 && (forced || fits))) break;
         }
         if (res < 1) return MTLG_OK;
         sd.resident = res;

@@ -356,8 +356,8 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "chunk_rows") c->chunk_rows = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 15)));
     else if (k == "vec_ctas_per_sm") c->vec_ctas_per_sm = int(std::max<int64_t>(1, std::min<int64_t>(value, 16)));
     else if (k == "sweep_cluster") {
-        if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8) {
-            set_error("sweep_cluster must be 0, 1, 2, 4 or 8");
+        if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16) {
+            set_error("sweep_cluster must be 0, 1, 2, 4, 8 or 16");
             return MTLG_ERR_INVALID_ARG;
         }
         c->sweep_cluster = int(value);
