@@ -147,7 +147,13 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * passes, 1-16, default 2), "pc_apply_sync" (1, default:
  * mtlg_pc_apply waits for its sweeps and reports an expired device wait;
  * 0: it only enqueues them, and an expired wait is reported by the next
- * synchronous apply of the same preconditioner).
+ * synchronous apply of the same preconditioner), "reduction_order" (FP64
+ * dots and norms of mtlg_dot, mtlg_two_norm, mtlg_spmv_dot and the CG /
+ * BiCGSTAB solves: 0, default, tile-parallel sums; 1, the reference build's
+ * summation order -- four strided partial sums per reduction, combined as
+ * mtl::dot, two_norm and the fused lazy dots do -- so that FP64 results and
+ * iteration counts equal the reference's bitwise, at about a microsecond
+ * per thousand entries per reduction).
  * Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
 int mtlg_ctx_set_tuning(mtlg_ctx* ctx, const char* key, int64_t value);
 int mtlg_ctx_get_tuning(mtlg_ctx* ctx, const char* key, int64_t* value);

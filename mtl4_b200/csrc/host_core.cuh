@@ -1,6 +1,7 @@
 // Host side: context, device memory accounting, CSR / vector handles, tiling.
 #pragma once
 #include "sweep.cuh"
+#include "refdot.cuh"
 
 #include <algorithm>
 #include <memory>
@@ -28,6 +29,7 @@ struct mtlg_ctx {
     int vec_ctas_per_sm = 2;    // tuning: CTAs per SM of the vector passes
     int sweep_kernel = 0;       // tuning: 0 chunked waves, 1 flat level order
     int pc_apply_sync = 1;      // tuning: 1 each preconditioner apply checks its device waits (synchronizes), 0 queued
+    int red_order = 0;          // tuning: FP64 dots and norms, 0 tile-parallel, 1 the reference's summation order
     int* d_scratch_err = nullptr;
     int sweep_blocks() const
     {
@@ -318,13 +320,68 @@ inline int init_kernel_shapes()
     MTLG_TRY((SpmvShape<float, XF, ASG>::init()));
     MTLG_SPMV_VARIANTS(MTLG_SPMV_INIT)
 #undef MTLG_SPMV_INIT
+    MTLG_CUDA(cudaFuncSetAttribute(k_dot_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDots * kRefWarpSmem));
     return MTLG_OK;
+}
+
+// Reference summation order (tuning "reduction_order" 1, FP64 only): a pass
+// that reduces dots runs without them, and k_dot_ref then reduces the same
+// vectors in the reference's order and finalizes.  Operand codes of the SpMV
+// epilogue (its output y, its transformed input x') name the vectors that
+// hold those values once the pass has run.
+template <typename T>
+inline bool ref_order_active(const mtlg_ctx* c, int ndot, int fin)
+{
+    return std::is_same<T, double>::value && c->red_order == 1 && ndot > 0 && fin != FIN_NONE;
+}
+
+inline int launch_dot_ref(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const RefDotOp& r)
+{
+    if (sv.n_sys == 0) return MTLG_OK;
+    k_dot_ref<<<sv.n_sys, 32 * r.ndot, r.ndot * kRefWarpSmem, st>>>(sv, r);
+    c->launches++;
+    return MTLG_OK;
+}
+
+template <typename OpT>
+inline RefDotOp ref_dot_op(const OpT& op)
+{
+    RefDotOp r;
+    memset(&r, 0, sizeof r);
+    r.ndot = op.ndot;
+    for (int j = 0; j < kMaxDots; ++j) {
+        r.va[j] = op.da[j]; r.vb[j] = op.db[j]; r.vc[j] = op.dc[j];
+        r.rk[j] = op.rk[j];
+    }
+    r.fin = op.fin;
+    r.skip = op.skip;
+    return r;
 }
 
 template <typename T>
 inline int launch_spmv(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const SpmvOp& op, int xf, int asg)
 {
     if (sv.n_tiles == 0) return MTLG_OK;
+    if (ref_order_active<T>(c, op.ndot, op.fin)) {
+        RefDotOp r = ref_dot_op(op);
+        auto resolve = [&](int code) {
+            if (code == OPND_Y) return op.y;
+            if (code == OPND_XP) return xf == XF_PLAIN ? op.x : op.pnew;
+            return code;
+        };
+        for (int j = 0; j < op.ndot; ++j) {
+            r.va[j] = resolve(op.da[j]); r.vb[j] = resolve(op.db[j]); r.vc[j] = resolve(op.dc[j]);
+            if (r.va[j] == SLOT_NONE || r.vb[j] == SLOT_NONE || r.vc[j] == SLOT_NONE) {
+                set_error("reference-order dot of an SpMV operand that is not stored");
+                return MTLG_ERR_NOT_SUPPORTED;
+            }
+        }
+        SpmvOp plain = op;
+        plain.ndot = 0;
+        plain.fin = FIN_NONE;
+        MTLG_TRY(launch_spmv<T>(c, st, sv, plain, xf, asg));
+        return launch_dot_ref(c, st, sv, r);
+    }
     const int smem = 2 * StageLayout<T>::BYTES;
 #define MTLG_SPMV_CASE(XF, ASG)                                                                    \
     if (xf == XF && asg == ASG) {                                                                 \
@@ -343,6 +400,14 @@ template <typename T>
 inline int launch_vec(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const VecOp& op)
 {
     if (sv.n_tiles == 0) return MTLG_OK;
+    if (ref_order_active<T>(c, op.ndot, op.fin)) {
+        // a finishing BiCGSTAB system still retires in the plain x/r pass
+        VecOp plain = op;
+        plain.ndot = 0;
+        plain.fin = FIN_NONE;
+        MTLG_TRY(launch_vec<T>(c, st, sv, plain));
+        return launch_dot_ref(c, st, sv, ref_dot_op(op));
+    }
     // one CTA per run of tiles, vec_ctas_per_sm per SM at most (each CTA
     // publishes its dot tally with one atomic on the system's counter)
     dim3 g(std::min(sv.n_tiles, c->vec_ctas_per_sm * c->sm_count)), b(kBlock);

@@ -289,6 +289,15 @@ inline void set_dot(VecOp& op, int j, int a, int b, int c = OPND_ONE)
     op.da[j] = a; op.db[j] = b; op.dc[j] = c;
     op.ndot = std::max(op.ndot, j + 1);
 }
+// The reference expression a dot stands for, which fixes its summation order
+// under "reduction_order" 1 (RK_DOT4 unless set): mtl::dot, two_norm, or the
+// lazy_dot / lazy_unary_dot of a fused expression.
+template <typename OpT>
+inline void set_kinds(OpT& op, int k0, int k1 = RK_DOT4)
+{
+    op.rk[0] = k0;
+    op.rk[1] = k1;
+}
 
 // ------------------------------------------------------------------ CG
 // Reference body (itl/krylov/cg.hpp:76-111):
@@ -311,9 +320,10 @@ inline int cg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inner_
     }
     SpmvOp op = spmv_op_default();
     op.x = SLOT_X; op.w = SLOT_B; op.y = V_R;
-    set_dot(op, 0, OPND_Y, OPND_Y);
-    if (ss.path == PATH_JACOBI) { set_dot(op, 1, OPND_Y, OPND_Y, OPND_D); op.fin = FIN_CG_INIT_JAC; }
+    set_dot(op, 0, OPND_Y, OPND_Y);      // rr = dot(r, r)
+    if (ss.path == PATH_JACOBI) { set_dot(op, 1, OPND_Y, OPND_Y, OPND_D); op.fin = FIN_CG_INIT_JAC; }   // dot(r, z)
     else op.fin = FIN_CG_INIT;
+    set_kinds(op, RK_DOT4, RK_DOT4);
     if (skip >= 0) op.skip = skip;
     return launch_spmv<T>(c, st, sv, op, XF_PLAIN, ASG_WMINUS);
 }
@@ -328,7 +338,8 @@ inline int cg_half(SolveSet& ss, cudaStream_t st, const SetView& sv, int pin, in
         MTLG_TRY(launch_sweep<T>(ss, st, sv, 0, V_R, V_Z0, V_Z, SKIP_INNER, 0));
         MTLG_TRY(launch_sweep<T>(ss, st, sv, 1, V_Z0, V_Z, V_Z0, SKIP_INNER, 1));
         VecOp d = vec_op_default(VOP_DOT);
-        set_dot(d, 0, V_R, V_Z);
+        set_dot(d, 0, V_R, V_Z);   // rho = dot(r, z)
+        set_kinds(d, RK_DOT4);
         d.fin = FIN_CG_RHO;
         d.skip = SKIP_INNER;
         d.count_body = 0;
@@ -339,17 +350,19 @@ inline int cg_half(SolveSet& ss, cudaStream_t st, const SetView& sv, int pin, in
     }
     SpmvOp op = spmv_op_default();
     op.z = zslot; op.p = pin; op.pnew = pout; op.y = V_Q;
-    set_dot(op, 0, OPND_XP, OPND_Y);
+    set_dot(op, 0, OPND_XP, OPND_Y);   // (q = A p) || (alpha_1 = lazy_dot(p, q))
+    set_kinds(op, RK_LDOT4);
     op.fin = FIN_CG_ALPHA;
     op.skip = SKIP_INNER;
     op.count_body = count ? 1 : 0;
     MTLG_TRY(launch_spmv<T>(c, st, sv, op, xf, ASG_SET));
     VecOp u = vec_op_default(VOP_CG_UPDATE);
     u.a = SLOT_X; u.b = pout; u.c = V_R; u.e = V_Q;
-    set_dot(u, 0, V_R, V_R);
-    if (ss.path == PATH_JACOBI) { set_dot(u, 1, V_R, V_R, OPND_D); u.fin = FIN_CG_UPDATE_JAC; }
+    set_dot(u, 0, V_R, V_R);   // (r -= alpha q) || (rr = lazy_unary_dot(r))
+    if (ss.path == PATH_JACOBI) { set_dot(u, 1, V_R, V_R, OPND_D); u.fin = FIN_CG_UPDATE_JAC; }   // dot(r, z)
     else if (ss.path == PATH_IDENTITY) u.fin = FIN_CG_UPDATE;
     else u.fin = FIN_CG_UPDATE_PC;
+    set_kinds(u, RK_UDOT4, RK_DOT4);
     u.skip = SKIP_INNER;
     return launch_vec<T>(c, st, sv, u);
 }
@@ -372,8 +385,9 @@ inline int bicg_init(SolveSet& ss, cudaStream_t st, const SetView& sv, bool inne
     }
     SpmvOp op = spmv_op_default();
     op.x = SLOT_X; op.w = SLOT_B; op.y = V_R; op.y2 = V_RT;   // r = b - A x; rtilde = r
-    set_dot(op, 0, OPND_Y, OPND_Y);
-    set_dot(op, 1, OPND_Y, OPND_Y);
+    set_dot(op, 0, OPND_Y, OPND_Y);   // rho_1 = dot(rtilde, r)
+    set_dot(op, 1, OPND_Y, OPND_Y);   // finished(r): two_norm(r)
+    set_kinds(op, RK_DOT4, RK_NORM4);
     op.fin = FIN_BI_TOP;
     if (skip >= 0) op.skip = skip;
     return launch_spmv<T>(c, st, sv, op, XF_PLAIN, ASG_WMINUS);
@@ -400,14 +414,16 @@ inline int bicg_body(SolveSet& ss, cudaStream_t st, const SetView& sv)
     }
     SpmvOp v = spmv_op_default();
     v.x = xin; v.y = V_V; v.pnew = pn;
-    set_dot(v, 0, V_RT, OPND_Y);
+    set_dot(v, 0, V_RT, OPND_Y);   // gamma = dot(rtilde, v)
+    set_kinds(v, RK_DOT4);
     v.fin = FIN_BI_GAMMA;
     v.skip = SKIP_INNER;
     MTLG_TRY(launch_spmv<T>(c, st, sv, v, xf, ASG_SET));
     // s = r - alpha v ; finished(s)?
     VecOp sop = vec_op_default(VOP_BI_S);
     sop.a = V_S; sop.b = V_R; sop.c = V_V;
-    set_dot(sop, 0, V_S, V_S);
+    set_dot(sop, 0, V_S, V_S);   // finished(s): two_norm(s)
+    set_kinds(sop, RK_NORM4);
     sop.fin = FIN_BI_S;
     sop.skip = SKIP_INNER;
     MTLG_TRY(launch_vec<T>(c, st, sv, sop));
@@ -423,16 +439,18 @@ inline int bicg_body(SolveSet& ss, cudaStream_t st, const SetView& sv)
     }
     SpmvOp t = spmv_op_default();
     t.x = sin; t.y = V_T; t.pnew = sn;
-    set_dot(t, 0, OPND_Y, V_S);
-    set_dot(t, 1, OPND_Y, OPND_Y);
+    set_dot(t, 0, OPND_Y, V_S);      // dot(t, s)
+    set_dot(t, 1, OPND_Y, OPND_Y);   // dot(t, t)
+    set_kinds(t, RK_DOT4, RK_DOT4);
     t.fin = FIN_BI_OMEGA;
     t.skip = SKIP_INNER;
     MTLG_TRY(launch_spmv<T>(c, st, sv, t, xf, ASG_SET));
     // x += omega shat + alpha phat ; r = s - omega t ; loop-top tests
     VecOp xr = vec_op_default(VOP_BI_XR);
     xr.a = SLOT_X; xr.b = phat; xr.c = shat; xr.e = V_S; xr.f = V_T; xr.g = V_R;
-    set_dot(xr, 0, V_RT, V_R);
-    set_dot(xr, 1, V_R, V_R);
+    set_dot(xr, 0, V_RT, V_R);   // rho_1 = dot(rtilde, r)
+    set_dot(xr, 1, V_R, V_R);    // finished(r): two_norm(r)
+    set_kinds(xr, RK_DOT4, RK_NORM4);
     xr.fin = FIN_BI_TOP;
     xr.skip = SKIP_RUNNING;
     return launch_vec<T>(c, st, sv, xr);
@@ -619,7 +637,8 @@ inline int run_plain(SolveSet& ss)
     const SetView sv = ss.view(false, false);
     if (need_nb) {
         VecOp nb = vec_op_default(VOP_DOT);
-        set_dot(nb, 0, SLOT_B, SLOT_B);
+        set_dot(nb, 0, SLOT_B, SLOT_B);   // basic_iteration(b, ...): two_norm(b)
+        set_kinds(nb, RK_NORM4);
         nb.fin = FIN_NORM_R0;
         MTLG_TRY(launch_vec<T>(c, c->stream, sv, nb));
     }

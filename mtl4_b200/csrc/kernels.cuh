@@ -4,11 +4,14 @@
 // (boost/numeric/mtl/operation/mat_vec_mult.hpp:614-683): every row is an
 // accumulator started at zero and updated entry by entry in storage order,
 // tmp += A.data[j] * v[A.ref_minor()[j]], then assigned/added/subtracted
-// into w (Assign::first_update).  The product is rounded before the addition
-// (the reference build does not fuse this loop).  Rows of up to kShortRow
-// entries keep that exact order (one thread per row), so their results are
-// bitwise the reference's in FP64 and FP32.  Longer rows are split over a
-// warp (or the whole CTA) and summed as a fixed tree.
+// into w (Assign::first_update).  The reference build (g++ -O3 with FMA
+// available) evaluates that loop in groups of four entries whose products
+// are rounded before the addition, and the row's last (L mod 4) entries as
+// fused multiply-adds; in FP32 every product is rounded first.  row_step
+// reproduces this, so rows of up to kShortRow entries, which keep the exact
+// order (one thread per row), are bitwise the reference's in FP64 and FP32.
+// Longer rows are split over a warp (or the whole CTA) and summed as a fixed
+// tree.
 #pragma once
 #include "common.cuh"
 
@@ -222,6 +225,7 @@ struct SpmvOp {
     int p, z, pnew;     // XF_CG_*: old p, z (or r), new p
     int ndot;
     int da[kMaxDots], db[kMaxDots], dc[kMaxDots];
+    int rk[kMaxDots];   // reference summation order of each dot (RK_*, refdot.cuh)
     int fin;
     int skip;
     int count_body;     // increments the body counter (first kernel of a loop body)
@@ -239,6 +243,16 @@ __device__ __forceinline__ bool skip_system(const SysState& s, int mode)
 // acc + a*x with the product rounded first (no contraction)
 __device__ __forceinline__ double mac(double acc, double a, double x) { return __dadd_rn(acc, __dmul_rn(a, x)); }
 __device__ __forceinline__ float mac(float acc, float a, float x) { return __fadd_rn(acc, __fmul_rn(a, x)); }
+// One step of a sequential row sum: entries before the row's last (L mod 4)
+// add the rounded product, the last ones are fused (FP64 only), as in the
+// reference build's row loop.  `fused` = the entry lies in that tail.
+__device__ __forceinline__ double row_step(double acc, double a, double x, bool fused)
+{
+    return fused ? __fma_rn(a, x, acc) : mac(acc, a, x);
+}
+__device__ __forceinline__ float row_step(float acc, float a, float x, bool) { return mac(acc, a, x); }
+// first entry of a row's fused tail: a + 4 * floor((e - a) / 4)
+__device__ __forceinline__ int fused_tail(int a, int e) { return a + ((e - a) & ~3); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
@@ -455,19 +469,21 @@ __global__ void __launch_bounds__(kBlock, 3) k_spmv(SetView sv, SpmvOp op)
                     if (e - a <= kShortRow) {
                         // gathers issued 8 at a time, summed in storage order
                         T acc = T(0);
+                        const int q = fused_tail(a, e);
                         int k = a;
                         for (; k + 8 <= e; k += 8) {
                             T xv[8];
 #pragma unroll
                             for (int u = 0; u < 8; ++u) xv[u] = xin(s_col[k + u - ca]);
 #pragma unroll
-                            for (int u = 0; u < 8; ++u) acc = mac(acc, s_val[k + u - ka], xv[u]);
+                            for (int u = 0; u < 8; ++u) acc = row_step(acc, s_val[k + u - ka], xv[u], k + u >= q);
                         }
                         T xv[8];
 #pragma unroll
                         for (int u = 0; u < 8; ++u) if (k + u < e) xv[u] = xin(s_col[k + u - ca]);
 #pragma unroll
-                        for (int u = 0; u < 8; ++u) if (k + u < e) acc = mac(acc, s_val[k + u - ka], xv[u]);
+                        for (int u = 0; u < 8; ++u)
+                            if (k + u < e) acc = row_step(acc, s_val[k + u - ka], xv[u], k + u >= q);
                         epi(i, acc, xin(i), dinv, d0, d1);
                     } else {
                         s_med[atomicAdd(&s_nmed, 1)] = i;
@@ -550,10 +566,10 @@ struct WarpTask {
 };
 
 // Run tasks: lanes load values and columns with coalesced loads and issue up
-// to 8 independent x gathers each; the rounded products go to shared memory
+// to 8 independent x gathers each; values and gathered x go to shared memory
 // and every lane then sums whole rows of up to kSeqRow entries from there,
-// sequentially in storage order (so such a row's result is bitwise that of a
-// sequential row sum); longer rows are summed by the whole warp.  No CTA
+// sequentially in storage order with row_step (so such a row's result is
+// bitwise the reference's row sum); longer rows are summed by the whole warp.  No CTA
 // barrier: warps proceed independently.  Long-row tasks: the warp strides
 // over the row (8 gathers in flight per lane) and reduces with a fixed tree.
 template <typename T, int ASG>
@@ -561,11 +577,13 @@ __global__ void __launch_bounds__(kBlock, 3)
 k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restrict__ rp, const int* __restrict__ ci,
             const T* __restrict__ va, const T* __restrict__ x, T* __restrict__ y)
 {
-    __shared__ T s_prod[kBlock / 32][kWarpNnz];
+    __shared__ T s_a[kBlock / 32][kWarpNnz];
+    __shared__ T s_x[kBlock / 32][kWarpNnz];
     __shared__ int s_rp[kBlock / 32][kWarpNnz + 1];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int gw = blockIdx.x * (blockDim.x >> 5) + wib, nwarps = gridDim.x * (blockDim.x >> 5);
-    T* prod = s_prod[wib];
+    T* sa = s_a[wib];
+    T* sx = s_x[wib];
     int* srp = s_rp[wib];
     for (int t = gw; t < ntasks; t += nwarps) {
         const WarpTask task = tasks[t];
@@ -603,7 +621,7 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restric
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int k = k0 + lane + 32 * u;
-            if (k < k1) prod[lane + 32 * u] = mul_rn(av[u], xv[u]);
+            if (k < k1) { sa[lane + 32 * u] = av[u]; sx[lane + 32 * u] = xv[u]; }
         }
         __syncwarp();
         // rows of up to kSeqRow entries: one lane each, summed sequentially
@@ -615,7 +633,8 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restric
             const bool seq = r < nr && srp[r + 1] - srp[r] <= kSeqRow;
             if (seq) {
                 T acc = T(0);
-                for (int e = srp[r]; e < srp[r + 1]; ++e) acc = add_rn(acc, prod[e]);
+                const int q = fused_tail(srp[r], srp[r + 1]);
+                for (int e = srp[r]; e < srp[r + 1]; ++e) acc = row_step(acc, sa[e], sx[e], e >= q);
                 const int row = task.row_begin + r;
                 const T yb = (ASG == ASG_SET) ? T(0) : y[row];
                 y[row] = assign_out<T, ASG>(yb, acc);
@@ -625,7 +644,7 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restric
                 const int rr = base + __ffs(lng) - 1;
                 lng &= lng - 1;
                 T acc = T(0);
-                for (int e = srp[rr] + lane; e < srp[rr + 1]; e += 32) acc = add_rn(acc, prod[e]);
+                for (int e = srp[rr] + lane; e < srp[rr + 1]; e += 32) acc = mac(acc, sa[e], sx[e]);
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
                 if (lane == 0) {
@@ -648,7 +667,7 @@ k_spmv_scalar(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
               const T* __restrict__ x, T* __restrict__ y)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int a = rp[i], e = rp[i + 1];
+        const int a = rp[i], e = rp[i + 1], q = fused_tail(a, e);
         T acc = T(0);
         int k = a;
         for (; k + 8 <= e; k += 8) {
@@ -656,13 +675,13 @@ k_spmv_scalar(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
 #pragma unroll
             for (int u = 0; u < 8; ++u) { av[u] = va[k + u]; xv[u] = x[ci[k + u]]; }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) acc = mac(acc, av[u], xv[u]);
+            for (int u = 0; u < 8; ++u) acc = row_step(acc, av[u], xv[u], k + u >= q);
         }
         T xv[8], av[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) if (k + u < e) { av[u] = va[k + u]; xv[u] = x[ci[k + u]]; }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) if (k + u < e) acc = mac(acc, av[u], xv[u]);
+        for (int u = 0; u < 8; ++u) if (k + u < e) acc = row_step(acc, av[u], xv[u], k + u >= q);
         const T base = (ASG == ASG_SET) ? T(0) : y[i];
         y[i] = assign_out<T, ASG>(base, acc);
     }
@@ -688,6 +707,7 @@ struct VecOp {
     int a, b, c, e, f, g;   // slots (meaning per op)
     int ndot;
     int da[kMaxDots], db[kMaxDots], dc[kMaxDots];
+    int rk[kMaxDots];   // reference summation order of each dot (RK_*, refdot.cuh)
     int fin;
     int skip;
     int count_body;
@@ -803,7 +823,9 @@ __global__ void __launch_bounds__(kBlock) k_vec(SetView sv, VecOp op)
                 if (finishing) {
                     A[i] = fma(alpha, B[i], A[i]);                          // x += alpha phat
                 } else {
-                    A[i] = A[i] + fma(omega, C[i], alpha * B[i]);           // x += omega shat + alpha phat
+                    // x += omega shat + alpha phat, evaluated as the reference
+                    // build does: x + fma(alpha, phat, omega shat)
+                    A[i] = A[i] + fma(alpha, B[i], omega * C[i]);
                     G[i] = fma(-omega, F[i], E[i]);                         // r = s - omega t
                 }
             } else if (OP == VOP_REF_CAST) {

@@ -17,9 +17,10 @@ struct SetKey {
     const mtlg_csr* A;
     const mtlg_pc* P;
     int solver, f32, mixed;
+    int red_order;   // the loop graphs hold the reduction kernels of that mode
     bool operator<(const SetKey& o) const
     {
-        return std::tie(A, P, solver, f32, mixed) < std::tie(o.A, o.P, o.solver, o.f32, o.mixed);
+        return std::tie(A, P, solver, f32, mixed, red_order) < std::tie(o.A, o.P, o.solver, o.f32, o.mixed, o.red_order);
     }
 };
 
@@ -353,6 +354,7 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
     else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
     else if (k == "pc_apply_sync") c->pc_apply_sync = value ? 1 : 0;
+    else if (k == "reduction_order") c->red_order = value ? 1 : 0;
     else if (k == "chunk_rows") c->chunk_rows = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 15)));
     else if (k == "vec_ctas_per_sm") c->vec_ctas_per_sm = int(std::max<int64_t>(1, std::min<int64_t>(value, 16)));
     else if (k == "sweep_cluster") {
@@ -382,6 +384,7 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     else if (k == "sm_count") *value = c->sm_count;
     else if (k == "sweep_kernel") *value = c->sweep_kernel;
     else if (k == "pc_apply_sync") *value = c->pc_apply_sync;
+    else if (k == "reduction_order") *value = c->red_order;
     else if (k == "chunk_rows") *value = c->chunk_rows;
     else if (k == "sweep_cluster") *value = c->sweep_cluster;
     else if (k == "vec_ctas_per_sm") *value = c->vec_ctas_per_sm;
@@ -613,7 +616,8 @@ static int spmv_impl(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, i
     op.x = SLOT_X;
     op.y = SLOT_B;
     if (pq) {
-        set_dot(op, 0, OPND_XP, OPND_Y);
+        set_dot(op, 0, OPND_XP, OPND_Y);   // (q = A p) || lazy_dot(p, q)
+        set_kinds(op, RK_LDOT4);
         op.fin = FIN_STORE;
     }
     const int asg = assign == MTLG_ASSIGN ? ASG_SET : (assign == MTLG_PLUS ? ASG_ADD : ASG_SUB);
@@ -657,7 +661,8 @@ int mtlg_spmv_dot(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* p, mtlg_vec* q, doub
     return spmv_impl(c, A, p, q, MTLG_ASSIGN, pq);
 }
 
-static int vec_binary(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, int kind, double scalar, double* out)
+static int vec_binary(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, int kind, double scalar, double* out,
+                      int rk = RK_DOT4)
 {
     MTLG_CHECK_ARG(c && x && y, "null handle");
     MTLG_CHECK_ARG(x->dtype == y->dtype, "dtypes differ");
@@ -679,6 +684,7 @@ static int vec_binary(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, int kin
     VecOp op = vec_op_default(kind);
     if (kind == VOP_DOT) {
         set_dot(op, 0, SLOT_X, SLOT_B);
+        set_kinds(op, rk);
         op.fin = FIN_STORE;
     } else {  // VOP_AXPY: y += a x
         op.a = SLOT_B;
@@ -701,7 +707,7 @@ int mtlg_dot(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, double* out)
 int mtlg_two_norm(mtlg_ctx* c, const mtlg_vec* x, double* out)
 {
     MTLG_CHECK_ARG(out, "out");
-    MTLG_TRY(vec_binary(c, x, x, VOP_DOT, 0.0, out));
+    MTLG_TRY(vec_binary(c, x, x, VOP_DOT, 0.0, out, RK_NORM4));
     *out = sqrt(fabs(*out));
     return MTLG_OK;
 }
@@ -916,7 +922,7 @@ int mtlg_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* L, mtlg_pc* R, mtl
     if (solver == MTLG_GMRES) return mtlg_gmres_impl(c, A, L, R, x, b, p, res);
     const int f32 = x->dtype == MTLG_F32;
     if (L && L->kind == MTLG_PC_IDENTITY) L = nullptr;   // is_identity(P) short-cut (cg.hpp:80-81)
-    SetKey key{A, L, solver, f32, 0};
+    SetKey key{A, L, solver, f32, 0, c->red_order};
     auto& slot = extra(c).sets[key];
     if (!slot) {
         std::unique_ptr<SolveSet> ss(new SolveSet);
@@ -1022,7 +1028,7 @@ int mtlg_refine_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* P, mtlg_vec
         set_error("the inner FP32 solve needs a preconditioner stored in FP32");
         return MTLG_ERR_INVALID_ARG;
     }
-    SetKey key{A, P, solver, 1, 1};
+    SetKey key{A, P, solver, 1, 1, c->red_order};
     auto& slot = extra(c).sets[key];
     if (!slot) {
         std::unique_ptr<SolveSet> ss(new SolveSet);

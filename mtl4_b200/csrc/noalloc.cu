@@ -18,7 +18,13 @@
 //    be serialized by the caller;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//    before any stream capture.  The address is kept per device together
+//    with the id of the CUDA context it belongs to; after cudaDeviceReset the
+//    next call sees a new context and looks the address up again (so that
+//    call, too, should come before any capture);
+//  * with n_rows > 0, row_ptr, col, val, p and q must all be non-null (a
+//    matrix without entries still passes a valid col and val pointer).
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -42,11 +48,40 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxCtas + 2];
 
 static std::mutex g_mu;
 static double* g_scratch_ptr[kMaxDevices] = {nullptr};
+static unsigned long long g_scratch_ctx[kMaxDevices] = {0};
 
-// One row per thread, entries summed in storage order with the product
-// rounded before each addition (as mtlg_spmv does for rows of up to 32
-// entries); the CTA's share of p.q goes to scratch[blockIdx.x]; the last CTA
-// to finish sums the partials in CTA order and writes *dot.
+// Driver entry points reached through the runtime (no link against libcuda):
+// the current context and its process-unique id.
+typedef CUresult (*PFN_ctx_current)(CUcontext*);
+typedef CUresult (*PFN_ctx_id)(CUcontext, unsigned long long*);
+
+unsigned long long current_ctx_id()
+{
+    static PFN_ctx_current get_current = nullptr;
+    static PFN_ctx_id get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+        cudaGetLastError();
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;   // unknown: the cached address is kept
+}
+
+// One row per thread, entries summed in storage order as mtlg_spmv does for
+// rows of up to 32 entries (products rounded before each addition, the row's
+// last (L mod 4) entries fused); the CTA's share of p.q goes to
+// scratch[blockIdx.x]; the last CTA to finish sums the partials in CTA order
+// and writes *dot.
 __global__ void __launch_bounds__(kNoAllocBlock)
 k_spmv_dot_noalloc(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                    const double* __restrict__ val, const double* __restrict__ p, double* __restrict__ q,
@@ -58,7 +93,9 @@ k_spmv_dot_noalloc(int n, const int32_t* __restrict__ rp, const int32_t* __restr
     double part = 0.0;
     if (i < n) {
         double acc = 0.0;
-        for (int k = rp[i]; k < rp[i + 1]; ++k) acc = __dadd_rn(acc, __dmul_rn(val[k], p[ci[k]]));
+        const int a = rp[i], e = rp[i + 1], tail = a + ((e - a) & ~3);
+        for (int k = a; k < e; ++k)
+            acc = k >= tail ? __fma_rn(val[k], p[ci[k]], acc) : __dadd_rn(acc, __dmul_rn(val[k], p[ci[k]]));
         q[i] = acc;
         part = p[i] * acc;
     }
@@ -87,14 +124,19 @@ int scratch_ptr(double** out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MTLG_ERR_CUDA;
+    // cudaFree(0) makes the device's primary context current, so that the
+    // id read next names the context the kernel will run in (allocates nothing)
+    cudaFree(nullptr);
+    const unsigned long long ctx = current_ctx_id();
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev] || (ctx != 0 && ctx != g_scratch_ctx[dev])) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
             cudaGetLastError();
             return MTLG_ERR_CUDA;
         }
         g_scratch_ptr[dev] = static_cast<double*>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch_ptr[dev];
     return MTLG_OK;
@@ -105,7 +147,7 @@ int scratch_ptr(double** out)
 extern "C" int mtlg_spmv_dot_noalloc(int64_t n_rows, int64_t n_cols, const int32_t* row_ptr, const int32_t* col,
                                      const double* val, const double* p, double* q, double* dot, void* stream)
 {
-    if (n_rows < 0 || n_cols < 0 || !dot || (n_rows > 0 && (!row_ptr || !p || !q))) {
+    if (n_rows < 0 || n_cols < 0 || !dot || (n_rows > 0 && (!row_ptr || !col || !val || !p || !q))) {
         mtlg::set_error("invalid argument: negative size or null pointer");
         return MTLG_ERR_INVALID_ARG;
     }

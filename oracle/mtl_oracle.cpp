@@ -29,14 +29,22 @@ struct Csr {
 
 // w (=|+=|-=) A*v: per row an accumulator started at zero, entries in
 // storage order, tmp += a * v[col] (mtl/operation/mat_vec_mult.hpp:614-683);
-// Assign::first_update then assigns, adds or subtracts.
+// Assign::first_update then assigns, adds or subtracts.  The reference build
+// (g++ -O3 -march=x86-64-v3 -ffp-contract=fast) evaluates the FP64 row loop
+// in groups of four entries that add the rounded product, and the row's last
+// (L mod 4) entries as fused multiply-adds; FP32 rows add rounded products
+// throughout.  Determined against the build's outputs, where this rule
+// reproduces every row bitwise (rows of 1 to 4096 entries).
 template <typename V, typename T>
 void spmv(const Csr& A, const V* val, const T* x, T* y, int assign)
 {
     for (int64_t i = 0; i < A.n; ++i) {
         T tmp = T(0);
-        // product rounded, then added: the reference build does not fuse here
-        for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) tmp = tmp + T(val[k]) * x[A.ci[k]];
+        const int64_t a = A.rp[i], e = A.rp[i + 1], tail = a + (e - a) / 4 * 4;
+        for (int64_t k = a; k < tail; ++k) tmp = tmp + T(val[k]) * x[A.ci[k]];
+        for (int64_t k = tail; k < e; ++k)
+            tmp = std::is_same<T, double>::value ? T(std::fma(double(val[k]), double(x[A.ci[k]]), double(tmp)))
+                                                 : T(tmp + T(val[k]) * x[A.ci[k]]);
         if (assign == 0) y[i] = tmp;
         else if (assign == 1) y[i] += tmp;
         else y[i] -= tmp;
@@ -60,6 +68,48 @@ double dot(int64_t n, const T* a, const T* b)
     for (int64_t i = 0; i < n; ++i) s += double(a[i]) * double(b[i]);
     return s;
 }
+
+// Reductions in the reference build's order (FP64).  Each keeps four partial
+// sums t[k] over the entries i = k (mod 4) of the first 4*floor(n/4), the
+// remaining entries go to t[0].  Determined against the build's outputs (the
+// unrolled loops are vectorized with rounded products; scalar tails are
+// contracted or not as listed):
+//   dot4   mtl::dot (operation/dot.hpp:99-145, Unroll 4): rounded products
+//          throughout; (t0 + t1) + (t2 + t3).
+//   norm4  mtl::two_norm squared (operation/two_norm.hpp:35-56,
+//          vector/reduction.hpp:85-175): rounded products, fused tail;
+//          t0 + (t1 + (t2 + t3)) (reduction<>::finish).
+//   ldot4  lazy_dot in a fused expression (vector/dot_index_evaluator.hpp:
+//          20-45, operation/fused_expr.hpp:60-75): rounded products;
+//          ((t0 + t1) + t2) + t3.
+//   udot4  lazy_unary_dot in a fused expression
+//          (vector/reduction_index_evaluator.hpp:31-34): fused products
+//          throughout; (t0 + t1) + (t2 + t3).
+inline double rprod(double a, double b) { return a * b; }   // -ffp-contract=off: rounded
+template <int Kind>
+double red4(int64_t n, const double* a, const double* b)
+{
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t nb = n / 4 * 4;
+    const bool fused_main = Kind == 3, fused_tail = Kind == 1 || Kind == 3;
+    for (int64_t i = 0; i < nb; i += 4)
+        for (int k = 0; k < 4; ++k)
+            t[k] = fused_main ? std::fma(a[i + k], b[i + k], t[k]) : t[k] + rprod(a[i + k], b[i + k]);
+    for (int64_t i = nb; i < n; ++i) t[0] = fused_tail ? std::fma(a[i], b[i], t[0]) : t[0] + rprod(a[i], b[i]);
+    if (Kind == 1) return t[0] + (t[1] + (t[2] + t[3]));
+    if (Kind == 2) return ((t[0] + t[1]) + t[2]) + t[3];
+    return (t[0] + t[1]) + (t[2] + t[3]);
+}
+inline double dot4(int64_t n, const double* a, const double* b) { return red4<0>(n, a, b); }
+inline double norm4(int64_t n, const double* a) { return red4<1>(n, a, a); }
+inline double ldot4(int64_t n, const double* a, const double* b) { return red4<2>(n, a, b); }
+inline double udot4(int64_t n, const double* a) { return red4<3>(n, a, a); }
+// FP32 vectors: dots accumulate in double in storage order (the GPU's FP32
+// inner solves accumulate in double as well)
+inline double dot4(int64_t n, const float* a, const float* b) { return dot(n, a, b); }
+inline double norm4(int64_t n, const float* a) { return dot(n, a, a); }
+inline double ldot4(int64_t n, const float* a, const float* b) { return dot(n, a, b); }
+inline double udot4(int64_t n, const float* a) { return dot(n, a, a); }
 
 // itl::basic_iteration (itl/iteration/basic_iteration.hpp:32-93).
 struct Iter {
@@ -247,35 +297,51 @@ void make_pc(const Csr& A, const double* a, int kind, PC<S>& P)
 }
 
 // Conjugate gradients (itl/krylov/cg.hpp:76-111; identity: cg.hpp:40-71).
+// r = b - A x; rr = dot(r, r); per iteration z = solve(L, r) and
+// rho = dot(r, z) (the fused pair evaluates as two passes, the preconditioner
+// not being index-evaluatable), p = z + (rho / rho_1) p, the fused
+// q = A p || lazy_dot(p, q), x += alpha p, the fused r -= alpha q ||
+// lazy_unary_dot(r).  The identity preconditioner runs the reference's
+// unpreconditioned body, where rho is the fused unary dot itself.
 template <typename V, typename T, typename S>
 int cg(const Csr& A, const V* val, T* x, const T* b, const PC<S>& P, Iter& it)
 {
     const int64_t n = A.n;
+    const bool ident = P.kind == 0;
     std::vector<T> p(n, T(0)), q(n), r(n), z(n);
     for (int64_t i = 0; i < n; ++i) r[i] = b[i];
     spmv(A, val, x, r.data(), 2);
-    double rho = 0, rho_1 = 0, rr = dot(n, r.data(), r.data());
-    while (!it.finished(std::sqrt(std::fabs(rr)))) {
+    double rho = 0, rho_1 = 0, rr = dot4(n, r.data(), r.data());
+    if (ident) rho = rr;
+    while (!it.finished(std::sqrt(std::fabs(ident ? rho : rr)))) {
         ++it.i;
-        P.apply(r.data(), z.data());
-        rho = dot(n, r.data(), z.data());
-        if (it.first()) p = z;
+        const T* zz = r.data();
+        if (!ident) {
+            P.apply(r.data(), z.data());
+            rho = dot4(n, r.data(), z.data());
+            zz = z.data();
+        }
+        if (it.first()) for (int64_t i = 0; i < n; ++i) p[i] = zz[i];
         else {
             const T beta = T(rho / rho_1);
-            for (int64_t i = 0; i < n; ++i) p[i] = std::fma(beta, p[i], z[i]);
+            for (int64_t i = 0; i < n; ++i) p[i] = std::fma(beta, p[i], zz[i]);
         }
         spmv(A, val, p.data(), q.data(), 0);
-        const T alpha = T(rho / dot(n, p.data(), q.data()));
+        const T alpha = T(rho / ldot4(n, p.data(), q.data()));
         for (int64_t i = 0; i < n; ++i) x[i] = std::fma(alpha, p[i], x[i]);
         rho_1 = rho;
         for (int64_t i = 0; i < n; ++i) r[i] = std::fma(-alpha, q[i], r[i]);
-        rr = dot(n, r.data(), r.data());
+        if (ident) rho = udot4(n, r.data());
+        else rr = udot4(n, r.data());
     }
     return it.error;
 }
 
 // BiCGSTAB (itl/krylov/bicgstab.hpp:29-77).  Returns -2 on the breakdowns
-// for which the reference throws unexpected_orthogonality.
+// for which the reference throws unexpected_orthogonality.  Norms are
+// two_norm (iter.finished(r), finished(s)), the scalars mtl::dot; the update
+// x += omega shat + alpha phat is evaluated x + fma(alpha, phat, omega shat)
+// as the reference build does.
 template <typename V, typename T, typename S>
 int bicgstab(const Csr& A, const V* val, T* x, const T* b, const PC<S>& P, Iter& it)
 {
@@ -285,9 +351,9 @@ int bicgstab(const Csr& A, const V* val, T* x, const T* b, const PC<S>& P, Iter&
     spmv(A, val, x, r.data(), 2);
     rt = r;
     double rho_1 = 0, rho_2 = 0, alpha = 0, beta = 0, omega = 0;
-    while (!it.finished(std::sqrt(dot(n, r.data(), r.data())))) {
+    while (!it.finished(std::sqrt(norm4(n, r.data())))) {
         ++it.i;
-        rho_1 = dot(n, rt.data(), r.data());
+        rho_1 = dot4(n, rt.data(), r.data());
         if (rho_1 == 0.0) return -2;
         if (it.first()) p = r;
         else {
@@ -297,19 +363,19 @@ int bicgstab(const Csr& A, const V* val, T* x, const T* b, const PC<S>& P, Iter&
         }
         P.apply(p.data(), phat.data());
         spmv(A, val, phat.data(), v.data(), 0);
-        const double gamma = dot(n, rt.data(), v.data());
+        const double gamma = dot4(n, rt.data(), v.data());
         if (gamma == 0.0) return -2;
         alpha = rho_1 / gamma;
         for (int64_t i = 0; i < n; ++i) s[i] = std::fma(-T(alpha), v[i], r[i]);
-        if (it.finished(std::sqrt(dot(n, s.data(), s.data())))) {
+        if (it.finished(std::sqrt(norm4(n, s.data())))) {
             for (int64_t i = 0; i < n; ++i) x[i] = std::fma(T(alpha), phat[i], x[i]);
             break;
         }
         P.apply(s.data(), shat.data());
         spmv(A, val, shat.data(), t.data(), 0);
-        omega = dot(n, t.data(), s.data()) / dot(n, t.data(), t.data());
+        omega = dot4(n, t.data(), s.data()) / dot4(n, t.data(), t.data());
         for (int64_t i = 0; i < n; ++i) {
-            x[i] = x[i] + std::fma(T(omega), shat[i], T(alpha) * phat[i]);
+            x[i] = x[i] + std::fma(T(alpha), phat[i], T(omega) * shat[i]);
             r[i] = std::fma(-T(omega), t[i], s[i]);
         }
         rho_2 = rho_1;
@@ -426,6 +492,9 @@ void mtlo_spmv_f32(int64_t n, const int64_t* rp, const int32_t* ci, const float*
 }
 
 double mtlo_dot(int64_t n, const double* a, const double* b) { return dot(n, a, b); }
+// mtl::dot and two_norm squared in the reference build's summation order
+double mtlo_dot4(int64_t n, const double* a, const double* b) { return dot4(n, a, b); }
+double mtlo_norm4(int64_t n, const double* a) { return norm4(n, a); }
 
 /// y = solve(P, x); storage_f32 selects the stored factor precision.
 void mtlo_pc_apply(int64_t n, const int64_t* rp, const int32_t* ci, const double* a, int kind, int storage_f32,
@@ -475,7 +544,7 @@ int mtlo_solve(int64_t n, const int64_t* rp, const int32_t* ci, const double* a,
     make_pc(A, a, kind, P);
     Iter it;
     it.max_iter = max_iter; it.rtol = rtol; it.atol = atol;
-    it.norm_r0 = norm_r0 >= 0 ? norm_r0 : std::sqrt(dot(n, b, b));
+    it.norm_r0 = norm_r0 >= 0 ? norm_r0 : std::sqrt(norm4(n, b));   // two_norm(b)
     int err = run(solver, A, a, x, b, P, it, restart);
     if (out) { *out = mtlo_result{it.i, err, it.resid, it.norm_r0 ? it.resid / it.norm_r0 : it.resid, 0, 0}; }
     return err;

@@ -88,6 +88,10 @@ def port_lib() -> C.CDLL:
         L.mtlo_spmv_f32.argtypes = [C.c_int64, VP, VP, VP, VP, VP, C.c_int]
         L.mtlo_dot.restype = C.c_double
         L.mtlo_dot.argtypes = [C.c_int64, VP, VP]
+        L.mtlo_dot4.restype = C.c_double
+        L.mtlo_dot4.argtypes = [C.c_int64, VP, VP]
+        L.mtlo_norm4.restype = C.c_double
+        L.mtlo_norm4.argtypes = [C.c_int64, VP]
         L.mtlo_pc_apply.argtypes = [C.c_int64, VP, VP, VP, C.c_int, C.c_int, VP, VP]
         L.mtlo_pc_apply_f32.argtypes = [C.c_int64, VP, VP, VP, C.c_int, VP, VP]
         L.mtlo_pc_factor.argtypes = [C.c_int64, VP, VP, VP, C.c_int, C.c_int, C.POINTER(C.c_int64), VP, VP, VP]

@@ -8,6 +8,7 @@ where the MTL4 tree is not available.
 """
 from __future__ import annotations
 
+import hashlib
 import sys
 from pathlib import Path
 
@@ -34,7 +35,7 @@ def main():
     out["lap32_spmv_f32"] = R.spmv(xs.astype(np.float32))
     out["lap32_b"] = b
     for solver, pc in [("cg", "diagonal"), ("cg", "identity"), ("cg", "ic_0"), ("bicgstab", "ilu_0"),
-                       ("bicgstab", "diagonal")]:
+                       ("bicgstab", "diagonal"), ("bicgstab", "identity"), ("bicgstab", "ic_0")]:
         r = R.solve(b, solver, pc, max_iter=2000, rtol=1e-8)
         out[f"lap32_{solver}_{pc}_iters"] = np.array(r["iterations"])
         out[f"lap32_{solver}_{pc}_x"] = r["x"]
@@ -65,6 +66,19 @@ def main():
     out["pl_x"] = xq
     out["pl_spmv"] = RQ.spmv(xq)
     out["pl_spmv_f32"] = RQ.spmv(xq.astype(np.float32))
+    # mtl::dot and mtl::two_norm (four strided partial sums) on general values
+    out["dot_x"] = xq[:1001]
+    out["dot_y"] = np.random.default_rng(14).standard_normal(1001)
+    out["dot_xy"] = np.array(O.ref_lib().mtlref_dot(1001, O._p(out["dot_x"]), O._p(out["dot_y"])))
+    out["norm_x"] = np.array(O.ref_lib().mtlref_two_norm(1001, O._p(out["dot_x"])))
+    # full-size solves: iteration counts, relative residuals and the SHA-256 of
+    # the solution's bytes (the reference's x itself is too large to keep)
+    for tag, (A_, b_), solver, pc in [("c1", P.config1()[:2], "cg", "diagonal"),
+                                      ("c2", P.config2_solve(128)[:2], "bicgstab", "ilu_0")]:
+        r = O.RefMatrix(A_).solve(b_, solver, pc, max_iter=2000, rtol=1e-8)
+        out[f"{tag}_iters"] = np.array(r["iterations"])
+        out[f"{tag}_relres"] = np.array(r["relresid"])
+        out[f"{tag}_x_sha256"] = np.array(hashlib.sha256(np.ascontiguousarray(r["x"]).tobytes()).hexdigest())
     np.savez_compressed(Path(__file__).with_name("golden.npz"), **out)
     print("wrote", len(out), "arrays")
 

@@ -40,3 +40,17 @@ def test_missing_library_fails_loudly(tmp_path):
     from mtl4_b200 import _lib
     with pytest.raises(ImportError):
         _lib.load(tmp_path / "nope.so")
+
+
+def test_noalloc_rejects_null_matrix_arrays_without_touching_the_gpu():
+    # argument checks run before any CUDA call, so this needs no GPU
+    import ctypes as C
+    from mtl4_b200 import _lib
+    L = _lib.load()
+    buf = (C.c_double * 8)()
+    ok = C.cast(buf, C.c_void_p)
+    for missing in range(5):
+        args = [ok] * 5
+        args[missing] = None   # row_ptr, col, val, p, q in turn
+        st = L.mtlg_spmv_dot_noalloc(4, 4, *args, ok, None)
+        assert st == _lib.ERR_INVALID_ARG, missing

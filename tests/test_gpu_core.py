@@ -1,8 +1,9 @@
 """GPU parity: the CUDA library (through its C ABI) against the oracle on the
-same seeded inputs.  SpMV: bitwise on stencils, <= 1e-14 relative per entry
-(FP64) otherwise; factors and preconditioner applies: bitwise; solves: the
-true FP64 residual meets the tolerance and the iteration count is within the
-stated bound of the reference's."""
+same seeded inputs.  SpMV: bitwise on every row of up to 32 entries (the
+oracle's row sum is bitwise the reference build's), <= 1e-14 relative per
+entry (FP64) on longer rows, which a warp sums as a tree; factors and
+preconditioner applies: bitwise; solves: the true FP64 residual meets the
+tolerance and the iteration count is at most the reference's + 2."""
 import numpy as np
 import pytest
 
@@ -74,6 +75,25 @@ def test_spmv_irregular(ctx, n):
     yf = mtl.dense_vector(n, np.float32, ctx)
     mtl.mult(Qd, vec(xf, ctx, np.float32), yf)
     assert spmv_rel_err(Q, xf, yf.numpy(), O.port_spmv(Q, xf)).max() <= 1e-6
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_spmv_general_values_bitwise(ctx, dtype):
+    # convection-diffusion values: products are not exact, so this pins the
+    # reference's contraction rule (rounded groups of four, fused FP64 tail)
+    # in the standalone SpMV and in the fused SpMV + dot of the solvers
+    from mtl4_b200 import mtl
+    A = P.convdiff_3d(20)
+    Ad = dev(A, ctx)
+    x = np.random.default_rng(6).uniform(-1, 1, A.n_rows).astype(dtype)
+    y = mtl.dense_vector(A.n_rows, dtype, ctx)
+    mtl.mult(Ad, vec(x, ctx, dtype), y)
+    ref = O.port_spmv(A, x)
+    assert np.array_equal(y.numpy(), ref)
+    if dtype == np.float64:
+        q = mtl.dense_vector(A.n_rows, dtype, ctx)
+        mtl.mult_dot(Ad, vec(x, ctx, dtype), q)
+        assert np.array_equal(q.numpy(), ref)
 
 
 def test_spmv_long_rows_and_empty_rows(ctx):

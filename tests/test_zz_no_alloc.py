@@ -23,12 +23,16 @@ def _dev(torch, a, dtype):
     return torch.from_numpy(np.ascontiguousarray(a).astype(dtype)).cuda()
 
 
-def _noalloc(L, torch, A, rp, ci, val, p, q, dot):
+def _noalloc(L, torch, A, rp, ci, val, p, q, dot, stream=None):
+    """One call; returns (status, device bytes that the call took)."""
+    stream = stream or torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
     st = L.mtlg_spmv_dot_noalloc(A.n_rows, A.n_cols, C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
                                  C.c_void_p(val.data_ptr()), C.c_void_p(p.data_ptr()), C.c_void_p(q.data_ptr()),
-                                 C.c_void_p(dot.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+                                 C.c_void_p(dot.data_ptr()), C.c_void_p(stream.cuda_stream))
     torch.cuda.synchronize()
-    return st
+    return st, free_before - torch.cuda.mem_get_info()[0]
 
 
 @pytest.mark.parametrize("kind", ["stencil", "irregular"])
@@ -43,12 +47,22 @@ def test_noalloc_matches_regular_entry_point_twice(kind):
     ci = _dev(torch, A.col, np.int32)
     val = _dev(torch, A.val, np.float64)
     rng = np.random.default_rng(17)
+    # set-up call: the first call on a device looks up the scratch array's
+    # address (and loads the module that holds it, which is where the array
+    # itself lives); the calls checked below must take no device memory
+    q0 = torch.zeros(A.n_rows, dtype=torch.float64, device="cuda")
+    d0 = torch.zeros(1, dtype=torch.float64, device="cuda")
+    assert _noalloc(L, torch, A, rp, ci, val, q0, q0.clone(), d0)[0] == _lib.OK
+    side = torch.cuda.Stream()
     for call in range(2):
         x = rng.standard_normal(A.n_rows)
         p = _dev(torch, x, np.float64)
         q = torch.full((A.n_rows,), 7.0, dtype=torch.float64, device="cuda")
         dot = torch.zeros(1, dtype=torch.float64, device="cuda")
-        assert _noalloc(L, torch, A, rp, ci, val, p, q, dot) == _lib.OK, call
+        # the second call runs on another stream (after the first finished)
+        st, taken = _noalloc(L, torch, A, rp, ci, val, p, q, dot, stream=side if call else None)
+        assert st == _lib.OK, call
+        assert taken == 0, (call, taken)
         # the regular entry point on the same inputs
         qd = mtl.dense_vector(A.n_rows, np.float64, ctx)
         d_ref = mtl.mult_dot(Ad, mtl.dense_vector(x, np.float64, ctx), qd)
