@@ -262,6 +262,18 @@ int mtlg_batch_solve(mtlg_batch* B, int precision, const mtlg_refine_params* ref
 int mtlg_batch_result(const mtlg_batch* B, int index, double* x_host, mtlg_iter_result* result);
 int mtlg_batch_size(const mtlg_batch* B);
 
+/* ---- several GPUs (one process per GPU) ------------------------------------- */
+/* Independent systems shard by whole systems, with no collective on the data
+ * path: every rank computes the same assignment, solves its share on its own
+ * GPU, and the results are gathered on the host.  Size-balanced greedy
+ * (longest processing time first): by decreasing cost (e.g. nnz + n), each
+ * system goes to the part with the least cost so far.  part_of[n_systems]
+ * receives the part of each system, part_cost[n_parts] (may be NULL) each
+ * part's total.  Host only, needs no GPU.  No reference counterpart (MTL4
+ * has no multi-process code). */
+int mtlg_partition_systems(int64_t n_systems, const int64_t* cost, int n_parts, int32_t* part_of,
+                           int64_t* part_cost);
+
 /* ---- served solves (continuous batching) ----------------------------------- */
 typedef struct {
     size_t hbm_budget;        /* bytes the server may hold on the device */

@@ -118,6 +118,7 @@ SIGNATURES = {
     "mtlg_batch_solve": (C.c_int, [VP, C.c_int, C.POINTER(RefineParams)]),
     "mtlg_batch_result": (C.c_int, [VP, C.c_int, VP, C.POINTER(IterResult)]),
     "mtlg_batch_size": (C.c_int, [VP]),
+    "mtlg_partition_systems": (C.c_int, [C.c_int64, VP, C.c_int, VP, VP]),
     "mtlg_server_create": (C.c_int, [VP, C.POINTER(ServerOpts), C.POINTER(VP)]),
     "mtlg_server_destroy": (C.c_int, [VP]),
     "mtlg_server_submit": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, C.c_int, C.c_int, C.c_int, PI64]),

@@ -69,6 +69,31 @@ int mtlg_batch_add(mtlg_batch* B, int64_t n, int64_t nnz, const int64_t* row_ptr
 
 int mtlg_batch_size(const mtlg_batch* B) { return B ? int(B->sys.size()) : 0; }
 
+// Size-balanced greedy assignment of independent systems to devices (longest
+// processing time first): systems in order of decreasing cost (ties by
+// index) each go to the part with the least cost so far (ties: lowest part).
+// Host only; deterministic, so every rank computes the same assignment.
+int mtlg_partition_systems(int64_t n_systems, const int64_t* cost, int n_parts, int32_t* part_of, int64_t* part_cost)
+{
+    MTLG_CHECK_ARG(n_systems >= 0 && n_parts >= 1, "sizes");
+    MTLG_CHECK_ARG(n_systems == 0 || (cost && part_of), "null array");
+    for (int64_t i = 0; i < n_systems; ++i) MTLG_CHECK_ARG(cost[i] >= 0, "negative cost");
+    std::vector<int64_t> order(static_cast<size_t>(n_systems), 0);
+    for (int64_t i = 0; i < n_systems; ++i) order[size_t(i)] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+    std::vector<int64_t> load(static_cast<size_t>(n_parts), 0);
+    for (int64_t i : order) {
+        int best = 0;
+        for (int p = 1; p < n_parts; ++p)
+            if (load[size_t(p)] < load[size_t(best)]) best = p;
+        part_of[i] = best;
+        load[size_t(best)] += cost[i];
+    }
+    if (part_cost)
+        for (int p = 0; p < n_parts; ++p) part_cost[p] = load[size_t(p)];
+    return MTLG_OK;
+}
+
 int mtlg_batch_solve(mtlg_batch* B, int precision, const mtlg_refine_params* refine)
 {
     MTLG_CHECK_ARG(B, "batch");

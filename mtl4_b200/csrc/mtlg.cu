@@ -575,6 +575,7 @@ int mtlg_vec_fill(mtlg_vec* v, double value)
     MTLG_TRY(vec_set(c, v->n, sv));
     SysDesc d;
     memset(&d, 0, sizeof d);
+    d.n = int(v->n);
     d.x = v->p;
     MTLG_CUDA(cudaMemcpyAsync(sv.desc, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
     VecOp op = vec_op_default(VOP_FILL);
@@ -678,6 +679,7 @@ static int vec_binary(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, int kin
     MTLG_TRY(vec_set(c, x->n, sv));
     SysDesc d;
     memset(&d, 0, sizeof d);
+    d.n = int(x->n);
     d.x = x->p;
     d.b = y->p;
     MTLG_CUDA(cudaMemcpyAsync(sv.desc, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
