@@ -162,6 +162,19 @@ size_t mtlg_ctx_bytes_in_use(mtlg_ctx* ctx);
 const char* mtlg_status_string(int status);
 const char* mtlg_last_error_message(void);
 
+/* ---- tracing (the reference's vampir_trace<N> hooks,
+ * boost/numeric/mtl/interface/vpt.hpp:37-78, ids from interface/vpt.cpp) ---
+ * Every traced entry point pushes an NVTX range "<id> <name>" (e.g.
+ * "7004 bicgstab", "5038 ilu_0::factorize", "3049 crs_cvec_mult"; 9xxx for
+ * steps without a reference id: set-up phases, refinement, batch, server).
+ * While enabled (this call, or MTLG_TRACE=1 in the environment) each scope
+ * also adds its host wall time to a per-event tally; the report is one line
+ * per event, "id name calls total_ms".  needed (may be NULL) receives the
+ * report's length + 1. */
+int mtlg_trace_enable(int on);
+int mtlg_trace_reset(void);
+int mtlg_trace_report(char* buf, size_t cap, size_t* needed);
+
 /* ---- CSR matrix (compressed2D) --------------------------------------------- */
 /* Host arrays are copied.  Columns must be sorted and in range in every row
  * (the reference's trisolves require sorted rows, lower_trisolve.hpp:105). */

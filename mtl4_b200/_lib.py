@@ -119,6 +119,9 @@ SIGNATURES = {
     "mtlg_batch_result": (C.c_int, [VP, C.c_int, VP, C.POINTER(IterResult)]),
     "mtlg_batch_size": (C.c_int, [VP]),
     "mtlg_partition_systems": (C.c_int, [C.c_int64, VP, C.c_int, VP, VP]),
+    "mtlg_trace_enable": (C.c_int, [C.c_int]),
+    "mtlg_trace_reset": (C.c_int, []),
+    "mtlg_trace_report": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "mtlg_server_create": (C.c_int, [VP, C.POINTER(ServerOpts), C.POINTER(VP)]),
     "mtlg_server_destroy": (C.c_int, [VP]),
     "mtlg_server_submit": (C.c_int, [VP, I64, I64, VP, VP, VP, VP, C.c_int, C.c_int, C.c_int, PI64]),

@@ -50,6 +50,7 @@ int mtlg_batch_add(mtlg_batch* B, int64_t n, int64_t nnz, const int64_t* row_ptr
                    const double* val, const double* b, int solver, int pc_kind, const mtlg_iter_params* params,
                    int* index)
 {
+    MTLG_TRACE(9121, "batch.add");
     MTLG_CHECK_ARG(B && b && params, "batch/b/params");
     MTLG_CHECK_ARG(solver == MTLG_CG || solver == MTLG_BICGSTAB, "batched solver must be CG or BiCGSTAB");
     MTLG_CHECK_ARG(pc_kind >= MTLG_PC_IDENTITY && pc_kind <= MTLG_PC_IC0, "pc kind");
@@ -96,6 +97,7 @@ int mtlg_partition_systems(int64_t n_systems, const int64_t* cost, int n_parts, 
 
 int mtlg_batch_solve(mtlg_batch* B, int precision, const mtlg_refine_params* refine)
 {
+    MTLG_TRACE(9120, "batch.solve");
     MTLG_CHECK_ARG(B, "batch");
     MTLG_CHECK_ARG(precision == MTLG_F64 || precision == MTLG_F32, "precision");
     mtlg_ctx* c = B->ctx;

@@ -2,6 +2,7 @@
 #pragma once
 #include "sweep.cuh"
 #include "refdot.cuh"
+#include "trace.cuh"
 
 #include <algorithm>
 #include <memory>

@@ -826,6 +826,8 @@ inline int pc_build(mtlg_pc* P)
     RowLists Lr, Ur;
     Lr.rp.assign(n + 1, 0);
     Ur.rp.assign(n + 1, 0);
+    {
+    MTLG_TRACE(9101, "pc.structure");
     if (P->kind == MTLG_PC_ILU0) {
         // L = strict_lower(LU) (unit diagonal), U = upper(LU) with the
         // inverted diagonal first (ilu_0.hpp:79-81, ilu.hpp:84-91)
@@ -864,10 +866,18 @@ inline int pc_build(mtlg_pc* P)
         MTLG_TRY(P->lt_row.upload(c, Lr.col.data(), std::max<size_t>(1, Lr.col.size())));
         MTLG_TRY(P->lt_src.upload(c, Lr.src.data(), std::max<size_t>(1, Lr.src.size())));
     }
+    }
     const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
-    MTLG_TRY(build_tri(c, Lr, n, true, P->L, B, int(P->ssize())));
-    MTLG_TRY(build_tri(c, Ur, n, false, P->U, B, int(P->ssize())));
+    {
+        MTLG_TRACE(9102, "pc.schedule_L");
+        MTLG_TRY(build_tri(c, Lr, n, true, P->L, B, int(P->ssize())));
+    }
+    {
+        MTLG_TRACE(9103, "pc.schedule_U");
+        MTLG_TRY(build_tri(c, Ur, n, false, P->U, B, int(P->ssize())));
+    }
     MTLG_TRY(pc_setup_single_set(P));
+    MTLG_TRACE(9104, "pc.factor_and_fill");
 
     // ---- numeric factorization on the device (FP64)
     MTLG_TRY(P->inv_dia.alloc(c, std::max(n, 1)));

@@ -318,6 +318,7 @@ int mtlg_server_destroy(mtlg_server* S)
 int mtlg_server_submit(mtlg_server* S, int64_t n, int64_t nnz, const int64_t* row_ptr, const int32_t* col,
                        const double* val, const double* b, int solver, int pc_kind, int max_iter, int64_t* id)
 {
+    MTLG_TRACE(9132, "server.submit");
     MTLG_CHECK_ARG(S && row_ptr && b && id && n > 0 && nnz >= 0, "server/arrays/id");
     MTLG_CHECK_ARG(solver == MTLG_CG || solver == MTLG_BICGSTAB, "served solver must be CG or BiCGSTAB");
     MTLG_CHECK_ARG(pc_kind == MTLG_PC_DIAGONAL || pc_kind == MTLG_PC_ILU0 || pc_kind == MTLG_PC_IC0,
@@ -353,6 +354,7 @@ int mtlg_server_submit(mtlg_server* S, int64_t n, int64_t nnz, const int64_t* ro
 
 int mtlg_server_step(mtlg_server* S)
 {
+    MTLG_TRACE(9130, "server.step");
     MTLG_CHECK_ARG(S, "server");
     mtlg_ctx* c = S->ctx;
     S->stats.steps++;

@@ -277,6 +277,44 @@ const char* mtlg_status_string(int s)
 
 const char* mtlg_last_error_message(void) { return last_error(); }
 
+int mtlg_trace_enable(int on)
+{
+    TraceState& t = trace_state();
+    std::lock_guard<std::mutex> lk(t.mu);
+    t.on = on ? 1 : 0;
+    return MTLG_OK;
+}
+
+int mtlg_trace_reset(void)
+{
+    TraceState& t = trace_state();
+    std::lock_guard<std::mutex> lk(t.mu);
+    t.events.clear();
+    return MTLG_OK;
+}
+
+int mtlg_trace_report(char* buf, size_t cap, size_t* needed)
+{
+    TraceState& t = trace_state();
+    std::string out;
+    {
+        std::lock_guard<std::mutex> lk(t.mu);
+        char line[160];
+        for (const auto& kv : t.events) {
+            snprintf(line, sizeof line, "%d %s %lld %.6f\n", kv.first, kv.second.name.c_str(), kv.second.calls,
+                     kv.second.seconds * 1e3);
+            out += line;
+        }
+    }
+    if (needed) *needed = out.size() + 1;
+    if (buf && cap) {
+        const size_t k = std::min(cap - 1, out.size());
+        memcpy(buf, out.data(), k);
+        buf[k] = 0;
+    }
+    return MTLG_OK;
+}
+
 // ------------------------------------------------------------------ context
 int mtlg_ctx_create(int device, size_t hbm_budget, mtlg_ctx** out)
 {
@@ -401,6 +439,7 @@ size_t mtlg_ctx_bytes_in_use(mtlg_ctx* c) { return c ? c->in_use : 0; }
 int mtlg_csr_create(mtlg_ctx* c, int64_t n_rows, int64_t n_cols, int64_t nnz, const int64_t* row_ptr,
                     const int32_t* col, const void* val, mtlg_dtype val_dtype, mtlg_csr** out)
 {
+    MTLG_TRACE(9001, "csr_create");
     MTLG_CHECK_ARG(c && out, "ctx/out");
     *out = nullptr;
     MTLG_CHECK_ARG(n_rows >= 0 && n_cols >= 0 && nnz >= 0, "negative size");
@@ -653,11 +692,13 @@ static int spmv_impl(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, i
 
 int mtlg_spmv(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, int assign)
 {
+    MTLG_TRACE(3049, "crs_cvec_mult");
     return spmv_impl(c, A, x, y, assign, nullptr);
 }
 
 int mtlg_spmv_dot(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* p, mtlg_vec* q, double* pq)
 {
+    MTLG_TRACE(9002, "crs_cvec_mult_dot");
     MTLG_CHECK_ARG(pq, "pq");
     return spmv_impl(c, A, p, q, MTLG_ASSIGN, pq);
 }
@@ -702,12 +743,14 @@ static int vec_binary(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, int kin
 
 int mtlg_dot(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, double* out)
 {
+    MTLG_TRACE(2003, "dot");
     MTLG_CHECK_ARG(out, "out");
     return vec_binary(c, x, y, VOP_DOT, 0.0, out);
 }
 
 int mtlg_two_norm(mtlg_ctx* c, const mtlg_vec* x, double* out)
 {
+    MTLG_TRACE(2039, "two_norm");
     MTLG_CHECK_ARG(out, "out");
     MTLG_TRY(vec_binary(c, x, x, VOP_DOT, 0.0, out, RK_NORM4));
     *out = sqrt(fabs(*out));
@@ -719,6 +762,9 @@ int mtlg_axpy(mtlg_ctx* c, double a, const mtlg_vec* x, mtlg_vec* y) { return ve
 // ------------------------------------------------------------------ preconditioners
 int mtlg_pc_create(mtlg_ctx* c, mtlg_csr* A, int kind, mtlg_dtype storage, mtlg_pc** out)
 {
+    MTLG_TRACE(kind == MTLG_PC_ILU0 ? 5038 : kind == MTLG_PC_IC0 ? 5035 : kind == MTLG_PC_DIAGONAL ? 5050 : 9100,
+               kind == MTLG_PC_ILU0 ? "ilu_0::factorize" : kind == MTLG_PC_IC0 ? "ic_0::factorize"
+               : kind == MTLG_PC_DIAGONAL ? "diagonal::setup" : "identity::setup");
     MTLG_CHECK_ARG(c && A && out, "null handle");
     MTLG_CHECK_ARG(kind >= MTLG_PC_IDENTITY && kind <= MTLG_PC_IC0, "pc kind");
     MTLG_CHECK_ARG(ok_dtype(storage), "storage dtype");
@@ -752,6 +798,9 @@ int mtlg_pc_destroy(mtlg_pc* P)
 int mtlg_pc_apply(mtlg_ctx* c, mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
 {
     MTLG_CHECK_ARG(c && P && x && y, "null handle");
+    MTLG_TRACE(P->kind == MTLG_PC_ILU0 ? 5039 : P->kind == MTLG_PC_IC0 ? 5036 : P->kind == MTLG_PC_DIAGONAL ? 5051 : 9109,
+               P->kind == MTLG_PC_ILU0 ? "ilu_0::solve" : P->kind == MTLG_PC_IC0 ? "ic_0::solve"
+               : P->kind == MTLG_PC_DIAGONAL ? "diagonal::solve" : "identity::solve");
     MTLG_CHECK_ARG(x->dtype == y->dtype, "x and y dtypes differ");
     if (x->n != P->n || y->n != P->n) {
         set_error("preconditioner of size %d applied to %lld -> %lld", P->n, (long long)x->n, (long long)y->n);
@@ -918,6 +967,9 @@ static int timed_result(mtlg_ctx* c, SolveSet& ss, cudaEvent_t e0, cudaEvent_t e
 int mtlg_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* L, mtlg_pc* R, mtlg_vec* x, const mtlg_vec* b,
                const mtlg_iter_params* p, mtlg_iter_result* res)
 {
+    MTLG_TRACE(solver == MTLG_CG ? ((L && L->kind != MTLG_PC_IDENTITY) ? 7002 : 7001) : solver == MTLG_BICGSTAB ? 7004 : 9111,
+               solver == MTLG_CG ? ((L && L->kind != MTLG_PC_IDENTITY) ? "cg" : "cg_without_pc")
+               : solver == MTLG_BICGSTAB ? "bicgstab" : "gmres");
     MTLG_CHECK_ARG(c && p, "ctx/params");
     MTLG_TRY(check_solve_args(solver, A, x, b, L));
     MTLG_CHECK_ARG(x->dtype == b->dtype, "x and b dtypes differ");
@@ -1021,6 +1073,7 @@ inline int fp64_budget(const mtlg_refine_params& rp, int used)
 int mtlg_refine_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* P, mtlg_vec* x, const mtlg_vec* b,
                       const mtlg_refine_params* rp, mtlg_iter_result* res)
 {
+    MTLG_TRACE(9110, "refine");
     MTLG_CHECK_ARG(c && rp, "ctx/params");
     MTLG_TRY(check_solve_args(solver, A, x, b, P));
     MTLG_CHECK_ARG(x->dtype == MTLG_F64 && b->dtype == MTLG_F64, "refinement takes FP64 x and b");

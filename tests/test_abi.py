@@ -54,3 +54,11 @@ def test_noalloc_rejects_null_matrix_arrays_without_touching_the_gpu():
         args[missing] = None   # row_ptr, col, val, p, q in turn
         st = L.mtlg_spmv_dot_noalloc(4, 4, *args, ok, None)
         assert st == _lib.ERR_INVALID_ARG, missing
+
+
+def test_trace_report_api_without_gpu():
+    from mtl4_b200 import trace
+    trace.reset()
+    trace.enable(True)
+    assert trace.report() == {}
+    trace.enable(False)

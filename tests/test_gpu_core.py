@@ -377,3 +377,20 @@ def test_gmres_max_iterations(ctx):
     it = itl.basic_iteration(bd, 25, 1e-8)
     itl.gmres(Ad, x, bd, None, None, it, 10)
     assert it.error_code() == 1 and it.iterations() == 25
+
+
+def test_trace_hooks_record_reference_event_ids(ctx):
+    # the reference's vampir_trace ids: 7004 bicgstab, 5038 ilu_0::factorize,
+    # 5039 ilu_0::solve (interface/vpt.cpp)
+    from mtl4_b200 import trace
+    trace.reset()
+    trace.enable(True)
+    try:
+        A, b, _ = P.config2_solve(12)
+        solve_gpu(ctx, A, b, "bicgstab", "ilu_0")
+    finally:
+        trace.enable(False)
+    rep = trace.report()
+    assert rep[7004][0] == "bicgstab" and rep[7004][1] == 1
+    assert rep[5038][0] == "ilu_0::factorize" and rep[5038][2] > 0
+    assert 9102 in rep and 9104 in rep   # set-up phases
