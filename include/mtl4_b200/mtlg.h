@@ -56,7 +56,9 @@ enum {
     MTLG_ERR_NOT_SUPPORTED = 12,
     MTLG_ERR_ADMISSION = 13,        /* serving: request does not fit the budget */
     MTLG_ERR_NOT_FOUND = 14,        /* serving: unknown request id              */
-    MTLG_PENDING = 15               /* serving: request not finished yet        */
+    MTLG_PENDING = 15,              /* serving: request not finished yet        */
+    MTLG_ERR_FILE_NOT_FOUND = 16,   /* mtl::io::file_not_found                  */
+    MTLG_ERR_FORMAT = 17            /* malformed input file (mtl::runtime_error) */
 };
 
 typedef enum { MTLG_F64 = 0, MTLG_F32 = 1 } mtlg_dtype;
@@ -182,6 +184,19 @@ int mtlg_csr_create(mtlg_ctx* ctx, int64_t n_rows, int64_t n_cols, int64_t nnz, 
                     const int32_t* col, const void* val, mtlg_dtype val_dtype, mtlg_csr** out);
 int mtlg_csr_destroy(mtlg_csr* A);
 int mtlg_csr_info(const mtlg_csr* A, int64_t* n_rows, int64_t* n_cols, int64_t* nnz);
+/* Matrix Market input (the reference's mtl::io::matrix_market_istream >>
+ * compressed2D, boost/numeric/mtl/io/matrix_market.hpp:44-214): coordinate
+ * or array files with real, integer or pattern values (pattern entries are
+ * stored as 0.0, as the reference does) and general, symmetric,
+ * skew-symmetric or Hermitian symmetry (off-diagonal entries mirrored as v,
+ * -v, v); a later entry at the same position replaces an earlier one; rows
+ * sorted by column.  Complex files are refused (MTLG_ERR_FORMAT), as the
+ * reference refuses them for a real matrix.  mtlg_mm_read puts the matrix
+ * on the device as FP64 CSR; mtlg_mm_read_host fills host arrays (call with
+ * null arrays to get the sizes). */
+int mtlg_mm_read(mtlg_ctx* ctx, const char* path, mtlg_csr** out);
+int mtlg_mm_read_host(const char* path, int64_t* n_rows, int64_t* n_cols, int64_t* nnz, int64_t* row_ptr,
+                      int32_t* col, double* val);
 /* Replace the values (same pattern), e.g. a new operator with the old graph. */
 int mtlg_csr_update_values(mtlg_csr* A, const void* val, mtlg_dtype val_dtype);
 /* SpMV tiling statistics: tiles by kind (0 stream, 1 long row, 2 unused). */

@@ -29,6 +29,8 @@ ERR_NOT_SUPPORTED = 12
 ERR_ADMISSION = 13
 ERR_NOT_FOUND = 14
 PENDING = 15
+ERR_FILE_NOT_FOUND = 16
+ERR_FORMAT = 17
 
 F64, F32 = 0, 1
 ASSIGN, PLUS, MINUS = 0, 1, 2
@@ -120,6 +122,9 @@ SIGNATURES = {
     "mtlg_batch_size": (C.c_int, [VP]),
     "mtlg_partition_systems": (C.c_int, [C.c_int64, VP, C.c_int, VP, VP]),
     "mtlg_trace_enable": (C.c_int, [C.c_int]),
+    "mtlg_mm_read": (C.c_int, [VP, C.c_char_p, C.POINTER(VP)]),
+    "mtlg_mm_read_host": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                    VP, VP, VP]),
     "mtlg_trace_reset": (C.c_int, []),
     "mtlg_trace_report": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "mtlg_server_create": (C.c_int, [VP, C.POINTER(ServerOpts), C.POINTER(VP)]),
@@ -189,6 +194,16 @@ class out_of_memory(MtlError):
     status = ERR_OOM
 
 
+class file_not_found(MtlError):
+    """mtl::io::file_not_found (io/matrix_market.hpp:53-58)."""
+    status = ERR_FILE_NOT_FOUND
+
+
+class runtime_error(MtlError):
+    """mtl::runtime_error, e.g. a malformed Matrix Market file."""
+    status = ERR_FORMAT
+
+
 _EXC = {
     ERR_NOT_SQUARE: matrix_not_square,
     ERR_MISSING_DIAGONAL: missing_diagonal,
@@ -198,6 +213,8 @@ _EXC = {
     ERR_OOM: out_of_memory,
     ERR_INVALID_ARG: logic_error,
     ERR_UNSORTED: logic_error,
+    ERR_FILE_NOT_FOUND: file_not_found,
+    ERR_FORMAT: runtime_error,
 }
 
 

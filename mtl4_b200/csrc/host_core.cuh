@@ -3,6 +3,7 @@
 #include "sweep.cuh"
 #include "refdot.cuh"
 #include "trace.cuh"
+#include "mmio.cuh"
 
 #include <algorithm>
 #include <memory>

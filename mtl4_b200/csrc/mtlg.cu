@@ -271,6 +271,8 @@ const char* mtlg_status_string(int s)
     case MTLG_ERR_ADMISSION: return "request exceeds the device budget";
     case MTLG_ERR_NOT_FOUND: return "unknown request";
     case MTLG_PENDING: return "pending";
+    case MTLG_ERR_FILE_NOT_FOUND: return "file not found";
+    case MTLG_ERR_FORMAT: return "malformed input";
     default: return "unknown status";
     }
 }
@@ -496,6 +498,32 @@ int mtlg_csr_create(mtlg_ctx* c, int64_t n_rows, int64_t n_cols, int64_t nnz, co
     MTLG_CUDA(cudaStreamSynchronize(c->stream));
     *out = A.release();
     return MTLG_OK;
+}
+
+int mtlg_mm_read_host(const char* path, int64_t* n_rows, int64_t* n_cols, int64_t* nnz, int64_t* row_ptr,
+                      int32_t* col, double* val)
+{
+    MTLG_TRACE(9003, "matrix_market_read");
+    MTLG_CHECK_ARG(path && n_rows && n_cols && nnz, "path/sizes");
+    MmCsr m;
+    MTLG_TRY(mm_read_file(path, m));
+    *n_rows = m.n_rows;
+    *n_cols = m.n_cols;
+    *nnz = int64_t(m.ci.size());
+    if (row_ptr) std::copy(m.rp.begin(), m.rp.end(), row_ptr);
+    if (col) std::copy(m.ci.begin(), m.ci.end(), col);
+    if (val) std::copy(m.val.begin(), m.val.end(), val);
+    return MTLG_OK;
+}
+
+int mtlg_mm_read(mtlg_ctx* c, const char* path, mtlg_csr** out)
+{
+    MTLG_TRACE(9003, "matrix_market_read");
+    MTLG_CHECK_ARG(c && path && out, "ctx/path/out");
+    MmCsr m;
+    MTLG_TRY(mm_read_file(path, m));
+    return mtlg_csr_create(c, m.n_rows, m.n_cols, int64_t(m.ci.size()), m.rp.data(), m.ci.data(), m.val.data(),
+                           MTLG_F64, out);
 }
 
 int mtlg_csr_destroy(mtlg_csr* A)

@@ -99,6 +99,20 @@ class compressed2D:
     def from_problem(cls, A, ctx: context | None = None) -> "compressed2D":
         return cls(A.row_ptr, A.col, A.val, (A.n_rows, A.n_cols), ctx)
 
+    @classmethod
+    def from_matrix_market(cls, path, ctx: context | None = None) -> "compressed2D":
+        """A = mtl::io::matrix_market(path) straight into device CSR (FP64)."""
+        self = cls.__new__(cls)
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(self.ctx._L.mtlg_mm_read(self.ctx.h, str(path).encode(), C.byref(h)), "matrix_market")
+        self.h = h
+        nr, nc, nz = C.c_int64(), C.c_int64(), C.c_int64()
+        check(self.ctx._L.mtlg_csr_info(h, C.byref(nr), C.byref(nc), C.byref(nz)), "csr_info")
+        self.shape = (nr.value, nc.value)
+        self.nnz = nz.value
+        return self
+
     def num_rows(self) -> int:
         return self.shape[0]
 
@@ -233,3 +247,19 @@ def two_norm(x: dense_vector) -> float:
 
 def axpy(a: float, x: dense_vector, y: dense_vector):
     check(x.ctx._L.mtlg_axpy(x.ctx.h, float(a), x.h, y.h), "axpy")
+
+
+def read_matrix_market(path):
+    """Host CSR of a Matrix Market file as the library's reader parses it
+    (mtl4_b200.problems.CSR; needs no GPU)."""
+    from .problems import CSR
+    L = _lib.lib()
+    nr, nc, nz = C.c_int64(), C.c_int64(), C.c_int64()
+    p = str(path).encode()
+    check(L.mtlg_mm_read_host(p, C.byref(nr), C.byref(nc), C.byref(nz), None, None, None), "matrix_market")
+    rp = np.zeros(nr.value + 1, np.int64)
+    ci = np.zeros(nz.value, np.int32)
+    v = np.zeros(nz.value, np.float64)
+    check(L.mtlg_mm_read_host(p, C.byref(nr), C.byref(nc), C.byref(nz), _ptr(rp), _ptr(ci), _ptr(v)),
+          "matrix_market")
+    return CSR(nr.value, nc.value, rp, ci, v)

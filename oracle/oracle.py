@@ -75,6 +75,8 @@ def ref_lib(omp: bool = False) -> C.CDLL:
         L.mtlref_refine_solve.argtypes = [VP, C.c_int, C.c_int, VP, VP, C.c_int, C.c_int, C.c_double, C.c_double,
                                           C.c_int, C.POINTER(RefResult)]
         L.mtlref_laplacian_setup.argtypes = [C.c_int, C.c_int, PI, VP, VP, VP]
+        L.mtlref_mm_read.restype = C.c_int
+        L.mtlref_mm_read.argtypes = [C.c_char_p, PI, PI, PI, VP, VP, VP]
         _REF[key] = L
     return _REF[key]
 
@@ -251,3 +253,20 @@ def solve(A, b, solver="cg", pc="identity", **kw):
     if ref_available():
         return RefMatrix(A).solve(b, solver, pc, **kw)
     return port_solve(A, b, solver, pc, **kw)
+
+
+def ref_matrix_market(path):
+    """(status, (n_rows, n_cols, row_ptr, col, val)) as the reference's
+    matrix_market_istream reads the file; status 1: file_not_found, 2: other
+    exception."""
+    L = ref_lib()
+    nr, nc, nz = C.c_int64(), C.c_int64(), C.c_int64()
+    p = str(path).encode()
+    st = L.mtlref_mm_read(p, C.byref(nr), C.byref(nc), C.byref(nz), None, None, None)
+    if st:
+        return st, None
+    rp = np.zeros(nr.value + 1, np.int64)
+    ci = np.zeros(nz.value, np.int32)
+    v = np.zeros(nz.value)
+    L.mtlref_mm_read(p, C.byref(nr), C.byref(nc), C.byref(nz), _p(rp), _p(ci), _p(v))
+    return 0, (nr.value, nc.value, rp, ci, v)

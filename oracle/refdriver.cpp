@@ -17,9 +17,11 @@
 // here around the reference's FP32 inner solvers so the GPU's refinement has
 // a reference-built checker.
 #include <boost/numeric/mtl/mtl.hpp>
+#include <boost/numeric/mtl/io/matrix_market.hpp>
 #include <boost/numeric/itl/itl.hpp>
 
 #include <chrono>
+#include <cstdio>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -170,6 +172,37 @@ double mtlref_two_norm(int64_t n, const double* a)
 {
     dvec va(std::size_t(n), const_cast<double*>(a));
     return mtl::two_norm(va);
+}
+
+// A = mtl::io::matrix_market(path) through matrix_market_istream >> A
+// (io/matrix_market.hpp:44-214) into compressed2D<double>; the CSR arrays
+// out (call with null arrays for the sizes).  Returns 0, 1 when the
+// reference throws file_not_found, 2 for any other exception.
+int mtlref_mm_read(const char* path, int64_t* n_rows, int64_t* n_cols, int64_t* nnz, int64_t* rp, int32_t* ci,
+                   double* val)
+{
+    try {
+        dmat A;
+        mtl::io::matrix_market_istream ms(path);
+        ms >> A;
+        *n_rows = int64_t(num_rows(A));
+        *n_cols = int64_t(num_cols(A));
+        *nnz = int64_t(A.nnz());
+        if (rp)
+            for (std::size_t i = 0; i <= num_rows(A); ++i) rp[i] = int64_t(A.address_major()[i]);
+        if (ci)
+            for (std::size_t k = 0; k < A.nnz(); ++k) ci[k] = int32_t(A.address_minor()[k]);
+        if (val)
+            for (std::size_t k = 0; k < A.nnz(); ++k) val[k] = A.address_data()[k];
+        return 0;
+    } catch (const mtl::file_not_found&) {
+        return 1;
+    } catch (const std::exception& e) {
+        fprintf(stderr, "mtlref_mm_read(%s): %s\n", path, e.what());
+        return 2;
+    } catch (...) {
+        return 2;
+    }
 }
 
 } // extern "C"

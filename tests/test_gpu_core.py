@@ -394,3 +394,32 @@ def test_trace_hooks_record_reference_event_ids(ctx):
     assert rep[7004][0] == "bicgstab" and rep[7004][1] == 1
     assert rep[5038][0] == "ilu_0::factorize" and rep[5038][2] > 0
     assert 9102 in rep and 9104 in rep   # set-up phases
+
+
+def test_matrix_market_to_device_csr(ctx, tmp_path):
+    # a symmetric-storage file (lower triangle) read straight into device CSR:
+    # the same operator as the generator's, SpMV bitwise the oracle's and CG
+    # + IC(0) on it as on the generated matrix
+    from mtl4_b200 import itl, mtl
+    A = P.vardiff_2d(40, sigma=0.5, seed=9)
+    f = tmp_path / "vd.mtx"
+    with open(f, "w") as fh:
+        lower = [(i, int(A.col[e]), float(A.val[e])) for i in range(A.n_rows)
+                 for e in range(A.row_ptr[i], A.row_ptr[i + 1]) if A.col[e] <= i]
+        fh.write("%%MatrixMarket matrix coordinate real symmetric\n% vardiff 40x40\n")
+        fh.write(f"{A.n_rows} {A.n_cols} {len(lower)}\n")
+        for i, j, v in lower:
+            fh.write(f"{i + 1} {j + 1} {v!r}\n")
+    Ad = mtl.compressed2D.from_matrix_market(f, ctx)
+    assert Ad.shape == (A.n_rows, A.n_cols) and Ad.nnz == A.nnz
+    x = np.random.default_rng(8).standard_normal(A.n_rows)
+    y = mtl.dense_vector(A.n_rows, np.float64, ctx)
+    mtl.mult(Ad, vec(x, ctx), y)
+    assert np.array_equal(y.numpy(), O.port_spmv(A, x))
+    _, b = P.rhs_from_solution(A, 2)
+    xs, it = solve_gpu(ctx, A, b, "cg", "ic_0")
+    xm = mtl.dense_vector(A.n_rows, np.float64, ctx)
+    Pm = itl.pc.ic_0(Ad)
+    itm = itl.basic_iteration(vec(b, ctx), 2000, 1e-8)
+    itl.cg(Ad, xm, vec(b, ctx), Pm, itm)
+    assert itm.iterations() == it.iterations() and np.array_equal(xm.numpy(), xs)
