@@ -155,7 +155,15 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * summation order -- four strided partial sums per reduction, combined as
  * mtl::dot, two_norm and the fused lazy dots do -- so that FP64 results and
  * iteration counts equal the reference's bitwise, at about a microsecond
- * per thousand entries per reduction).
+ * per thousand entries per reduction), "admission_free_bytes" (servers
+ * without a byte budget admit by the device's free memory; > 0 stands in for
+ * cudaMemGetInfo's figure, 0 queries it) and "admission_reserve_bytes"
+ * (memory kept out of admission; -1, default: max(1 GiB, 2% of the
+ * device)), "spin_limit" (polls before a device-side dependency wait of the
+ * triangular sweeps or factorizations gives up and the call returns
+ * MTLG_ERR_TIMEOUT; 0, default: 2^20, about half a second; applies to
+ * mtlg_pc_apply at once and to solves of preconditioners created
+ * afterwards).
  * Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
 int mtlg_ctx_set_tuning(mtlg_ctx* ctx, const char* key, int64_t value);
 int mtlg_ctx_get_tuning(mtlg_ctx* ctx, const char* key, int64_t* value);
@@ -304,7 +312,8 @@ int mtlg_partition_systems(int64_t n_systems, const int64_t* cost, int n_parts, 
 
 /* ---- served solves (continuous batching) ----------------------------------- */
 typedef struct {
-    size_t hbm_budget;        /* bytes the server may hold on the device */
+    size_t hbm_budget;        /* bytes the server may hold on the device; 0: admit by
+                                 the device's free memory (mtlg_server_admission) */
     int max_active;           /* systems advanced together */
     int iters_per_step;       /* inner iterations per engine step */
     int precision;            /* MTLG_F64 or MTLG_F32 (FP32 inner + FP64 refinement) */
@@ -334,6 +343,17 @@ int mtlg_server_step(mtlg_server* S);
 int mtlg_server_poll(mtlg_server* S, int64_t request_id, double* x_host, mtlg_iter_result* result);
 int mtlg_server_cancel(mtlg_server* S, int64_t request_id);
 int mtlg_server_stats_get(const mtlg_server* S, mtlg_server_stats* stats);
+/* The server's admission rule (host only, needs no GPU).  With a budget
+ * (> 0): admit while held + request <= budget; never when request > budget.
+ * Without: free_bytes (cudaMemGetInfo, or the context tuning key
+ * "admission_free_bytes") less reserve_bytes (tuning key
+ * "admission_reserve_bytes"; default max(1 GiB, 2% of the device)) must hold
+ * the request now; otherwise it waits while the server's held bytes would
+ * make room once active requests retire, and never fits beyond that.
+ * Returns 1 admit, 0 wait, -1 never fits (submit then fails with
+ * MTLG_ERR_ADMISSION).  No reference counterpart. */
+int mtlg_server_admission(size_t request_bytes, size_t held_bytes, size_t budget, size_t free_bytes,
+                          size_t reserve_bytes);
 
 #ifdef __cplusplus
 }

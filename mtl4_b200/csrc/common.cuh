@@ -61,7 +61,7 @@ constexpr int kMaxDots = 4;           // dots a fused pass can reduce at once
 constexpr int kNumVec = 16;           // workspace vectors per system
 constexpr double kRefMinGain = 0.5;  // refinement: an outer step must at least halve the FP64 residual
 constexpr int kScalarMeanRow = 12;   // SpMV auto choice: thread per row up to this mean row length
-constexpr long long kSpinLimit = 1LL << 20;  // polls before a device wait gives up (~0.5 s)
+constexpr long long kSpinLimit = 1LL << 20;  // polls before a device wait gives up (~0.5 s); default spin_limit
 
 // Tile kinds of the SpMV / vector tiling.
 enum TileKind : int { TILE_STREAM = 0, TILE_LONG = 1 };
@@ -206,6 +206,7 @@ struct SetView {
     int* err;                    // device error flags (timeouts)
     unsigned long long cond;     // cudaGraphConditionalHandle (0: not in a graph)
     int use_cond;
+    long long spin;              // polls before a dependency wait gives up (context "spin_limit"; 0: kSpinLimit)
 };
 
 // ----------------------------------------------------------------- device helpers

@@ -895,6 +895,7 @@ inline int pc_build(mtlg_pc* P)
     op.inv_dia = P->inv_dia.p;
     op.dpos = A->dpos.p;
     op.err = P->misc.p + 1;
+    op.spin = c->spin_limit;
     if (P->kind == MTLG_PC_ILU0) {
         MTLG_TRY(lu.alloc(c, size_t(std::max<int64_t>(1, A->nnz))));
         MTLG_CUDA(cudaMemcpyAsync(lu.p, A->v64.p, size_t(A->nnz) * 8, cudaMemcpyDeviceToDevice, c->stream));

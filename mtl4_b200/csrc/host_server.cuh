@@ -90,6 +90,36 @@ inline size_t srv_estimate(int64_t n, int64_t nnz, bool refine)
     return size_t(nnz) * (4 + 8 + 4 + 2 * (4 + 4 + 4 + 4 + vb)) + size_t(n) * (4 * 6 + 16 + kNumVec * vb + 8 + 64);
 }
 
+// Admission rule.  With a byte budget: a request fits when the server's
+// held bytes plus its estimate stay within the budget, and never fits when
+// the estimate alone exceeds it.  Without a budget: the device's free memory
+// (cudaMemGetInfo, or the context's "admission_free_bytes" stand-in) less a
+// reserve; a request that does not fit now waits while the memory the
+// server's active requests hold would make room once they retire, and never
+// fits otherwise.  Returns 1 admit, 0 wait, -1 never fits.
+inline int admission_decision(size_t need, size_t held, size_t budget, size_t free_bytes, size_t reserve)
+{
+    if (budget) {
+        if (need > budget) return -1;
+        return held + need <= budget ? 1 : 0;
+    }
+    const size_t usable = free_bytes > reserve ? free_bytes - reserve : 0;
+    if (need <= usable) return 1;
+    return need <= usable + held ? 0 : -1;
+}
+
+// Free device memory and the reserve kept out of admission (default: the
+// larger of 1 GiB and 2% of the device).
+inline int free_memory(mtlg_ctx* c, size_t& free_bytes, size_t& reserve)
+{
+    size_t fr = 0, total = 0;
+    MTLG_CUDA(cudaMemGetInfo(&fr, &total));
+    free_bytes = c->admission_free_bytes > 0 ? size_t(c->admission_free_bytes) : fr;
+    reserve = c->admission_reserve_bytes >= 0 ? size_t(c->admission_reserve_bytes)
+                                              : std::max<size_t>(size_t(1) << 30, total / 50);
+    return MTLG_OK;
+}
+
 inline int srv_engine_init(mtlg_server* S, int e)
 {
     mtlg_ctx* c = S->ctx;
@@ -307,6 +337,12 @@ int mtlg_server_create(mtlg_ctx* c, const mtlg_server_opts* opts, mtlg_server** 
     return MTLG_OK;
 }
 
+int mtlg_server_admission(size_t request_bytes, size_t held_bytes, size_t budget, size_t free_bytes,
+                          size_t reserve_bytes)
+{
+    return admission_decision(request_bytes, held_bytes, budget, free_bytes, reserve_bytes);
+}
+
 int mtlg_server_destroy(mtlg_server* S)
 {
     if (!S) return MTLG_OK;
@@ -325,9 +361,13 @@ int mtlg_server_submit(mtlg_server* S, int64_t n, int64_t nnz, const int64_t* ro
                    "served preconditioner must be diagonal, ILU(0) or IC(0)");
     S->stats.submitted++;
     const size_t est = srv_estimate(n, nnz, S->refine);
-    if (S->o.hbm_budget && est > S->o.hbm_budget) {
+    size_t fr = 0, reserve = 0;
+    if (!S->o.hbm_budget) MTLG_TRY(free_memory(S->ctx, fr, reserve));
+    if (admission_decision(est, S->bytes_held, S->o.hbm_budget, fr, reserve) < 0) {
         S->stats.rejected++;
-        set_error("request needs ~%zu bytes, the server budget is %zu", est, S->o.hbm_budget);
+        if (S->o.hbm_budget) set_error("request needs ~%zu bytes, the server budget is %zu", est, S->o.hbm_budget);
+        else set_error("request needs ~%zu bytes, the device has %zu free (%zu reserved) and the server holds %zu",
+                       est, fr, reserve, S->bytes_held);
         return MTLG_ERR_ADMISSION;
     }
     std::unique_ptr<mtlg_server::Req> R(new mtlg_server::Req);
@@ -418,8 +458,17 @@ int mtlg_server_step(mtlg_server* S)
         int slot = -1;
         for (int s = 0; s < E.ss.S; ++s) if (E.slot_req[s] < 0) { slot = s; break; }
         if (slot < 0) break;
-        if (S->o.hbm_budget && S->bytes_held + R.est > S->o.hbm_budget) break;
+        size_t fr = 0, reserve = 0;
+        if (!S->o.hbm_budget) MTLG_TRY(free_memory(c, fr, reserve));
+        const int adm = admission_decision(R.est, S->bytes_held, S->o.hbm_budget, fr, reserve);
+        if (adm == 0) break;   // waits for active requests to retire
         S->queue.pop_front();
+        if (adm < 0) {
+            R.state = 4;
+            R.status_code = MTLG_ERR_ADMISSION;
+            S->stats.rejected++;
+            continue;
+        }
         int st = srv_admit(S, R, e, slot);
         if (st != MTLG_OK) {
             R.release();

@@ -84,6 +84,7 @@ struct SolveSet {
         v.err = misc.p + 1;
         v.cond = in_graph ? cond : 0;
         v.use_cond = in_graph ? 1 : 0;
+        v.spin = ctx ? ctx->spin_limit : 0;
         return v;
     }
 };

@@ -117,6 +117,7 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
     sv.st = P->st.p;
     sv.running = P->misc.p;
     sv.err = P->misc.p + 1;
+    sv.spin = c->spin_limit;
     SysDesc d;
     memset(&d, 0, sizeof d);
     d.n = P->n;
@@ -395,6 +396,9 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
     else if (k == "pc_apply_sync") c->pc_apply_sync = value ? 1 : 0;
     else if (k == "reduction_order") c->red_order = value ? 1 : 0;
+    else if (k == "spin_limit") c->spin_limit = std::max<int64_t>(0, value);
+    else if (k == "admission_free_bytes") c->admission_free_bytes = std::max<int64_t>(0, value);
+    else if (k == "admission_reserve_bytes") c->admission_reserve_bytes = std::max<int64_t>(-1, value);
     else if (k == "chunk_rows") c->chunk_rows = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 15)));
     else if (k == "vec_ctas_per_sm") c->vec_ctas_per_sm = int(std::max<int64_t>(1, std::min<int64_t>(value, 16)));
     else if (k == "sweep_cluster") {
@@ -425,6 +429,9 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     else if (k == "sweep_kernel") *value = c->sweep_kernel;
     else if (k == "pc_apply_sync") *value = c->pc_apply_sync;
     else if (k == "reduction_order") *value = c->red_order;
+    else if (k == "spin_limit") *value = c->spin_limit > 0 ? c->spin_limit : kSpinLimit;
+    else if (k == "admission_free_bytes") *value = c->admission_free_bytes;
+    else if (k == "admission_reserve_bytes") *value = c->admission_reserve_bytes;
     else if (k == "chunk_rows") *value = c->chunk_rows;
     else if (k == "sweep_cluster") *value = c->sweep_cluster;
     else if (k == "vec_ctas_per_sm") *value = c->vec_ctas_per_sm;

@@ -4,7 +4,8 @@
 // rows a row reads).  Work is handed out in tasks of kSweepRows rows through
 // one atomic ticket, so a task is taken only by a running warp and every row
 // it waits on belongs to an earlier task: the waits always end.  Each wait is
-// still bounded (kSpinLimit polls); on expiry the kernel records a timeout
+// still bounded (the context's spin_limit polls, default kSpinLimit); on
+// expiry the kernel records a timeout
 // in err[0] and finishes with a zero in place of the missing value.
 //
 // Readiness is carried by the value itself: the output vector is filled with
@@ -53,18 +54,19 @@ __device__ __forceinline__ int grab_task(int* ticket, int ntasks)
     return __shfl_sync(0xffffffffu, t, 0);
 }
 
-// Polls p until it holds a value.  Gives up after kSpinLimit polls (sets
+// Polls p until it holds a value.  Gives up after lim polls (the context's
+// "spin_limit"; sets
 // err[0]) or as soon as another wait has given up, so a failed sweep drains
 // in one bounded wait instead of one per row.
 template <typename T>
-__device__ __forceinline__ T wait_value(const T* p, int* err, int sleep_ns)
+__device__ __forceinline__ T wait_value(const T* p, int* err, int sleep_ns, long long lim)
 {
     T w = ld_volatile(p);
     if (!is_sentinel(w)) return w;
     long long spins = 0;
     do {
         if ((++spins & 255) == 0 && *(volatile int*)err) return T(0);
-        if (spins > kSpinLimit) {
+        if (spins > (lim > 0 ? lim : kSpinLimit)) {
             atomicExch(err, 1);
             return T(0);
         }
@@ -131,9 +133,9 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            if (j < nr) rr = sweep_step<T, S>(rr, av[j], wait_value(y + cc[j], sv.err, op.sleep_ns));
+            if (j < nr) rr = sweep_step<T, S>(rr, av[j], wait_value(y + cc[j], sv.err, op.sleep_ns, sv.spin));
         }
-        for (int j = a + 8; j < e; ++j) rr = sweep_step<T, S>(rr, fv[j], wait_value(y + fc[j], sv.err, op.sleep_ns));
+        for (int j = a + 8; j < e; ++j) rr = sweep_step<T, S>(rr, fv[j], wait_value(y + fc[j], sv.err, op.sleep_ns, sv.spin));
         const S dia = static_cast<const S*>(F.dia)[k];
         typedef typename std::conditional<(sizeof(S) > sizeof(T)), S, T>::type W;   // promoted type
         st_volatile(y + row, unsentinel(T(W(rr) * W(dia))));
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(kBlock) k_sweep(SetView sv, SweepOp op)
 // and the chunk's outputs written back at its end by all warps, coalesced.  Chunks
 // depend on earlier chunks only and waves on earlier waves, and a chunk is
 // held by a running CTA, so the waits end; they are bounded all the same
-// (kSpinLimit polls, then a timeout flag and a drain).  The arithmetic per
+// (spin_limit polls, then a timeout flag and a drain).  The arithmetic per
 // row is k_sweep's (same entry order, same roundings).
 constexpr int kStageBufs = 3;
 constexpr int kRecvDepth = 2;                       // receive quads in flight per receiver lane
@@ -232,6 +234,10 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 
 // Bounded mbarrier wait: after kSpinLimit polls it records a timeout and
 // keeps waiting up to the same bound again (a staged copy always completes).
+// The bound is fixed, not the context's spin_limit: it guards the copies of
+// the chunk's own structure, which are in flight whatever the dependencies
+// do, so a CTA never reads a buffer before its copy lands, never refills one
+// the compute warps still read, and never ends with a copy in flight.
 __device__ __forceinline__ void mbar_wait(unsigned long long* bar, unsigned parity, int* err)
 {
     long long spins = 0;
@@ -335,13 +341,13 @@ __device__ __forceinline__ void st_slot(double* p, double v)
 
 // A result of an earlier chunk read directly (same bound and drain rule as wait_value).
 template <typename T>
-__device__ __noinline__ T poll_value(const T* p, int* err, int sleep_ns)
+__device__ __noinline__ T poll_value(const T* p, int* err, int sleep_ns, long long lim)
 {
     T w = ld_relaxed_gpu(p);
     long long spins = 0;
     while (is_sentinel(w)) {
         if ((++spins & 255) == 0 && *(volatile int*)err) return T(0);
-        if (spins > kSpinLimit) {
+        if (spins > (lim > 0 ? lim : kSpinLimit)) {
             atomicExch(err, 1);
             return T(0);
         }
@@ -353,13 +359,13 @@ __device__ __noinline__ T poll_value(const T* p, int* err, int sleep_ns)
 
 // A receive slot not filled yet: wait for the receiver (same bound and drain rule).
 template <typename T>
-__device__ __noinline__ T poll_slot(const T* p, int* err)
+__device__ __noinline__ T poll_slot(const T* p, int* err, long long lim)
 {
     T w = ld_slot(p);
     long long spins = 0;
     while (is_sentinel(w)) {
         if ((++spins & 255) == 0 && *(volatile int*)err) return T(0);
-        if (spins > kSpinLimit) {
+        if (spins > (lim > 0 ? lim : kSpinLimit)) {
             atomicExch(err, 1);
             return T(0);
         }
@@ -407,7 +413,7 @@ __device__ __forceinline__ void st_slot4(double* p, const double* v)
 template <typename T, bool PULL>
 __device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, const int2* __restrict__ cquad,
                                               const int* __restrict__ cqpull, int x0, int nx, const T* ypos, T* slot,
-                                              int rw, int lane, int* err, int sleep_ns)
+                                              int rw, int lane, int* err, int sleep_ns, long long lim)
 {
     const int q0 = x0 >> 2, nq = nx >> 2;
     for (int row0 = rw; 32 * row0 < nq; row0 += kRecvWarps * kRecvDepth) {
@@ -464,7 +470,7 @@ __device__ __forceinline__ void receive_chunk(const int* __restrict__ cext, cons
             }
             if (!left) break;
             if ((++spins & 255) == 0 && *(volatile int*)err) break;
-            if (spins > kSpinLimit) {
+            if (spins > (lim > 0 ? lim : kSpinLimit)) {
                 atomicExch(err, 1);
                 break;
             }
@@ -687,10 +693,10 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
             // receiver warps
             if (cqpull)
                 receive_chunk<T, true>(cext, TF.cquad, cqpull, x0, nx, ypos, vec + B + kSlotBase, (tid - CT) >> 5,
-                                       tid & 31, sv.err, op.sleep_ns);
+                                       tid & 31, sv.err, op.sleep_ns, sv.spin);
             else
                 receive_chunk<T, false>(cext, TF.cquad, nullptr, x0, nx, ypos, vec + B + kSlotBase, (tid - CT) >> 5,
-                                        tid & 31, sv.err, op.sleep_ns);
+                                        tid & 31, sv.err, op.sleep_ns, sv.spin);
         } else {
             // compute warps: all waves of the chunk, one cursor across
             // segments; the next wave's rows load while this one computes
@@ -748,7 +754,7 @@ __global__ void __launch_bounds__(32 * (CW + kChunkExtraWarps)) k_sweep_chunk(Se
                         for (int k = 0; k < KM; ++k) {
                             if (is_sentinel(dv[q][k])) {
                                 const int c = cur.col[q][k];
-                                dv[q][k] = c >= 0 ? poll_slot(vec + c, sv.err) : poll_value(ypos + (-c - 2), sv.err, op.sleep_ns);
+                                dv[q][k] = c >= 0 ? poll_slot(vec + c, sv.err, sv.spin) : poll_value(ypos + (-c - 2), sv.err, op.sleep_ns, sv.spin);
                             }
                         }
                 }
@@ -829,16 +835,17 @@ struct FactorOp {
     const int* lt_row;        // k
     const double* a;          // A's FP64 values (IC(0) reads, never writes)
     int* err;
+    long long spin;           // polls before a dependency wait gives up
 };
 
-__device__ __forceinline__ double wait_acquire(const double* p, int* err)
+__device__ __forceinline__ double wait_acquire(const double* p, int* err, long long lim)
 {
     double w;
     asm volatile("ld.acquire.gpu.global.f64 %0, [%1];" : "=d"(w) : "l"(p) : "memory");
     long long spins = 0;
     while (is_sentinel(w)) {
         if ((++spins & 255) == 0 && *(volatile int*)err) return 1.0;
-        if (spins > kSpinLimit) {
+        if (spins > (lim > 0 ? lim : kSpinLimit)) {
             atomicExch(err, 1);
             return 1.0;
         }
@@ -865,7 +872,7 @@ __global__ void __launch_bounds__(kBlock) k_ilu0_factor(FactorOp op)
         for (int kc = a; kc < e; ++kc) {
             const int k = op.ci[kc];
             if (k >= i) break;
-            const double ik = wait_acquire(op.inv_dia + k, op.err);
+            const double ik = wait_acquire(op.inv_dia + k, op.err, op.spin);
             const double aik = __dmul_rn(op.lu[kc], ik);
             op.lu[kc] = aik;
             // merge-walk row k (sorted) against the rest of row i (sorted)
@@ -900,7 +907,7 @@ __global__ void __launch_bounds__(kBlock) k_ic0_factor(FactorOp op)
         double diag = op.a[op.dpos[i]];
         for (int q = op.lt_rp[i]; q < op.lt_rp[i + 1]; ++q) {
             const int k = op.lt_row[q];
-            const double ik = wait_acquire(op.inv_dia + k, op.err);
+            const double ik = wait_acquire(op.inv_dia + k, op.err, op.spin);
             const double dk = __dmul_rn(op.a[op.lt_src[q]], ik);
             // u_ii -= d * d with the product rounded first, as the reference
             // evaluates it (no fused multiply-add)

@@ -62,3 +62,19 @@ def test_trace_report_api_without_gpu():
     trace.enable(True)
     assert trace.report() == {}
     trace.enable(False)
+
+
+def test_server_admission_rule_without_gpu():
+    from mtl4_b200 import _lib
+    L = _lib.load()
+    GiB = 1 << 30
+    # with a byte budget
+    assert L.mtlg_server_admission(3 * GiB, 6 * GiB, 10 * GiB, 0, 0) == 1
+    assert L.mtlg_server_admission(5 * GiB, 6 * GiB, 10 * GiB, 0, 0) == 0    # waits for retirements
+    assert L.mtlg_server_admission(11 * GiB, 0, 10 * GiB, 0, 0) == -1        # never fits
+    # by free memory (simulated 8 GiB free, 1 GiB reserve)
+    assert L.mtlg_server_admission(7 * GiB, 0, 0, 8 * GiB, GiB) == 1
+    assert L.mtlg_server_admission(7 * GiB + 1, 0, 0, 8 * GiB, GiB) == -1
+    assert L.mtlg_server_admission(9 * GiB, 4 * GiB, 0, 8 * GiB, GiB) == 0   # room once held requests retire
+    assert L.mtlg_server_admission(12 * GiB, 4 * GiB, 0, 8 * GiB, GiB) == -1
+    assert L.mtlg_server_admission(1, 0, 0, GiB // 2, GiB) == -1            # free memory below the reserve

@@ -141,6 +141,48 @@ def test_server_admission_and_cancel(ctx):
     assert srv2.stats()["cancelled"] == 1
 
 
+def test_server_admits_by_free_device_memory(ctx):
+    # no byte budget: admission by the device's free memory less a reserve.
+    # The free figure is simulated (context tuning) so that one request fits
+    # at a time; the others wait in the queue and are admitted as earlier
+    # ones retire; a request larger than free + held memory is refused.
+    from mtl4_b200 import _lib, serve
+    A = P.vardiff_2d(48, sigma=1.0, seed=4)
+    b = P.random_rhs(A.n_rows, 3)
+    probe = serve.server(ctx, max_active=4, iters_per_step=8)
+    probe.submit(A, b, "cg", "ic_0")
+    probe.step()
+    one = probe.stats()["bytes_in_use"]
+    assert one > 0
+    del probe
+    old = {k: ctx.get_tuning(k) for k in ("admission_free_bytes", "admission_reserve_bytes")}
+    ctx.set_tuning("admission_free_bytes", int(one * 1.5))
+    ctx.set_tuning("admission_reserve_bytes", 0)
+    try:
+        srv = serve.server(ctx, max_active=4, iters_per_step=8)
+        ids = [srv.submit(A, b, "cg", "ic_0") for _ in range(3)]
+        most = 0
+        done = {}
+        for _ in range(5000):
+            srv.step()
+            most = max(most, srv.stats()["active"])
+            for i in ids:
+                if i not in done and i in srv.n:
+                    r = srv.poll(i)
+                    if r is not None:
+                        done[i] = r
+            if len(done) == len(ids):
+                break
+        assert most == 1 and len(done) == 3
+        assert all(r.error_code == 0 and relres(A, r.x, b) <= 1.05e-8 for r in done.values())
+        big = P.vardiff_2d(160, sigma=1.0, seed=4)
+        with pytest.raises(_lib.MtlError):
+            srv.submit(big, P.random_rhs(big.n_rows, 3), "cg", "ic_0")   # more than free + held
+    finally:
+        for k, v in old.items():
+            ctx.set_tuning(k, v)
+
+
 def test_batch_and_server_finish_stalled_refinement_in_fp64(ctx):
     # the served stream's request 33 is too ill-conditioned for the FP32 inner
     # solve; batch and server finish it in FP64 and report that they did

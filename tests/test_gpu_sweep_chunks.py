@@ -202,3 +202,56 @@ def test_batch_many_chunks_matches_standalone(ctx, solver, kind):
             assert r.error_code == 0
             assert r.iterations == it.iterations()
             assert np.array_equal(r.x, x.numpy())
+
+
+@pytest.mark.parametrize("cluster", [1, 4])
+def test_expired_dependency_waits_report_timeout_and_recover(ctx, cluster):
+    # the context's spin_limit bounds every dependency wait of the sweeps; at
+    # one poll the chunks' waits on earlier chunks expire: the apply reports
+    # MTLG_ERR_TIMEOUT (device_timeout) with the context still usable, and
+    # the next apply at the default limit is bitwise the oracle's again.  The
+    # chunks' own staging copies keep their fixed bound, so nothing is in
+    # flight when a CTA ends.
+    from mtl4_b200 import _lib, itl
+    A = P.convdiff_3d(40)
+    v = np.random.default_rng(5).standard_normal(A.n_rows).astype(np.float32)
+    want = O.port_pc_apply(A, "ilu_0", v)
+    with tuning(ctx, chunk_rows=1600, sweep_cluster=cluster):
+        Pc = itl.pc.ilu_0(dev(A, ctx), np.float32)
+        assert Pc.sweep_plan(np.float32)["chunks"] >= 16
+        assert np.array_equal(itl.solve(Pc, vec(v, ctx, np.float32)).numpy(), want)
+        with tuning(ctx, spin_limit=1):
+            with pytest.raises(_lib.device_timeout):
+                itl.solve(Pc, vec(v, ctx, np.float32))
+        for _ in range(2):
+            assert np.array_equal(itl.solve(Pc, vec(v, ctx, np.float32)).numpy(), want)
+
+
+def test_expired_waits_in_a_solve_report_timeout_and_recover(ctx):
+    # a solve whose loop graphs were built at a one-poll limit: the sweeps'
+    # waits expire inside the graph, the solve reports MTLG_ERR_TIMEOUT, and
+    # the preconditioner's sweep state is re-armed; later solves (sets built
+    # at the default limit) are bitwise the earlier ones
+    from mtl4_b200 import _lib, itl, mtl
+    A = P.convdiff_3d(32)
+    _, b = P.rhs_from_solution(A, 1)
+    Ad = dev(A, ctx)
+
+    def solve(Pc):
+        x = mtl.dense_vector(A.n_rows, np.float64, ctx)
+        it = itl.basic_iteration(vec(b, ctx), 500, 1e-8)
+        itl.bicgstab(Ad, x, vec(b, ctx), Pc, it)
+        return x.numpy(), it
+
+    with tuning(ctx, chunk_rows=1024):
+        Pa = itl.pc.ilu_0(Ad, np.float64)
+        Pb = itl.pc.ilu_0(Ad, np.float64)
+        x0, it0 = solve(Pa)
+        with tuning(ctx, spin_limit=1):
+            with pytest.raises(_lib.device_timeout):
+                solve(Pb)
+        Pc = itl.pc.ilu_0(Ad, np.float64)
+        x1, it1 = solve(Pc)
+        x2, it2 = solve(Pa)
+    assert it0.is_converged() and it1.iterations() == it0.iterations() and np.array_equal(x1, x0)
+    assert it2.iterations() == it0.iterations() and np.array_equal(x2, x0)
