@@ -24,6 +24,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <iostream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -86,6 +87,15 @@ class context {
     }
     mtlg_ctx* get() const { return h_.get(); }
     void synchronize() const { check(mtlg_ctx_synchronize(get()), "synchronize"); }
+    /// Device residual log of at least `tests` termination tests (grown, never shrunk).
+    void ensure_residual_log(int tests)
+    {
+        if (tests > log_cap_) {
+            check(mtlg_ctx_set_residual_log(get(), tests), "residual log");
+            log_cap_ = tests;
+        }
+    }
+    int residual_log_capacity() const { return log_cap_; }
     int64_t kernel_launches() const { return mtlg_ctx_kernel_launches(get()); }
     static context& default_context()
     {
@@ -95,6 +105,7 @@ class context {
 
   private:
     std::shared_ptr<mtlg_ctx> h_;
+    int log_cap_ = 0;
 };
 
 template <typename T> struct mat_cvec_times;
@@ -253,6 +264,24 @@ inline double two_norm(const dense_vector<T>& x)
 }
 
 }  // namespace gpu
+
+#ifdef MTL_COLLECTION_INCLUDE
+// With MTL4's headers included first, its templates take their defaults from
+// mtl::Collection (concept/collection.hpp:43-55), e.g. the Value argument of
+// itl::pc::diagonal<Matrix, Value>: the GPU types are collections of T.
+template <typename T>
+struct Collection<gpu::compressed2D<T> > {
+    typedef T value_type;
+    typedef const T& const_reference;
+    typedef std::size_t size_type;
+};
+template <typename T>
+struct Collection<gpu::dense_vector<T> > {
+    typedef T value_type;
+    typedef const T& const_reference;
+    typedef std::size_t size_type;
+};
+#endif
 }  // namespace mtl
 
 namespace itl {
@@ -300,17 +329,119 @@ class basic_iteration {
 };
 #endif
 
+#ifndef ITL_CYCLIC_ITERATION_INCLUDE
+#define ITL_CYCLIC_ITERATION_INCLUDE
+/// Termination control that prints the residual every `cycle` iterations
+/// and a summary from error_code(), as the reference's cyclic_iteration
+/// (itl/iteration/cyclic_iteration.hpp:22-95) does.  On the GPU the tests run
+/// on the device; their (iteration, residual) log is replayed through
+/// finished() after the solve, so the output is the same lines.
+template <class Real, class OStream = std::ostream>
+class cyclic_iteration : public basic_iteration<Real> {
+    typedef basic_iteration<Real> super;
+
+  public:
+    template <class Vector>
+    cyclic_iteration(const Vector& r0, int max_iter, Real tol, Real atol = Real(0), int cycle = 100,
+                     OStream& out = std::cout)
+        : super(r0, max_iter, tol, atol), cycle_(cycle), last_print_(-1), multi_print_(false), out_(out)
+    {}
+    cyclic_iteration(Real r0, int max_iter, Real tol, Real atol = Real(0), int cycle = 100, OStream& out = std::cout)
+        : super(r0, max_iter, tol, atol), cycle_(cycle), last_print_(-1), multi_print_(false), out_(out)
+    {}
+    bool finished(const Real& r)
+    {
+        const bool ret = super::finished(r);
+        print_resid();
+        return ret;
+    }
+    cyclic_iteration& operator++() { super::operator++(); return *this; }
+    cyclic_iteration& operator+=(int n) { super::operator+=(n); return *this; }
+    operator int() const { return error_code(); }
+    bool is_multi_print() const { return multi_print_; }
+    void set_multi_print(bool m) { multi_print_ = m; }
+    void set_cycle(int c) { cycle_ = c; }
+    /// Error code with the final summary (printed on every call, as the reference does).
+    int error_code() const
+    {
+        out_ << "finished! error code = " << super::error_code() << '\n'
+             << this->iterations() << " iterations\n"
+             << this->resid() << " is actual final residual. \n"
+             << this->relresid() << " is actual relative tolerance achieved. \n"
+             << "Relative tol: " << this->tol() << "  Absolute tol: " << this->atol() << '\n'
+             << "Convergence:  " << std::pow(this->relresid(), 1.0 / double(this->iterations())) << std::endl;
+        return super::error_code();
+    }
+
+  private:
+    void print_resid()
+    {
+        if (this->iterations() % cycle_ == 0 && (multi_print_ || this->iterations() != last_print_)) {
+            out_ << "iteration " << this->iterations() << ": resid " << this->resid() << std::endl;
+            last_print_ = this->iterations();
+        }
+    }
+    int cycle_, last_print_;
+    bool multi_print_;
+    OStream& out_;
+};
+#endif
+
+#ifndef ITL_NOISY_ITERATION_INCLUDE
+#define ITL_NOISY_ITERATION_INCLUDE
+/// cyclic_iteration printing every iteration (itl/iteration/noisy_iteration.hpp:22-35).
+template <class Real, class OStream = std::ostream>
+class noisy_iteration : public cyclic_iteration<Real, OStream> {
+  public:
+    template <class Vector>
+    noisy_iteration(const Vector& r0, int max_iter, Real tol, Real atol = Real(0), OStream& out = std::cout)
+        : cyclic_iteration<Real, OStream>(r0, max_iter, tol, atol, 1, out)
+    {}
+};
+#endif
+
 namespace gpu {
 /// Takes a device result into any iteration object with the reference's
 /// members (iterations via +=, resid via finished(), error via fail()).
+/// With a residual log, every device-side termination test is replayed
+/// through finished() in order, so iteration objects that act on each test
+/// (cyclic_iteration, noisy_iteration, the reference's own) see the same
+/// sequence as in the reference's loop.  error_code() is not read here: the
+/// reference's cyclic_iteration prints its summary on each call, and the
+/// solver's return reads it once.
 template <class Iteration>
-inline int take_result(Iteration& iter, const mtlg_iter_result& r)
+inline int take_result(Iteration& iter, const mtlg_iter_result& r, const std::vector<double>* log = nullptr)
 {
-    const int add = r.iterations - iter.iterations();
-    if (add > 0) iter += add;
-    iter.finished(typename Iteration::real(r.resid));
-    if (r.error_code != iter.error_code()) iter.fail(r.error_code);
+    typedef typename Iteration::real Real;
+    if (log && !log->empty()) {
+        for (std::size_t k = 0; k + 1 < log->size(); k += 2) {
+            const int add = int((*log)[k]) - iter.iterations();
+            if (add > 0) iter += add;
+            iter.finished(Real((*log)[k + 1]));
+        }
+        const int add = r.iterations - iter.iterations();
+        if (add > 0) iter += add;
+    } else {
+        const int add = r.iterations - iter.iterations();
+        if (add > 0) iter += add;
+        iter.finished(Real(r.resid));
+    }
+    if (r.error_code > 1) iter.fail(r.error_code);
     return r.error_code;
+}
+
+/// The residual log of the context's last solve (empty when it holds more
+/// tests than the capacity, or none).
+inline std::vector<double> residual_log(const mtl::gpu::context& c)
+{
+    int count = 0;
+    mtl::gpu::check(mtlg_ctx_residual_log(c.get(), nullptr, 0, &count), "residual log");
+    std::vector<double> out;
+    if (count > 0 && count <= c.residual_log_capacity()) {
+        out.resize(std::size_t(2 * count));
+        mtl::gpu::check(mtlg_ctx_residual_log(c.get(), out.data(), count, &count), "residual log");
+    }
+    return out;
 }
 
 template <class Iteration>
@@ -418,9 +549,12 @@ inline int run(int solver, const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_v
 {
     mtlg_iter_params p = params_of(iter, restart);
     mtlg_iter_result r;
+    // BiCGSTAB tests twice per iteration: room for every test of the solve
+    A.ctx().ensure_residual_log(2 * iter.max_iterations() + 8);
     const int s = mtlg_solve(A.ctx().get(), solver, A.get(), L ? L->get() : nullptr, R ? R->get() : nullptr,
                              x.get(), b.get(), &p, &r);
-    take_result(iter, r);
+    const std::vector<double> log = residual_log(A.ctx());
+    take_result(iter, r, &log);
     mtl::gpu::check(s, solver == MTLG_CG ? "cg" : solver == MTLG_BICGSTAB ? "bicgstab" : "gmres");
     return iter.error_code();
 }

@@ -167,6 +167,17 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * Read-only keys for get: "sweep_max_blocks_per_sm", "sm_count". */
 int mtlg_ctx_set_tuning(mtlg_ctx* ctx, const char* key, int64_t value);
 int mtlg_ctx_get_tuning(mtlg_ctx* ctx, const char* key, int64_t* value);
+/* Residual log of CG and BiCGSTAB solves made through mtlg_solve: with a
+ * capacity > 0 every termination test of the next solves (basic_iteration::
+ * finished, basic_iteration.hpp:50-65; BiCGSTAB tests r at the loop top and s
+ * mid-iteration) is recorded on the device as (iteration, residual) and read
+ * back for the last solve with mtlg_ctx_residual_log: pairs[2k], pairs[2k+1]
+ * for k < min(count, capacity); count may exceed the capacity (truncated).
+ * Replaying the pairs through finished() gives a cyclic_iteration /
+ * noisy_iteration (itl/iteration/cyclic_iteration.hpp:29-95) its per-cycle
+ * output.  0 turns the log off (default).  GMRES records no log. */
+int mtlg_ctx_set_residual_log(mtlg_ctx* ctx, int capacity);
+int mtlg_ctx_residual_log(mtlg_ctx* ctx, double* pairs, int capacity, int* count);
 /* Bytes of device memory the context's objects hold. */
 size_t mtlg_ctx_bytes_in_use(mtlg_ctx* ctx);
 const char* mtlg_status_string(int status);

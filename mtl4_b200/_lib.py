@@ -122,6 +122,8 @@ SIGNATURES = {
     "mtlg_batch_size": (C.c_int, [VP]),
     "mtlg_partition_systems": (C.c_int, [C.c_int64, VP, C.c_int, VP, VP]),
     "mtlg_trace_enable": (C.c_int, [C.c_int]),
+    "mtlg_ctx_set_residual_log": (C.c_int, [VP, C.c_int]),
+    "mtlg_ctx_residual_log": (C.c_int, [VP, VP, C.c_int, C.POINTER(C.c_int)]),
     "mtlg_server_admission": (C.c_int, [C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t]),
     "mtlg_mm_read": (C.c_int, [VP, C.c_char_p, C.POINTER(VP)]),
     "mtlg_mm_read_host": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),

@@ -190,6 +190,8 @@ struct SysState {
     int outer, max_outer;
     int inner_total, inner_max;
     double inner_rtol, outer_rtol;
+    double* log;            // residual log: (iteration, resid) of every termination test
+    int log_cap, log_n;     // capacity in tests; tests made (log_n > log_cap: truncated)
 };
 
 // Per-launch view of the system set.
@@ -378,8 +380,21 @@ __device__ __forceinline__ void set_cond(const SetView& sv, unsigned v)
 // 85-93): converged if resid <= rtol*norm_r0 or resid <= atol (atol only when
 // norm_r0 == 0); otherwise "too many iterations" once iter >= max_iter.
 // Returns true when the system stops; retires it from the running count.
+// One termination test into the system's residual log (when it has one):
+// the (iteration, residual) pairs let the host replay the tests into an
+// iteration object, e.g. a cyclic_iteration that prints every cycle.
+__device__ __forceinline__ void log_check(SysState& s, double resid)
+{
+    if (s.log && s.log_n < s.log_cap) {
+        s.log[2 * s.log_n] = double(s.iter);
+        s.log[2 * s.log_n + 1] = resid;
+    }
+    s.log_n += 1;
+}
+
 __device__ __forceinline__ bool check_finished(const SetView& sv, SysState& s, double resid)
 {
+    log_check(s, resid);
     s.resid = resid;
     bool conv = (s.norm_r0 == 0.0) ? (resid <= s.atol) : (resid <= s.rtol * s.norm_r0 || resid <= s.atol);
     if (conv) {

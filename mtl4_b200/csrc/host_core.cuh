@@ -34,6 +34,9 @@ struct mtlg_ctx {
     int red_order = 0;          // tuning: FP64 dots and norms, 0 tile-parallel, 1 the reference's summation order
     int64_t admission_free_bytes = 0;     // tuning: stand-in for cudaMemGetInfo's free bytes (0: query)
     int64_t spin_limit = 0;               // tuning: polls before a device dependency wait gives up (0: kSpinLimit)
+    double* log_dev = nullptr;            // residual log of single solves (2 * log_cap doubles)
+    int log_cap = 0;
+    int log_n = 0;                        // tests of the last logged solve (CG / BiCGSTAB)
     int64_t admission_reserve_bytes = -1; // tuning: bytes kept out of admission (-1: max(1 GiB, 2%))
     int* d_scratch_err = nullptr;
     int sweep_blocks() const

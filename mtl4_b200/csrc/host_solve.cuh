@@ -17,6 +17,8 @@ struct SysInput {
     const void* b = nullptr;
     int max_iter = 0;
     double rtol = 0, atol = 0, norm_r0 = -1;
+    double* log = nullptr;       // device residual log (2 * log_cap doubles) or null
+    int log_cap = 0;
 };
 
 struct SolveSet {
@@ -617,6 +619,9 @@ inline SysState initial_state(const SysInput& si)
     s.norm_r0 = si.norm_r0;
     s.status = MTLG_ST_RUNNING;
     s.ostatus = MTLG_ST_RUNNING;
+    s.log = si.log;
+    s.log_cap = si.log_cap;
+    s.log_n = 0;
     return s;
 }
 

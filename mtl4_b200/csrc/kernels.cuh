@@ -168,6 +168,7 @@ __device__ void finalize(const SetView& sv, int fin, int sys, const double* dots
         // iter.finished(s) (bicgstab.hpp:64): on true, x += alpha*phat is
         // still due; the x/r pass does it and then retires the system.
         const double res = sqrt(fabs(dots[0]));
+        log_check(s, res);
         s.resid = res;
         bool conv = (s.norm_r0 == 0.0) ? (res <= s.atol) : (res <= s.rtol * s.norm_r0 || res <= s.atol);
         if (conv) { s.flags |= FLAG_FINISHING; s.error = 0; s.dots[3] = MTLG_ST_CONVERGED; }

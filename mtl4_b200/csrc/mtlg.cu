@@ -280,6 +280,40 @@ const char* mtlg_status_string(int s)
 
 const char* mtlg_last_error_message(void) { return last_error(); }
 
+int mtlg_ctx_set_residual_log(mtlg_ctx* c, int capacity)
+{
+    MTLG_CHECK_ARG(c && capacity >= 0, "ctx/capacity");
+    if (c->log_dev) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->log_dev);
+        c->in_use -= size_t(c->log_cap) * 16;
+        c->log_dev = nullptr;
+    }
+    c->log_cap = 0;
+    c->log_n = 0;
+    if (capacity > 0) {
+        MTLG_CUDA(cudaSetDevice(c->device));
+        if (cudaMalloc(&c->log_dev, size_t(capacity) * 16) != cudaSuccess) {
+            cudaGetLastError();
+            c->log_dev = nullptr;
+            set_error("residual log of %d tests", capacity);
+            return MTLG_ERR_OOM;
+        }
+        c->in_use += size_t(capacity) * 16;
+        c->log_cap = capacity;
+    }
+    return MTLG_OK;
+}
+
+int mtlg_ctx_residual_log(mtlg_ctx* c, double* pairs, int capacity, int* count)
+{
+    MTLG_CHECK_ARG(c && count, "ctx/count");
+    *count = c->log_n;
+    const int k = std::min(std::min(c->log_n, c->log_cap), capacity);
+    if (pairs && k > 0) MTLG_CUDA(cudaMemcpy(pairs, c->log_dev, size_t(k) * 16, cudaMemcpyDeviceToHost));
+    return MTLG_OK;
+}
+
 int mtlg_trace_enable(int on)
 {
     TraceState& t = trace_state();
@@ -363,6 +397,7 @@ int mtlg_ctx_destroy(mtlg_ctx* c)
             }
         }
     }
+    if (c->log_dev) cudaFree(c->log_dev);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return MTLG_OK;
@@ -983,6 +1018,7 @@ static int timed_result(mtlg_ctx* c, SolveSet& ss, cudaEvent_t e0, cudaEvent_t e
         fill_result(h, ss.mixed != 0, res);
         res->seconds = ms * 1e-3;
     }
+    if (c->log_cap) c->log_n = h.log_n;
     if (flags[0]) {
         int z = 0;
         MTLG_CUDA(cudaMemcpy(ss.misc.p + 1, &z, sizeof z, cudaMemcpyHostToDevice));
@@ -1008,7 +1044,10 @@ int mtlg_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* L, mtlg_pc* R, mtl
     MTLG_CHECK_ARG(c && p, "ctx/params");
     MTLG_TRY(check_solve_args(solver, A, x, b, L));
     MTLG_CHECK_ARG(x->dtype == b->dtype, "x and b dtypes differ");
-    if (solver == MTLG_GMRES) return mtlg_gmres_impl(c, A, L, R, x, b, p, res);
+    if (solver == MTLG_GMRES) {
+        c->log_n = 0;   // GMRES runs its tests on the host: no residual log
+        return mtlg_gmres_impl(c, A, L, R, x, b, p, res);
+    }
     const int f32 = x->dtype == MTLG_F32;
     if (L && L->kind == MTLG_PC_IDENTITY) L = nullptr;   // is_identity(P) short-cut (cg.hpp:80-81)
     SetKey key{A, L, solver, f32, 0, c->red_order};
@@ -1032,6 +1071,9 @@ int mtlg_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* L, mtlg_pc* R, mtl
     si.rtol = p->rtol;
     si.atol = p->atol;
     si.norm_r0 = p->norm_r0;
+    si.log = c->log_dev;
+    si.log_cap = c->log_cap;
+    c->log_n = 0;
     ss.h_desc[0].x = x->p;
     ss.h_desc[0].b = b->p;
     MTLG_CUDA(cudaMemcpyAsync(ss.desc.p, ss.h_desc.data(), sizeof(SysDesc), cudaMemcpyHostToDevice, c->stream));

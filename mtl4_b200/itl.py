@@ -13,6 +13,7 @@ breakdown raises unexpected_orthogonality.
 from __future__ import annotations
 
 import ctypes as C
+import sys
 import math
 
 import numpy as np
@@ -69,6 +70,74 @@ class basic_iteration:
         self.fp64_fallback = bool(r.fp64_fallback)
         if r.norm_r0 > 0 or self._norm_r0 == 0:
             self._norm_r0 = r.norm_r0
+
+
+class cyclic_iteration(basic_iteration):
+    """basic_iteration that prints the residual every `cycle` iterations and
+    a summary from error_code(), as the reference's cyclic_iteration
+    (itl/iteration/cyclic_iteration.hpp:22-95).  The termination tests run on
+    the device; their (iteration, residual) log is replayed through
+    finished() after the solve, so the lines are the ones the reference's
+    loop prints (C++ stream formatting: 6 significant digits)."""
+
+    wants_log = True
+
+    def __init__(self, r0_or_norm, max_iter: int, rtol: float, atol: float = 0.0, cycle: int = 100, out=None):
+        super().__init__(r0_or_norm, max_iter, rtol, atol)
+        self.cycle = int(cycle)
+        self.last_print = -1
+        self.multi_print = False
+        self.quiet = False
+        self.suppress = False
+        self.out = out if out is not None else sys.stdout
+
+    def set_multi_print(self, m: bool):
+        self.multi_print = bool(m)
+
+    def set_cycle(self, c: int):
+        self.cycle = int(c)
+
+    def finished(self, r: float) -> bool:
+        """basic_iteration::finished(r) (basic_iteration.hpp:43-65), then the
+        cycle's print-out."""
+        self._resid = float(r)
+        nr0 = self._norm_r0
+        conv = (r <= self._atol) if nr0 == 0 else (r <= self.rtol * nr0 or r <= self._atol)
+        done = conv
+        if not conv and self.i >= self.max_iter:
+            self.error, done = 1, True
+        if not self.quiet and self.i % self.cycle == 0 and (self.multi_print or self.i != self.last_print):
+            self.out.write(f"iteration {self.i}: resid {_g(self._resid)}\n")
+            self.last_print = self.i
+        return done
+
+    def error_code(self) -> int:
+        if not self.suppress:
+            it = max(self.i, 1)
+            self.out.write(f"finished! error code = {self.error}\n{self.i} iterations\n"
+                           f"{_g(self._resid)} is actual final residual. \n"
+                           f"{_g(self.relresid())} is actual relative tolerance achieved. \n"
+                           f"Relative tol: {_g(self.rtol)}  Absolute tol: {_g(self._atol)}\n"
+                           f"Convergence:  {_g(self.relresid() ** (1.0 / it))}\n")
+        return self.error
+
+    def _replay(self, log, r: _lib.IterResult):
+        for k in range(len(log) // 2):
+            self.i = int(log[2 * k])
+            self.finished(float(log[2 * k + 1]))
+        self.i = max(self.i, r.iterations)
+
+
+class noisy_iteration(cyclic_iteration):
+    """cyclic_iteration printing every iteration (itl/iteration/noisy_iteration.hpp:22-35)."""
+
+    def __init__(self, r0_or_norm, max_iter: int, rtol: float, atol: float = 0.0, out=None):
+        super().__init__(r0_or_norm, max_iter, rtol, atol, 1, out)
+
+
+def _g(v: float) -> str:
+    """A double as std::ostream prints it by default (%g, 6 digits)."""
+    return "%g" % v
 
 
 class pc:
@@ -155,9 +224,22 @@ def adjoint_solve(P: pc._base, x: dense_vector, y: dense_vector | None = None) -
 def _solve(kind, A, x, b, L, R, it: basic_iteration, restart=0) -> int:
     res = _lib.IterResult()
     params = it._params(restart)
+    logged = getattr(it, "wants_log", False)
+    if logged:
+        A.ctx.ensure_residual_log(2 * it.max_iter + 8)
     st = A.ctx._L.mtlg_solve(A.ctx.h, kind, A.h, L.h if L is not None else None, R.h if R is not None else None,
                              x.h, b.h, C.byref(params), C.byref(res))
-    it._take(res)
+    if logged:
+        log = A.ctx.residual_log()
+        norm_r0 = it._norm_r0
+        it._take(res)
+        if log is not None and len(log):
+            it._norm_r0 = norm_r0 if res.norm_r0 <= 0 else res.norm_r0
+            err, resid = it.error, it._resid
+            it._replay(log, res)
+            it.error, it._resid = err, resid
+    else:
+        it._take(res)
     check(st, ["cg", "bicgstab", "gmres"][kind])
     return it.error_code()
 

@@ -46,6 +46,24 @@ class context:
         check(self._L.mtlg_ctx_get_tuning(self.h, key.encode(), C.byref(v)), "get_tuning")
         return v.value
 
+    def ensure_residual_log(self, tests: int):
+        """Device residual log of at least `tests` termination tests."""
+        if tests > getattr(self, "_log_cap", 0):
+            check(self._L.mtlg_ctx_set_residual_log(self.h, int(tests)), "residual log")
+            self._log_cap = int(tests)
+
+    def residual_log(self):
+        """(iteration, residual) pairs of the last CG / BiCGSTAB solve as a flat
+        array, or None when the log overflowed."""
+        n = C.c_int()
+        check(self._L.mtlg_ctx_residual_log(self.h, None, 0, C.byref(n)), "residual log")
+        if n.value > getattr(self, "_log_cap", 0):
+            return None
+        out = np.zeros(2 * n.value)
+        if n.value:
+            check(self._L.mtlg_ctx_residual_log(self.h, _ptr(out), n.value, C.byref(n)), "residual log")
+        return out
+
     def set_stream(self, cuda_stream_ptr: int | None):
         check(self._L.mtlg_ctx_set_stream(self.h, C.c_void_p(cuda_stream_ptr or 0)), "set_stream")
 

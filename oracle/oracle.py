@@ -75,6 +75,9 @@ def ref_lib(omp: bool = False) -> C.CDLL:
         L.mtlref_refine_solve.argtypes = [VP, C.c_int, C.c_int, VP, VP, C.c_int, C.c_int, C.c_double, C.c_double,
                                           C.c_int, C.POINTER(RefResult)]
         L.mtlref_laplacian_setup.argtypes = [C.c_int, C.c_int, PI, VP, VP, VP]
+        L.mtlref_solve_cyclic.restype = C.c_int
+        L.mtlref_solve_cyclic.argtypes = [VP, C.c_int, C.c_int, VP, VP, C.c_int, C.c_double, C.c_int, C.c_int,
+                                          C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
         L.mtlref_mm_read.restype = C.c_int
         L.mtlref_mm_read.argtypes = [C.c_char_p, PI, PI, PI, VP, VP, VP]
         _REF[key] = L
@@ -163,6 +166,19 @@ class RefMatrix:
                                       rtol, atol, restart, C.byref(r))
         return {"x": x, "iterations": r.iterations, "error": err, "resid": r.resid, "relresid": r.relresid,
                 "setup_s": r.setup_s, "solve_s": r.solve_s}
+
+    def solve_cyclic(self, b, solver="cg", pc="identity", max_iter=2000, rtol=1e-8, cycle=100, multi_print=False):
+        """FP64 solve with itl::cyclic_iteration printing into a string;
+        returns (error, text)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.A.n_rows)
+        need = C.c_size_t()
+        args = [self.h, SOLVER[solver], PC_KIND[pc], _p(b), None, max_iter, rtol, cycle, int(multi_print)]
+        self.L.mtlref_solve_cyclic(*args[:4], _p(x), *args[5:], None, 0, C.byref(need))
+        buf = C.create_string_buffer(need.value)
+        x[:] = 0
+        err = self.L.mtlref_solve_cyclic(*args[:4], _p(x), *args[5:], buf, need.value, None)
+        return err, buf.value.decode()
 
     def refine(self, b, solver="cg", pc="ic_0", max_outer=20, max_inner=2000, rtol=1e-8, inner_rtol=1e-4):
         r = RefResult()

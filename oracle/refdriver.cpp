@@ -25,6 +25,8 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <sstream>
+#include <string>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -317,7 +319,48 @@ static int solve_typed(int solver, int kind, int pc_f32, const Mat& A, const Fac
     }
 }
 
+template <typename PC>
+static int run_cyclic(int solver, const dmat& A, dvec& x, const dvec& b, const PC& P,
+                      itl::cyclic_iteration<double>& iter)
+{
+    if (solver == 0) return itl::cg(A, x, b, P, iter);
+    return itl::bicgstab(A, x, b, P, iter);
+}
+
 extern "C" {
+
+/// FP64 CG (solver 0) or BiCGSTAB (1) with itl::cyclic_iteration<double>
+/// (itl/iteration/cyclic_iteration.hpp:22-95) printing into a string: the
+/// per-cycle residual lines and the final summary that the solver's return
+/// (iter converted to int, error_code()) prints.  text receives at most cap
+/// bytes (NUL-terminated); needed gets the full length + 1.
+int mtlref_solve_cyclic(void* p, int solver, int kind, const double* b, double* x, int max_iter, double rtol,
+                        int cycle, int multi_print, char* text, size_t cap, size_t* needed)
+{
+    RefCsr* h = static_cast<RefCsr*>(p);
+    dvec vb(h->n_rows, const_cast<double*>(b)), vx(h->n_rows, x);
+    std::ostringstream os;
+    itl::cyclic_iteration<double> iter(vb, max_iter, rtol, 0.0, cycle, os);
+    iter.set_multi_print(multi_print != 0);
+    int err = -1;
+    try {
+        const dmat& A = *h->A;
+        if (kind == 0) { itl::pc::identity<dmat> P(A); err = run_cyclic(solver, A, vx, vb, P, iter); }
+        else if (kind == 1) { itl::pc::diagonal<dmat> P(A); err = run_cyclic(solver, A, vx, vb, P, iter); }
+        else if (kind == 2) { itl::pc::ilu_0<dmat> P(A); err = run_cyclic(solver, A, vx, vb, P, iter); }
+        else if (kind == 3) { itl::pc::ic_0<dmat> P(A); err = run_cyclic(solver, A, vx, vb, P, iter); }
+    } catch (const itl::unexpected_orthogonality&) {
+        err = -2;
+    }
+    const std::string t = os.str();
+    if (needed) *needed = t.size() + 1;
+    if (text && cap) {
+        const size_t k = std::min(cap - 1, t.size());
+        std::memcpy(text, t.data(), k);
+        text[k] = 0;
+    }
+    return err;
+}
 
 /// FP64 solve: solver 0 cg, 1 bicgstab, 2 gmres(restart) with right PC = identity.
 /// x is in/out (initial guess on entry).  BiCGSTAB breakdown

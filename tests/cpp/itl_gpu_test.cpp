@@ -3,6 +3,8 @@
 // only the matrix and vector types are the GPU ones.  Exit code 0 = pass.
 #include <cmath>
 #include <cstdio>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "mtl4_b200/itl_gpu.hpp"
@@ -71,6 +73,22 @@ int main()
         itl::bicgstab(A, x, b, P, iter);
         std::printf("bicgstab+ilu_0: %d iterations, relres %.3e\n", iter.iterations(), relres(A, x, b));
         REQUIRE(iter.error_code() == 0 && relres(A, x, b) <= 1.05e-8, "bicgstab+ilu_0");
+    }
+    {
+        // itl::cyclic_iteration: one line per cycle of the device-side tests,
+        // then the summary the solver's return prints
+        itl::pc::diagonal<matrix_type> P(A);
+        std::ostringstream out;
+        itl::cyclic_iteration<double> iter(b, 2000, 1.e-8, 0.0, 25, out);
+        x = 0.0;
+        itl::cg(A, x, b, P, iter);
+        const std::string t = out.str();
+        int lines = 0;
+        for (std::size_t k = 0; (k = t.find("iteration ", k)) != std::string::npos; ++k) ++lines;
+        std::printf("cg+diagonal, cyclic_iteration(25): %d iterations, %d residual lines\n", iter.iterations(), lines);
+        REQUIRE(t.rfind("iteration 0: resid ", 0) == 0, "cyclic first line");
+        REQUIRE(lines == iter.iterations() / 25 + 1, "cyclic line count");
+        REQUIRE(t.find("finished! error code = 0") != std::string::npos, "cyclic summary");
     }
     {
         itl::pc::identity<matrix_type> L(A), R(A);

@@ -66,6 +66,12 @@ def main():
     out["pl_x"] = xq
     out["pl_spmv"] = RQ.spmv(xq)
     out["pl_spmv_f32"] = RQ.spmv(xq.astype(np.float32))
+    # itl::cyclic_iteration output of the reference's loops (per-cycle residual
+    # lines and the summary the solver's return prints)
+    for solver, pc, cycle, multi in [("cg", "diagonal", 10, 0), ("bicgstab", "ilu_0", 1, 0),
+                                     ("bicgstab", "identity", 5, 1)]:
+        err, text = R.solve_cyclic(b, solver, pc, max_iter=2000, rtol=1e-8, cycle=cycle, multi_print=bool(multi))
+        out[f"lap32_{solver}_{pc}_cyclic{cycle}_{multi}"] = np.array(text)
     # mtl::dot and mtl::two_norm (four strided partial sums) on general values
     out["dot_x"] = xq[:1001]
     out["dot_y"] = np.random.default_rng(14).standard_normal(1001)

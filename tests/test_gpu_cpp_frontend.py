@@ -27,3 +27,20 @@ def test_cpp_frontend_runs(tmp_path):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "PASS" in r.stdout
+
+
+MTL4_FIRST = ROOT / "oracle" / "_ref" / "mtl4_first_test"
+
+
+@pytest.mark.gpu
+def test_front_end_next_to_mtl4_headers_runs():
+    # tests/cpp/mtl4_first_test.cpp, built by oracle/Makefile against the
+    # MTL4 tree: the reference's own iteration and preconditioner templates
+    # with the GPU types; CPU (MTL4) and GPU (reference summation order) runs
+    # print identical cyclic_iteration output and give bitwise equal x
+    if not MTL4_FIRST.exists():
+        pytest.skip("oracle/_ref/mtl4_first_test not built (needs the MTL4 tree)")
+    r = subprocess.run([str(MTL4_FIRST)], capture_output=True, text=True, timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "PASS" in r.stdout and r.stdout.count("identical") == 6

@@ -114,3 +114,27 @@ def test_config1_cg_diagonal_default_order(ctx, golden):
     assert it.is_converged()
     assert iterations_ok("cg", it.iterations(), int(golden["c1_iters"])), it.iterations()
     assert np.linalg.norm(A.matvec(x) - b) <= 1.05e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("solver,pc,cycle,multi", [("cg", "diagonal", 10, 0), ("bicgstab", "ilu_0", 1, 0),
+                                                   ("bicgstab", "identity", 5, 1)])
+def test_cyclic_iteration_prints_the_reference_lines(rctx, golden, solver, pc, cycle, multi):
+    # itl::cyclic_iteration / noisy_iteration: the device-side termination
+    # tests are logged and replayed through finished(); in the reference
+    # summation order the printed lines (residuals at 6 digits, the final
+    # summary) are the reference build's, character for character
+    import io
+    from mtl4_b200 import itl, mtl
+    A = csr_from(golden, "lap32")
+    Ad = mtl.compressed2D.from_problem(A, rctx)
+    Pc = None if pc == "identity" else getattr(itl.pc, pc)(Ad, np.float64)
+    x = mtl.dense_vector(A.n_rows, np.float64, rctx)
+    bd = mtl.dense_vector(golden["lap32_b"], np.float64, rctx)
+    out = io.StringIO()
+    if cycle == 1:
+        it = itl.noisy_iteration(bd, 2000, 1e-8, out=out)
+    else:
+        it = itl.cyclic_iteration(bd, 2000, 1e-8, cycle=cycle, out=out)
+    it.set_multi_print(bool(multi))
+    getattr(itl, solver)(Ad, x, bd, Pc, it)
+    assert out.getvalue() == str(golden[f"lap32_{solver}_{pc}_cyclic{cycle}_{multi}"])
