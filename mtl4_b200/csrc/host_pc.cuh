@@ -76,6 +76,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     B = std::max(32, (B + 31) / 32 * 32);
     const int nch = (n + B - 1) / B;
     // rows of each chunk sorted by (level, flat order) and the largest wave
+    MTLG_TRACE(9153, "pc.chunk_order");
     std::vector<int> order;
     order.reserve(n);
     std::vector<int> cbeg(nch + 1, 0);
@@ -124,6 +125,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         cur = SegRec{int(wv.size()), 0, int(crow.size()), 0, int(ccol.size()), 0, 0, 0};
         open = true;
     };
+    MTLG_TRACE(9154, "pc.chunk_waves");
     std::vector<int> pos_of(n, -1);   // position of each row in this layout
     std::vector<int> cpbeg;            // first position of each chunk (and the end)
     for (int p = 0; p < nch; ++p) {
@@ -195,6 +197,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         T.max_slots = std::max(T.max_slots, nslot);
     }
     cpbeg.push_back(int(crow.size()));
+    MTLG_TRACE(9155, "pc.chunk_pushes");
     // pushes: a row of chunk p - 1 fills the first slot of chunk p that reads
     // it (when the two chunks run in neighbouring CTAs of a cluster); the
     // receivers fetch the other slots
@@ -247,6 +250,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     T.threads = NT;
     T.seg_rows = SR;
     T.seg_ents = SE;
+    MTLG_TRACE(9156, "pc.chunk_upload");
     MTLG_TRY(T.cseg.upload(c, cseg.data(), cseg.size()));
     MTLG_TRY(T.cxr.upload(c, cxr.data(), cxr.size()));
     MTLG_TRY(T.cext.upload(c, cext.data(), cext.size()));
@@ -606,7 +610,11 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
     T.n = n;
     T.lower = lower;
     std::vector<int> lev;
-    compute_levels(F, n, lower, lev, T.nlev);
+    {
+        MTLG_TRACE(9150, "pc.levels");
+        compute_levels(F, n, lower, lev, T.nlev);
+    }
+    MTLG_TRACE(9151, "pc.flat_layout");
     std::vector<int> cnt(T.nlev + 1, 0);
     for (int i = 0; i < n; ++i) cnt[lev[i]]++;
     // padded level starts
@@ -647,6 +655,7 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
     }
     std::vector<SweepTask> tasks(T.npad / kSweepRows);
     for (size_t t = 0; t < tasks.size(); ++t) tasks[t] = {0, int(t) * kSweepRows};
+    MTLG_TRACE(9152, "pc.flat_upload");
     MTLG_TRY(T.row_of.upload(c, T.h_row_of.data(), T.h_row_of.size()));
     MTLG_TRY(T.rp.upload(c, T.h_rp.data(), T.h_rp.size()));
     MTLG_TRY(T.ci.upload(c, T.h_ci.data(), T.h_ci.size()));
