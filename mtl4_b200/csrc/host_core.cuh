@@ -6,6 +6,8 @@
 #include "mmio.cuh"
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <memory>
 #include <mutex>
 
@@ -14,7 +16,7 @@ struct mtlg_ctx {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     size_t budget = 0;
-    size_t in_use = 0;
+    std::atomic<size_t> in_use{0};   // set-up may allocate from several host threads
     int64_t launches = 0;
     int sm_count = 148;
     int max_threads_per_sm = 2048, regs_per_sm = 65536;
@@ -71,7 +73,7 @@ inline int dalloc(mtlg_ctx* c, void** p, size_t bytes)
     if (bytes == 0) bytes = 16;
     const size_t b = round_up(bytes + 16, 256);
     if (c->budget && c->in_use + b > c->budget) {
-        set_error("device budget exceeded: %zu + %zu > %zu bytes", c->in_use, b, c->budget);
+        set_error("device budget exceeded: %zu + %zu > %zu bytes", c->in_use.load(), b, c->budget);
         return MTLG_ERR_OOM;
     }
     cudaError_t e = cudaMalloc(p, b);
@@ -90,7 +92,32 @@ inline void dfree(mtlg_ctx* c, void* p, size_t bytes)
     if (bytes == 0) bytes = 16;
     cudaFree(p);
     const size_t b = round_up(bytes + 16, 256);
-    c->in_use = c->in_use >= b ? c->in_use - b : 0;
+    size_t cur = c->in_use.load();
+    while (!c->in_use.compare_exchange_weak(cur, cur >= b ? cur - b : 0)) {
+    }
+}
+
+// Runs f(i) for i in [0, n) on up to `threads` host threads (0: the
+// hardware's), each taking the next index; f must be safe to run
+// concurrently for different i.
+template <typename F>
+inline void parallel_for(int n, F&& f, int threads = 0)
+{
+    int t = threads > 0 ? threads : int(std::thread::hardware_concurrency());
+    t = std::max(1, std::min(std::min(t, 32), n));
+    if (t <= 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    pool.reserve(size_t(t - 1));
+    auto work = [&]() {
+        for (int i = next++; i < n; i = next++) f(i);
+    };
+    for (int k = 1; k < t; ++k) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
 }
 
 // Typed owning device buffer.

@@ -75,64 +75,90 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     if (n == 0 || B <= 0 || kmax > kChunkMaxEntries) return MTLG_OK;
     B = std::max(32, (B + 31) / 32 * 32);
     const int nch = (n + B - 1) / B;
-    // rows of each chunk sorted by (level, flat order) and the largest wave
+    // rows of each chunk in (level, flat order): a counting sort by level per
+    // chunk (rows visited ascending for L, descending for U, so rows of one
+    // level keep the flat layout's order), and the largest wave
     MTLG_TRACE(9153, "pc.chunk_order");
-    std::vector<int> order;
-    order.reserve(n);
+    std::vector<int> order(size_t(n), 0);
     std::vector<int> cbeg(nch + 1, 0);
-    std::vector<std::pair<int, int>> key;
-    int maxw = 0;
     for (int p = 0; p < nch; ++p) {
         const int ch = lower ? p : nch - 1 - p;
-        const int r0 = ch * B, r1 = std::min(n, r0 + B);
-        key.clear();
-        for (int r = r0; r < r1; ++r) key.push_back({lev[r], lower ? r : -r});
-        std::sort(key.begin(), key.end());
-        int run = 0;
-        for (size_t q = 0; q < key.size(); ++q) {
-            run = (q > 0 && key[q].first == key[q - 1].first) ? run + 1 : 1;
-            maxw = std::max(maxw, run);
-            order.push_back(lower ? key[q].second : -key[q].second);
-        }
-        cbeg[p + 1] = int(order.size());
+        cbeg[p + 1] = cbeg[p] + (std::min(n, ch * B + B) - ch * B);
     }
+    std::vector<int> maxw_p(nch, 0);
+    parallel_for(nch, [&](int p) {
+        const int ch = lower ? p : nch - 1 - p;
+        const int r0 = ch * B, r1 = std::min(n, r0 + B);
+        int lo = lev[r0], hi = lev[r0];
+        for (int r = r0; r < r1; ++r) {
+            lo = std::min(lo, lev[r]);
+            hi = std::max(hi, lev[r]);
+        }
+        std::vector<int> cnt(size_t(hi - lo + 2), 0);
+        for (int r = r0; r < r1; ++r) cnt[size_t(lev[r] - lo + 1)]++;
+        int mw = 0;
+        for (size_t k = 1; k < cnt.size(); ++k) {
+            mw = std::max(mw, cnt[k]);
+            cnt[k] += cnt[k - 1];
+        }
+        int* out = order.data() + cbeg[p];
+        if (lower)
+            for (int r = r0; r < r1; ++r) out[cnt[size_t(lev[r] - lo)]++] = r;
+        else
+            for (int r = r1 - 1; r >= r0; --r) out[cnt[size_t(lev[r] - lo)]++] = r;
+        maxw_p[p] = mw;
+    });
+    int maxw = 0;
+    for (int p = 0; p < nch; ++p) maxw = std::max(maxw, maxw_p[p]);
     const int KB = entries_bucket(kmax);
     const int NT = std::min(chunk_wave_cap(KB, ssz), std::max(32, (maxw + 31) / 32 * 32));
     // segment capacity: a multiple of 32 rows, so every staged array (and
     // every staging buffer) starts 16-byte aligned in shared memory
     const int SR = std::max(NT, (1024 / KB + 31) / 32 * 32);
     const int SE = SR * KB;
-    std::vector<int> cseg(1, 0), cxr(1, 0), cext, crow, ccol, csrc, cmul;
-    std::vector<unsigned> wv;
-    std::vector<SegRec> segs;
-    SegRec cur{};
-    bool open = false;
-    auto close_seg = [&]() {
-        if (!open) return;
-        cur.np = int(crow.size()) - cur.p0;
-        cur.ne = int(ccol.size()) - cur.e0;
-        cur.nw = int(wv.size()) - cur.w0;
-        segs.push_back(cur);
-        open = false;
-    };
-    auto open_seg = [&]() {
-        wv.resize(round4(int(wv.size())), 0u);
-        crow.resize(round4(int(crow.size())), -1);
-        const int e = round4(int(ccol.size()));
-        ccol.resize(e, -1);
-        csrc.resize(e, 0);
-        cmul.resize(e, -1);
-        cur = SegRec{int(wv.size()), 0, int(crow.size()), 0, int(ccol.size()), 0, 0, 0};
-        open = true;
-    };
+
+    // Each chunk's layout is built on its own (host threads), positions and
+    // entries counted from the chunk's start; rows of earlier chunks are
+    // kept as row ids (cext) or -(row + 2) (overflow codes) until every
+    // chunk's position is known.  A chunk's arrays start 4-aligned in the
+    // concatenation (its first segment opens 4-aligned).
     MTLG_TRACE(9154, "pc.chunk_waves");
-    std::vector<int> pos_of(n, -1);   // position of each row in this layout
-    std::vector<int> cpbeg;            // first position of each chunk (and the end)
-    for (int p = 0; p < nch; ++p) {
+    struct ChunkLocal {
+        std::vector<unsigned> wv;
+        std::vector<int> crow, ccol, csrc, cmul, cext;
+        std::vector<SegRec> segs;
+        int nslot = 0;
+    };
+    std::vector<ChunkLocal> loc(static_cast<size_t>(nch));
+    std::vector<int> lpos(size_t(n), -1);   // position of each row inside its chunk
+    parallel_for(nch, [&](int p) {
+        ChunkLocal& L = loc[size_t(p)];
+        std::vector<unsigned>& wv = L.wv;
+        std::vector<int>&crow = L.crow, &ccol = L.ccol, &csrc = L.csrc, &cmul = L.cmul, &cext = L.cext;
+        std::vector<SegRec>& segs = L.segs;
+        SegRec cur{};
+        bool open = false;
+        auto close_seg = [&]() {
+            if (!open) return;
+            cur.np = int(crow.size()) - cur.p0;
+            cur.ne = int(ccol.size()) - cur.e0;
+            cur.nw = int(wv.size()) - cur.w0;
+            segs.push_back(cur);
+            open = false;
+        };
+        auto open_seg = [&]() {
+            wv.resize(round4(int(wv.size())), 0u);
+            crow.resize(round4(int(crow.size())), -1);
+            const int e = round4(int(ccol.size()));
+            ccol.resize(e, -1);
+            csrc.resize(e, 0);
+            cmul.resize(e, -1);
+            cur = SegRec{int(wv.size()), 0, int(crow.size()), 0, int(ccol.size()), 0, 0, 0};
+            open = true;
+        };
         const int ch = lower ? p : nch - 1 - p;
         const int r0 = ch * B, r1 = std::min(n, r0 + B);
         int nslot = 0;
-        cpbeg.push_back(int(crow.size()));
         for (int q = cbeg[p]; q < cbeg[p + 1];) {
             int qe = q + 1;
             while (qe < cbeg[p + 1] && qe - q < NT && lev[order[qe]] == lev[order[q]]) ++qe;
@@ -159,7 +185,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
             bool ovf = false;
             const size_t ent = ccol.size();
             for (int j = q; j < qe; ++j) {
-                pos_of[order[j]] = int(crow.size());
+                lpos[order[j]] = int(crow.size());
                 crow.push_back(order[j]);
             }
             ccol.resize(ent + size_t(K) * nw, B);     // padding: the zero cell, value 0
@@ -174,11 +200,11 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
                     if (col >= r0 && col < r1) {
                         code = col - r0;                 // row of this chunk
                     } else if (nslot < B) {
-                        cext.push_back(pos_of[col]);     // earlier chunk: receive slot
+                        cext.push_back(col);             // earlier chunk: receive slot (row id for now)
                         code = B + kSlotBase + nslot;
                         ++nslot;
                     } else {
-                        code = -(pos_of[col] + 2);       // earlier chunk beyond the slots: polled directly
+                        code = -(col + 2);               // earlier chunk beyond the slots (row id for now)
                         ovf = true;
                     }
                     ccol[e] = code;
@@ -191,12 +217,57 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         }
         close_seg();
         while (cext.size() % 4) cext.push_back(-1);
-        nslot = round4(nslot);
-        cseg.push_back(int(segs.size()));
-        cxr.push_back(int(cext.size()));
-        T.max_slots = std::max(T.max_slots, nslot);
+        L.nslot = round4(nslot);
+    });
+    // concatenation: chunk bases, then the arrays with row ids turned into
+    // positions (every earlier chunk's position is known now)
+    std::vector<size_t> bw(nch), bp(nch), be(nch), bx(nch), bs(nch);
+    size_t sw = 0, sp = 0, se = 0, sx = 0, ss = 0;
+    std::vector<int> cpbeg(size_t(nch) + 1, 0);   // first position of each chunk (and the end)
+    for (int p = 0; p < nch; ++p) {
+        const ChunkLocal& L = loc[size_t(p)];
+        sw = size_t(round4(int(sw)));
+        sp = size_t(round4(int(sp)));
+        se = size_t(round4(int(se)));
+        bw[p] = sw; bp[p] = sp; be[p] = se; bx[p] = sx; bs[p] = ss;
+        cpbeg[p] = int(sp);
+        sw += L.wv.size(); sp += L.crow.size(); se += L.ccol.size(); sx += L.cext.size(); ss += L.segs.size();
+        T.max_slots = std::max(T.max_slots, L.nslot);
     }
-    cpbeg.push_back(int(crow.size()));
+    cpbeg[nch] = int(sp);
+    std::vector<int> cseg(size_t(nch) + 1, 0), cxr(size_t(nch) + 1, 0);
+    for (int p = 0; p < nch; ++p) {
+        cseg[p + 1] = int(bs[p] + loc[size_t(p)].segs.size());
+        cxr[p + 1] = int(bx[p] + loc[size_t(p)].cext.size());
+    }
+    std::vector<unsigned> wv(sw, 0u);
+    std::vector<int> crow(sp, -1), ccol(se, -1), csrc(se, 0), cmul(se, -1), cext(sx, -1);
+    std::vector<SegRec> segs(ss);
+    auto pos_of = [&](int row) {
+        const int ch = row / B;
+        const int p = lower ? ch : nch - 1 - ch;
+        return int(bp[p]) + lpos[row];
+    };
+    parallel_for(nch, [&](int p) {
+        const ChunkLocal& L = loc[size_t(p)];
+        std::copy(L.wv.begin(), L.wv.end(), wv.begin() + bw[p]);
+        std::copy(L.crow.begin(), L.crow.end(), crow.begin() + bp[p]);
+        for (size_t k = 0; k < L.ccol.size(); ++k) {
+            const int v = L.ccol[k];
+            ccol[be[p] + k] = v <= -2 ? -(pos_of(-v - 2) + 2) : v;
+        }
+        std::copy(L.csrc.begin(), L.csrc.end(), csrc.begin() + be[p]);
+        std::copy(L.cmul.begin(), L.cmul.end(), cmul.begin() + be[p]);
+        for (size_t k = 0; k < L.cext.size(); ++k) cext[bx[p] + k] = L.cext[k] >= 0 ? pos_of(L.cext[k]) : -1;
+        for (size_t k = 0; k < L.segs.size(); ++k) {
+            SegRec g = L.segs[k];
+            g.w0 += int(bw[p]);
+            g.p0 += int(bp[p]);
+            g.e0 += int(be[p]);
+            segs[bs[p] + k] = g;
+        }
+    });
+    loc.clear();
     MTLG_TRACE(9155, "pc.chunk_pushes");
     // pushes: a row of chunk p - 1 fills the first slot of chunk p that reads
     // it (when the two chunks run in neighbouring CTAs of a cluster); the
@@ -643,16 +714,20 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
     T.h_ci.resize(T.nnz);
     T.h_src.resize(T.nnz);
     T.h_mul.resize(T.nnz);
-    for (int k = 0; k < T.npad; ++k) {
-        const int r = T.h_row_of[k];
-        if (r < 0) continue;
-        int o = T.h_rp[k];
-        for (int e = F.rp[r]; e < F.rp[r + 1]; ++e, ++o) {
-            T.h_ci[o] = F.col[e];
-            T.h_src[o] = F.src[e];
-            T.h_mul[o] = F.mul[e];
+    constexpr int kRowsPerBlock = 16384;
+    parallel_for((T.npad + kRowsPerBlock - 1) / kRowsPerBlock, [&](int blk) {
+        const int k1 = std::min(T.npad, (blk + 1) * kRowsPerBlock);
+        for (int k = blk * kRowsPerBlock; k < k1; ++k) {
+            const int r = T.h_row_of[k];
+            if (r < 0) continue;
+            int o = T.h_rp[k];
+            for (int e = F.rp[r]; e < F.rp[r + 1]; ++e, ++o) {
+                T.h_ci[o] = F.col[e];
+                T.h_src[o] = F.src[e];
+                T.h_mul[o] = F.mul[e];
+            }
         }
-    }
+    });
     std::vector<SweepTask> tasks(T.npad / kSweepRows);
     for (size_t t = 0; t < tasks.size(); ++t) tasks[t] = {0, int(t) * kSweepRows};
     MTLG_TRACE(9152, "pc.flat_upload");
@@ -840,6 +915,12 @@ inline int pc_build(mtlg_pc* P)
     if (P->kind == MTLG_PC_ILU0) {
         // L = strict_lower(LU) (unit diagonal), U = upper(LU) with the
         // inverted diagonal first (ilu_0.hpp:79-81, ilu.hpp:84-91)
+        const size_t off = size_t(std::max<int64_t>(0, A->nnz - n));
+        for (RowLists* R : {&Lr, &Ur}) {
+            R->col.reserve(off / 2 + 16);
+            R->src.reserve(off / 2 + 16);
+            R->mul.reserve(off / 2 + 16);
+        }
         for (int i = 0; i < n; ++i) {
             for (int64_t e = rp[i]; e < rp[i + 1]; ++e) {
                 if (ci[e] < i) { Lr.col.push_back(ci[e]); Lr.src.push_back(int(e)); Lr.mul.push_back(-1); }
@@ -878,12 +959,27 @@ inline int pc_build(mtlg_pc* P)
     }
     const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
     {
-        MTLG_TRACE(9102, "pc.schedule_L");
-        MTLG_TRY(build_tri(c, Lr, n, true, P->L, B, int(P->ssize())));
-    }
-    {
-        MTLG_TRACE(9103, "pc.schedule_U");
-        MTLG_TRY(build_tri(c, Ur, n, false, P->U, B, int(P->ssize())));
+        // the two factors' schedules are independent: U on a second host thread
+        MTLG_TRACE(9102, "pc.schedule");
+        int su = MTLG_OK;
+        std::string eu;
+        std::thread tu([&]() {
+            cudaSetDevice(c->device);   // the thread's uploads go to the context's device
+            MTLG_TRACE(9103, "pc.schedule_U");
+            su = build_tri(c, Ur, n, false, P->U, B, int(P->ssize()));
+            if (su != MTLG_OK) eu = last_error();
+        });
+        int sl = MTLG_OK;
+        {
+            MTLG_TRACE(9105, "pc.schedule_L");
+            sl = build_tri(c, Lr, n, true, P->L, B, int(P->ssize()));
+        }
+        tu.join();
+        if (sl != MTLG_OK) return sl;
+        if (su != MTLG_OK) {
+            set_error("%s", eu.c_str());
+            return su;
+        }
     }
     MTLG_TRY(pc_setup_single_set(P));
     MTLG_TRACE(9104, "pc.factor_and_fill");

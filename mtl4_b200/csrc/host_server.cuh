@@ -109,12 +109,19 @@ inline int admission_decision(size_t need, size_t held, size_t budget, size_t fr
 }
 
 // Free device memory and the reserve kept out of admission (default: the
-// larger of 1 GiB and 2% of the device).
-inline int free_memory(mtlg_ctx* c, size_t& free_bytes, size_t& reserve)
+// larger of 1 GiB and 2% of the device).  The "admission_free_bytes" stand-in
+// is the free memory before this server's own requests, so the bytes it holds
+// come off it as they do off cudaMemGetInfo's figure.
+inline int free_memory(mtlg_ctx* c, size_t held, size_t& free_bytes, size_t& reserve)
 {
     size_t fr = 0, total = 0;
     MTLG_CUDA(cudaMemGetInfo(&fr, &total));
-    free_bytes = c->admission_free_bytes > 0 ? size_t(c->admission_free_bytes) : fr;
+    if (c->admission_free_bytes > 0) {
+        const size_t f = size_t(c->admission_free_bytes);
+        free_bytes = f > held ? f - held : 0;
+    } else {
+        free_bytes = fr;
+    }
     reserve = c->admission_reserve_bytes >= 0 ? size_t(c->admission_reserve_bytes)
                                               : std::max<size_t>(size_t(1) << 30, total / 50);
     return MTLG_OK;
@@ -362,7 +369,7 @@ int mtlg_server_submit(mtlg_server* S, int64_t n, int64_t nnz, const int64_t* ro
     S->stats.submitted++;
     const size_t est = srv_estimate(n, nnz, S->refine);
     size_t fr = 0, reserve = 0;
-    if (!S->o.hbm_budget) MTLG_TRY(free_memory(S->ctx, fr, reserve));
+    if (!S->o.hbm_budget) MTLG_TRY(free_memory(S->ctx, S->bytes_held, fr, reserve));
     if (admission_decision(est, S->bytes_held, S->o.hbm_budget, fr, reserve) < 0) {
         S->stats.rejected++;
         if (S->o.hbm_budget) set_error("request needs ~%zu bytes, the server budget is %zu", est, S->o.hbm_budget);
@@ -459,7 +466,7 @@ int mtlg_server_step(mtlg_server* S)
         for (int s = 0; s < E.ss.S; ++s) if (E.slot_req[s] < 0) { slot = s; break; }
         if (slot < 0) break;
         size_t fr = 0, reserve = 0;
-        if (!S->o.hbm_budget) MTLG_TRY(free_memory(c, fr, reserve));
+        if (!S->o.hbm_budget) MTLG_TRY(free_memory(c, S->bytes_held, fr, reserve));
         const int adm = admission_decision(R.est, S->bytes_held, S->o.hbm_budget, fr, reserve);
         if (adm == 0) break;   // waits for active requests to retire
         S->queue.pop_front();

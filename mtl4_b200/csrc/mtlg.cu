@@ -477,7 +477,7 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     return MTLG_OK;
 }
 int64_t mtlg_ctx_kernel_launches(mtlg_ctx* c) { return c ? c->launches : 0; }
-size_t mtlg_ctx_bytes_in_use(mtlg_ctx* c) { return c ? c->in_use : 0; }
+size_t mtlg_ctx_bytes_in_use(mtlg_ctx* c) { return c ? c->in_use.load() : size_t(0); }
 
 // ------------------------------------------------------------------ CSR
 int mtlg_csr_create(mtlg_ctx* c, int64_t n_rows, int64_t n_cols, int64_t nnz, const int64_t* row_ptr,
