@@ -83,6 +83,8 @@ typedef struct mtlg_csr mtlg_csr;
 typedef struct mtlg_vec mtlg_vec;
 typedef struct mtlg_pc mtlg_pc;
 typedef struct mtlg_batch mtlg_batch;
+typedef struct mtlg_ell mtlg_ell;
+typedef struct mtlg_banded mtlg_banded;
 typedef struct mtlg_server mtlg_server;
 
 /* basic_iteration<double>(r0 or norm, max_iter, rtol, atol).  norm_r0 < 0
@@ -220,6 +222,32 @@ int mtlg_mm_read_host(const char* path, int64_t* n_rows, int64_t* n_cols, int64_
 int mtlg_csr_update_values(mtlg_csr* A, const void* val, mtlg_dtype val_dtype);
 /* SpMV tiling statistics: tiles by kind (0 stream, 1 long row, 2 unused). */
 int mtlg_csr_plan_info(const mtlg_csr* A, int64_t* tiles_by_kind3, int* max_row_len);
+
+/* ---- ELL and sparse_banded matrices ------------------------------------------ */
+/* mtl::mat::ell_matrix (boost/numeric/mtl/matrix/ell_matrix.hpp:31-170) in its
+ * own layout: entry j of row r at k = r + j * stride (stride >= n_rows; the
+ * reference rounds n_rows up to 32), `slots` entries per row, short rows
+ * padded with value 0 (the reference repeats the row's last column there).
+ * minor[slots * stride], data likewise (val_dtype).  y (=|+=|-=) E x sums each
+ * row's slots in order with rounded products, as the reference build does
+ * (operation/mat_vec_mult.hpp:686-700): FP64 bitwise the reference's. */
+int mtlg_ell_create(mtlg_ctx* ctx, int64_t n_rows, int64_t n_cols, int64_t slots, int64_t stride,
+                    const int64_t* minor, const void* data, mtlg_dtype val_dtype, mtlg_ell** out);
+int mtlg_ell_destroy(mtlg_ell* E);
+int mtlg_ell_spmv(mtlg_ctx* ctx, mtlg_ell* E, const mtlg_vec* x, mtlg_vec* y, int assign);
+/* mtl::mat::sparse_banded (matrix/sparse_banded.hpp:38-160): nbands strictly
+ * increasing diagonal offsets (column - row) and the values row by row, one
+ * per band (data[r * nbands + b]; entries outside the matrix are ignored).
+ * y (=|+=|-=) S x sums each row's bands inside the matrix in increasing order
+ * with the reference build's roundings (operation/mat_vec_mult.hpp:704-803:
+ * rows in 4-row blocks add rounded products in pairs and fuse an odd last
+ * band, other rows with >= 4 bands in fours with the rest fused, shorter ones
+ * round every product): FP64 bitwise the reference's.  Rows with no band
+ * inside the matrix get 0 for '=' and are left alone by '+=' / '-='. */
+int mtlg_banded_create(mtlg_ctx* ctx, int64_t n_rows, int64_t n_cols, int64_t nbands, const int64_t* bands,
+                       const void* data, mtlg_dtype val_dtype, mtlg_banded** out);
+int mtlg_banded_destroy(mtlg_banded* S);
+int mtlg_banded_spmv(mtlg_ctx* ctx, mtlg_banded* S, const mtlg_vec* x, mtlg_vec* y, int assign);
 
 /* ---- dense vectors (dense_vector) ----------------------------------------- */
 int mtlg_vec_create(mtlg_ctx* ctx, int64_t n, mtlg_dtype dtype, mtlg_vec** out);   /* zero-filled */

@@ -122,6 +122,12 @@ SIGNATURES = {
     "mtlg_batch_size": (C.c_int, [VP]),
     "mtlg_partition_systems": (C.c_int, [C.c_int64, VP, C.c_int, VP, VP]),
     "mtlg_trace_enable": (C.c_int, [C.c_int]),
+    "mtlg_ell_create": (C.c_int, [VP, C.c_int64, C.c_int64, C.c_int64, C.c_int64, VP, VP, C.c_int, C.POINTER(VP)]),
+    "mtlg_ell_destroy": (C.c_int, [VP]),
+    "mtlg_ell_spmv": (C.c_int, [VP, VP, VP, VP, C.c_int]),
+    "mtlg_banded_create": (C.c_int, [VP, C.c_int64, C.c_int64, C.c_int64, VP, VP, C.c_int, C.POINTER(VP)]),
+    "mtlg_banded_destroy": (C.c_int, [VP]),
+    "mtlg_banded_spmv": (C.c_int, [VP, VP, VP, VP, C.c_int]),
     "mtlg_ctx_set_residual_log": (C.c_int, [VP, C.c_int]),
     "mtlg_ctx_residual_log": (C.c_int, [VP, VP, C.c_int, C.POINTER(C.c_int)]),
     "mtlg_server_admission": (C.c_int, [C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t]),

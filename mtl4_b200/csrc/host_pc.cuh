@@ -272,24 +272,29 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     // pushes: a row of chunk p - 1 fills the first slot of chunk p that reads
     // it (when the two chunks run in neighbouring CTAs of a cluster); the
     // receivers fetch the other slots
+    // (chunk p writes only positions of chunk p - 1: chunks run in parallel)
     std::vector<int> cpush(crow.size(), -1);
     std::vector<char> pushed(cext.size(), 0);
-    for (int p = 1; p < nch; ++p)
+    parallel_for(nch - 1, [&](int pm) {
+        const int p = pm + 1;
         for (int e = cxr[p]; e < cxr[p + 1]; ++e) {
             const int x = cext[e];
             if (x < cpbeg[p - 1] || x >= cpbeg[p] || cpush[x] >= 0) continue;
             cpush[x] = e - cxr[p];
             pushed[e] = 1;
         }
-    std::vector<int> cqpull(cext.size() / 4 + 1, 0);
-    for (size_t q = 0; q < cext.size() / 4; ++q)
-        for (int j = 0; j < 4; ++j)
-            if (cext[4 * q + j] >= 0 && !pushed[4 * q + j]) cqpull[q] |= 1 << j;
+    });
+    const int nq = int(cext.size() / 4);
+    constexpr int kQuadBlock = 65536;
+    std::vector<int> cqpull(size_t(nq) + 1, 0);
     // receive quads (slots 4q .. 4q+3): {first position, mask of used slots};
     // first position -1 where the used slots are not four consecutive
     // positions starting 4-aligned (fetched one by one)
-    std::vector<int2> cquad(cext.size() / 4 + 1, make_int2(-1, 0));
-    for (size_t q = 0; q < cext.size() / 4; ++q) {
+    std::vector<int2> cquad(size_t(nq) + 1, make_int2(-1, 0));
+    parallel_for((nq + kQuadBlock - 1) / kQuadBlock, [&](int blk) {
+    for (int q = blk * kQuadBlock; q < std::min(nq, (blk + 1) * kQuadBlock); ++q) {
+        for (int j = 0; j < 4; ++j)
+            if (cext[4 * q + j] >= 0 && !pushed[4 * q + j]) cqpull[q] |= 1 << j;
         int mask = 0, p = -2;
         bool vec = true;
         for (int j = 0; j < 4; ++j) {
@@ -302,6 +307,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         if (p < 0 || p % 4) vec = false;
         cquad[q] = make_int2(vec && mask ? p : -1, mask);
     }
+    });
     // tails: a staged copy rounds each array's segment up to 16 bytes
     wv.resize(round4(int(wv.size())) + 4, 0u);
     crow.resize(round4(int(crow.size())) + 4, -1);
@@ -915,20 +921,31 @@ inline int pc_build(mtlg_pc* P)
     if (P->kind == MTLG_PC_ILU0) {
         // L = strict_lower(LU) (unit diagonal), U = upper(LU) with the
         // inverted diagonal first (ilu_0.hpp:79-81, ilu.hpp:84-91)
-        const size_t off = size_t(std::max<int64_t>(0, A->nnz - n));
-        for (RowLists* R : {&Lr, &Ur}) {
-            R->col.reserve(off / 2 + 16);
-            R->src.reserve(off / 2 + 16);
-            R->mul.reserve(off / 2 + 16);
-        }
+        // row counts, offsets, then the entries (rows in parallel)
         for (int i = 0; i < n; ++i) {
+            int nl = 0, nu = 0;
             for (int64_t e = rp[i]; e < rp[i + 1]; ++e) {
-                if (ci[e] < i) { Lr.col.push_back(ci[e]); Lr.src.push_back(int(e)); Lr.mul.push_back(-1); }
-                else if (ci[e] > i) { Ur.col.push_back(ci[e]); Ur.src.push_back(int(e)); Ur.mul.push_back(-1); }
+                nl += ci[e] < i;
+                nu += ci[e] > i;
             }
-            Lr.rp[i + 1] = int(Lr.col.size());
-            Ur.rp[i + 1] = int(Ur.col.size());
+            Lr.rp[i + 1] = Lr.rp[i] + nl;
+            Ur.rp[i + 1] = Ur.rp[i] + nu;
         }
+        for (RowLists* R : {&Lr, &Ur}) {
+            R->col.resize(size_t(R->rp[n]));
+            R->src.resize(size_t(R->rp[n]));
+            R->mul.assign(size_t(R->rp[n]), -1);
+        }
+        constexpr int kRowBlock = 16384;
+        parallel_for((n + kRowBlock - 1) / kRowBlock, [&](int blk) {
+            for (int i = blk * kRowBlock; i < std::min(n, (blk + 1) * kRowBlock); ++i) {
+                int ol = Lr.rp[i], ou = Ur.rp[i];
+                for (int64_t e = rp[i]; e < rp[i + 1]; ++e) {
+                    if (ci[e] < i) { Lr.col[ol] = ci[e]; Lr.src[ol++] = int(e); }
+                    else if (ci[e] > i) { Ur.col[ou] = ci[e]; Ur.src[ou++] = int(e); }
+                }
+            }
+        });
     } else {
         // U = upper(A) scaled by its row's inverse pivot; L = trans(U) with
         // the diagonal last (ic_0.hpp:47-57, 80-87)

@@ -1205,3 +1205,4 @@ int mtlg_refine_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* P, mtlg_vec
 
 #include "host_gmres.cuh"
 #include "host_batch.cuh"
+#include "formats.cuh"

@@ -239,9 +239,110 @@ class dense_vector:
 _ASSIGN = {"=": _lib.ASSIGN, "+=": _lib.PLUS, "-=": _lib.MINUS}
 
 
-def mult(A: compressed2D, x: dense_vector, y: dense_vector, assign: str = "="):
-    """y = A x, y += A x or y -= A x."""
-    check(A.ctx._L.mtlg_spmv(A.ctx.h, A.h, x.h, y.h, _ASSIGN[assign]), "mult")
+def ell_layout(A):
+    """MTL4's ELL form of a host CSR (matrix/ell_matrix.hpp:127-170): stride =
+    rows rounded up to 32, slots = the longest row, entry j of row r at
+    r + j * stride; short rows padded with value 0 at their last column (0
+    for an empty row).  Returns (stride, slots, minor, data)."""
+    n = A.n_rows
+    lens = np.diff(A.row_ptr)
+    slots = int(lens.max()) if n else 0
+    stride = (n + 31) // 32 * 32
+    minor = np.zeros(slots * stride, np.int64)
+    data = np.zeros(slots * stride)
+    for j in range(slots):
+        has = lens > j
+        k = j * stride + np.arange(n)
+        e = A.row_ptr[:-1] + np.minimum(j, np.maximum(lens - 1, 0))
+        last = np.where(lens > 0, A.col[np.minimum(e, max(A.nnz - 1, 0))] if A.nnz else 0, 0)
+        minor[k] = last
+        data[k] = np.where(has, A.val[np.minimum(A.row_ptr[:-1] + j, max(A.nnz - 1, 0))] if A.nnz else 0.0, 0.0)
+    return stride, slots, minor, data
+
+
+def banded_layout(A):
+    """MTL4's sparse_banded form of a host CSR: the distinct offsets col - row
+    in increasing order and one value per band and row, row by row (0 where a
+    row has no entry on a band).  Returns (bands, data)."""
+    rows = np.repeat(np.arange(A.n_rows), np.diff(A.row_ptr))
+    off = A.col.astype(np.int64) - rows
+    bands = np.unique(off)
+    data = np.zeros(A.n_rows * bands.size)
+    data[rows * bands.size + np.searchsorted(bands, off)] = A.val
+    return bands, data
+
+
+class ell_matrix:
+    """mtl::mat::ell_matrix on the device (its own layout; see ell_layout)."""
+
+    def __init__(self, n_rows, n_cols, slots, stride, minor, data, ctx: context | None = None):
+        self.ctx = ctx or default_context()
+        mi = np.ascontiguousarray(minor, np.int64)
+        v = np.ascontiguousarray(data)
+        if v.dtype not in _DT:
+            v = v.astype(np.float64)
+        h = C.c_void_p()
+        check(self.ctx._L.mtlg_ell_create(self.ctx.h, int(n_rows), int(n_cols), int(slots), int(stride), _ptr(mi),
+                                          _ptr(v), _DT[v.dtype], C.byref(h)), "ell_matrix")
+        self.h = h
+        self.shape = (int(n_rows), int(n_cols))
+
+    @classmethod
+    def from_csr(cls, A, ctx: context | None = None) -> "ell_matrix":
+        st, sl, mi, da = ell_layout(A)
+        return cls(A.n_rows, A.n_cols, sl, st, mi, da, ctx)
+
+    def __mul__(self, v: "dense_vector") -> "_MatVec":
+        return _MatVec(self, v)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.ctx.h:
+                self.ctx._L.mtlg_ell_destroy(self.h)
+        except Exception:
+            pass
+
+
+class sparse_banded:
+    """mtl::mat::sparse_banded on the device (values kept band by band)."""
+
+    def __init__(self, n_rows, n_cols, bands, data, ctx: context | None = None):
+        self.ctx = ctx or default_context()
+        b = np.ascontiguousarray(bands, np.int64)
+        v = np.ascontiguousarray(data)
+        if v.dtype not in _DT:
+            v = v.astype(np.float64)
+        h = C.c_void_p()
+        check(self.ctx._L.mtlg_banded_create(self.ctx.h, int(n_rows), int(n_cols), b.size, _ptr(b), _ptr(v),
+                                             _DT[v.dtype], C.byref(h)), "sparse_banded")
+        self.h = h
+        self.shape = (int(n_rows), int(n_cols))
+
+    @classmethod
+    def from_csr(cls, A, ctx: context | None = None) -> "sparse_banded":
+        bands, data = banded_layout(A)
+        return cls(A.n_rows, A.n_cols, bands, data, ctx)
+
+    def __mul__(self, v: "dense_vector") -> "_MatVec":
+        return _MatVec(self, v)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.ctx.h:
+                self.ctx._L.mtlg_banded_destroy(self.h)
+        except Exception:
+            pass
+
+
+def mult(A, x: dense_vector, y: dense_vector, assign: str = "="):
+    """y = A x, y += A x or y -= A x (A: compressed2D, ell_matrix or
+    sparse_banded)."""
+    if isinstance(A, ell_matrix):
+        check(A.ctx._L.mtlg_ell_spmv(A.ctx.h, A.h, x.h, y.h, _ASSIGN[assign]), "mult")
+    elif isinstance(A, sparse_banded):
+        check(A.ctx._L.mtlg_banded_spmv(A.ctx.h, A.h, x.h, y.h, _ASSIGN[assign]), "mult")
+    else:
+        check(A.ctx._L.mtlg_spmv(A.ctx.h, A.h, x.h, y.h, _ASSIGN[assign]), "mult")
 
 
 def mult_dot(A: compressed2D, p: dense_vector, q: dense_vector) -> float:

@@ -485,6 +485,90 @@ void mtlo_spmv(int64_t n, const int64_t* rp, const int32_t* ci, const double* va
     spmv(Csr{n, rp, ci}, val, x, y, assign);
 }
 
+// w (=|+=|-=) E v for MTL4's ELL layout (operation/mat_vec_mult.hpp:686-700):
+// per row the slots in order, entry (r, i) at k = r + i * stride, padding
+// included (value 0); the reference build adds rounded products throughout.
+void mtlo_ell_spmv(int64_t n, int64_t stride, int64_t slots, const int64_t* minor, const double* data,
+                   const double* x, double* y, int assign)
+{
+    for (int64_t r = 0; r < n; ++r) {
+        double s = 0.0;
+        for (int64_t i = 0, k = r; i < slots; ++i, k += stride) s = s + data[k] * x[minor[k]];
+        if (assign == 0) y[r] = s;
+        else if (assign == 1) y[r] += s;
+        else y[r] -= s;
+    }
+}
+
+// Rows of sparse_banded's product loop (operation/mat_vec_mult.hpp:704-803)
+// run in 4-row blocks or singly: the row range is cut where a band starts or
+// ends; in each piece [from, to) rows from .. from + 4 floor((to-from)/4) go
+// in blocks, the rest singly.  flags[r] = 1 for a blocked row; rows outside
+// every band's range get 2 (no active band).
+void mtlo_banded_row_kinds(int64_t nr, int64_t nc, int64_t nb, const int64_t* bands, unsigned char* flags)
+{
+    for (int64_t r = 0; r < nr; ++r) flags[r] = 2;
+    if (nb == 0) return;
+    std::vector<int64_t> begin_rows(nb), end_rows(nb);
+    for (int64_t b = 0; b < nb; ++b) {
+        begin_rows[b] = std::max<int64_t>(0, -bands[b]);
+        end_rows[b] = std::min<int64_t>(nr, nc - bands[b]);
+    }
+    int64_t bp = 0, ep = nb - 1;
+    while (bp < nb && begin_rows[bp] > 0) bp++;
+    if (bp == nb) --bp;
+    int64_t from = begin_rows[bp];
+    while (bp > 0 && begin_rows[bp - 1] == from) bp--;
+    for (bool active = true; active;) {
+        const int64_t to = bp > 0 && begin_rows[bp - 1] <= end_rows[ep] ? begin_rows[bp - 1] : end_rows[ep];
+        const int64_t blocked_to = ((to - from) & -4) + from;
+        for (int64_t r = from; r < to; ++r) flags[r] = r < blocked_to ? 1 : 0;
+        if (bp > 0) {
+            if (begin_rows[bp - 1] == to) bp--;
+            if (end_rows[ep] == to) ep--;
+        } else {
+            if (end_rows[0] == to) active = false;
+            else ep--;
+        }
+        from = to;
+    }
+}
+
+// w (=|+=|-=) S v for MTL4's sparse_banded layout (values row by row, one
+// per band): per row the bands inside the matrix in increasing order; the
+// reference build adds rounded products in groups of 2 (blocked rows) or 4
+// (single rows of at least 4 bands; shorter single rows round every product)
+// and fuses the rest.  Rows with no band inside the matrix get
+// 0 for '=' and stay as they are for '+=' / '-='.
+void mtlo_banded_spmv(int64_t nr, int64_t nc, int64_t nb, const int64_t* bands, const double* data,
+                      const double* x, double* y, int assign)
+{
+    std::vector<unsigned char> kind(size_t(nr), 2);
+    mtlo_banded_row_kinds(nr, nc, nb, bands, kind.data());
+    for (int64_t r = 0; r < nr; ++r) {
+        if (kind[r] == 2) {
+            if (assign == 0) y[r] = 0.0;
+            continue;
+        }
+        int64_t lo = 0, hi = nb;
+        while (lo < nb && r + bands[lo] < 0) ++lo;
+        while (hi > lo && r + bands[hi - 1] >= nc) --hi;
+        // blocked rows: groups of 2, the odd last band fused; single rows:
+        // groups of 4 and the rest fused when the row has 4 bands or more,
+        // else every product rounded
+        const int64_t cnt = hi - lo;
+        const int64_t q = kind[r] == 1 ? lo + cnt / 2 * 2 : (cnt >= 4 ? lo + cnt / 4 * 4 : hi);
+        double s = 0.0;
+        for (int64_t b = lo; b < hi; ++b) {
+            const double a = data[r * nb + b], v = x[r + bands[b]];
+            s = b < q ? s + a * v : std::fma(a, v, s);
+        }
+        if (assign == 0) y[r] = s;
+        else if (assign == 1) y[r] += s;
+        else y[r] -= s;
+    }
+}
+
 void mtlo_spmv_f32(int64_t n, const int64_t* rp, const int32_t* ci, const float* val, const float* x, float* y,
                    int assign)
 {

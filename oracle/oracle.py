@@ -75,6 +75,10 @@ def ref_lib(omp: bool = False) -> C.CDLL:
         L.mtlref_refine_solve.argtypes = [VP, C.c_int, C.c_int, VP, VP, C.c_int, C.c_int, C.c_double, C.c_double,
                                           C.c_int, C.POINTER(RefResult)]
         L.mtlref_laplacian_setup.argtypes = [C.c_int, C.c_int, PI, VP, VP, VP]
+        L.mtlref_ell_export.argtypes = [VP, PI, PI, VP, VP]
+        L.mtlref_ell_spmv.argtypes = [VP, VP, VP, C.c_int]
+        L.mtlref_banded_export.argtypes = [VP, PI, VP, VP]
+        L.mtlref_banded_spmv.argtypes = [VP, VP, VP, C.c_int]
         L.mtlref_solve_cyclic.restype = C.c_int
         L.mtlref_solve_cyclic.argtypes = [VP, C.c_int, C.c_int, VP, VP, C.c_int, C.c_double, C.c_int, C.c_int,
                                           C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
@@ -93,6 +97,9 @@ def port_lib() -> C.CDLL:
         L.mtlo_spmv_f32.argtypes = [C.c_int64, VP, VP, VP, VP, VP, C.c_int]
         L.mtlo_dot.restype = C.c_double
         L.mtlo_dot.argtypes = [C.c_int64, VP, VP]
+        L.mtlo_ell_spmv.argtypes = [C.c_int64, C.c_int64, C.c_int64, VP, VP, VP, VP, C.c_int]
+        L.mtlo_banded_row_kinds.argtypes = [C.c_int64, C.c_int64, C.c_int64, VP, VP]
+        L.mtlo_banded_spmv.argtypes = [C.c_int64, C.c_int64, C.c_int64, VP, VP, VP, VP, C.c_int]
         L.mtlo_dot4.restype = C.c_double
         L.mtlo_dot4.argtypes = [C.c_int64, VP, VP]
         L.mtlo_norm4.restype = C.c_double
@@ -124,6 +131,34 @@ class RefMatrix:
         else:
             y = np.zeros(self.A.n_rows) if y is None else np.array(y, np.float64)
             self.L.mtlref_spmv(self.h, _p(x), _p(y), assign)
+        return y
+
+    def ell(self):
+        """(stride, slots, minor, data) of MTL4's ELL form of A."""
+        st, sl = C.c_int64(), C.c_int64()
+        self.L.mtlref_ell_export(self.h, C.byref(st), C.byref(sl), None, None)
+        mi = np.zeros(st.value * sl.value, np.int64)
+        da = np.zeros(st.value * sl.value)
+        self.L.mtlref_ell_export(self.h, C.byref(st), C.byref(sl), _p(mi), _p(da))
+        return st.value, sl.value, mi, da
+
+    def ell_spmv(self, x, assign=0, y=None):
+        y = np.zeros(self.A.n_rows) if y is None else np.array(y, np.float64)
+        self.L.mtlref_ell_spmv(self.h, _p(np.ascontiguousarray(x, np.float64)), _p(y), assign)
+        return y
+
+    def banded(self):
+        """(bands, data) of MTL4's sparse_banded form of A."""
+        nb = C.c_int64()
+        self.L.mtlref_banded_export(self.h, C.byref(nb), None, None)
+        bands = np.zeros(nb.value, np.int64)
+        data = np.zeros(self.A.n_rows * nb.value)
+        self.L.mtlref_banded_export(self.h, C.byref(nb), _p(bands), _p(data))
+        return bands, data
+
+    def banded_spmv(self, x, assign=0, y=None):
+        y = np.zeros(self.A.n_rows) if y is None else np.array(y, np.float64)
+        self.L.mtlref_banded_spmv(self.h, _p(np.ascontiguousarray(x, np.float64)), _p(y), assign)
         return y
 
     def spmv_timed(self, x, reps):
@@ -286,3 +321,21 @@ def ref_matrix_market(path):
     v = np.zeros(nz.value)
     L.mtlref_mm_read(p, C.byref(nr), C.byref(nc), C.byref(nz), _p(rp), _p(ci), _p(v))
     return 0, (nr.value, nc.value, rp, ci, v)
+
+
+def port_ell_spmv(n_rows, stride, slots, minor, data, x, assign=0, y=None):
+    L = port_lib()
+    y = np.zeros(n_rows) if y is None else np.array(y, np.float64)
+    mi = np.ascontiguousarray(minor, np.int64)
+    da = np.ascontiguousarray(data, np.float64)
+    L.mtlo_ell_spmv(n_rows, stride, slots, _p(mi), _p(da), _p(np.ascontiguousarray(x, np.float64)), _p(y), assign)
+    return y
+
+
+def port_banded_spmv(n_rows, n_cols, bands, data, x, assign=0, y=None):
+    L = port_lib()
+    y = np.zeros(n_rows) if y is None else np.array(y, np.float64)
+    b = np.ascontiguousarray(bands, np.int64)
+    da = np.ascontiguousarray(data, np.float64)
+    L.mtlo_banded_spmv(n_rows, n_cols, b.size, _p(b), _p(da), _p(np.ascontiguousarray(x, np.float64)), _p(y), assign)
+    return y

@@ -40,9 +40,14 @@ typedef mtl::compressed2D<float, para_t> fmat;
 typedef mtl::dense_vector<double> dvec;
 typedef mtl::dense_vector<float> fvec;
 
+typedef mtl::mat::ell_matrix<double> dell;
+typedef mtl::mat::sparse_banded<double> dband;
+
 struct RefCsr {
     std::unique_ptr<dmat> A;
     std::unique_ptr<fmat> Af;   // lazily built FP32 copy (values rounded once)
+    std::unique_ptr<dell> E;    // lazily built ELL copy (E = A)
+    std::unique_ptr<dband> S;   // lazily built sparse_banded copy (S = A)
     std::size_t n_rows = 0, n_cols = 0, nnz = 0;
 };
 
@@ -328,6 +333,70 @@ static int run_cyclic(int solver, const dmat& A, dvec& x, const dvec& b, const P
 }
 
 extern "C" {
+
+static dell& ell_copy(RefCsr* h)
+{
+    if (!h->E) {
+        h->E.reset(new dell(h->n_rows, h->n_cols));
+        *h->E = *h->A;
+    }
+    return *h->E;
+}
+
+static dband& band_copy(RefCsr* h)
+{
+    if (!h->S) {
+        h->S.reset(new dband(h->n_rows, h->n_cols));
+        *h->S = *h->A;
+    }
+    return *h->S;
+}
+
+/// The ELL form of A as MTL4 builds it (ell_matrix = compressed2D,
+/// matrix/ell_matrix.hpp:127-170): entry j of row i at k = i + j * stride,
+/// stride = n_rows rounded up to 32, slots = longest row; padding repeats the
+/// row's last column with value 0.  Null arrays: sizes only.
+void mtlref_ell_export(void* p, int64_t* stride, int64_t* slots, int64_t* minor, double* data)
+{
+    dell& E = ell_copy(static_cast<RefCsr*>(p));
+    *stride = int64_t(E.stride());
+    *slots = int64_t(E.slots());
+    const std::size_t m = E.stride() * E.slots();
+    if (minor)
+        for (std::size_t k = 0; k < m; ++k) minor[k] = int64_t(E.ref_minor()[k]);
+    if (data)
+        for (std::size_t k = 0; k < m; ++k) data[k] = E.ref_data()[k];
+}
+
+/// w (=|+=|-=) E * v (operation/mat_vec_mult.hpp:686-700)
+void mtlref_ell_spmv(void* p, const double* x, double* y, int assign)
+{
+    RefCsr* h = static_cast<RefCsr*>(p);
+    dvec vx(h->n_cols, const_cast<double*>(x)), vy(h->n_rows, y);
+    spmv_impl(ell_copy(h), vx, vy, assign);
+}
+
+/// The sparse_banded form of A (sparse_banded = compressed2D,
+/// matrix/sparse_banded.hpp:168-260): the diagonal offsets in increasing
+/// order and the values row by row, one per band (0 outside the matrix).
+void mtlref_banded_export(void* p, int64_t* nb, int64_t* bands, double* data)
+{
+    RefCsr* h = static_cast<RefCsr*>(p);
+    dband& S = band_copy(h);
+    *nb = int64_t(S.ref_bands().size());
+    if (bands)
+        for (std::size_t b = 0; b < S.ref_bands().size(); ++b) bands[b] = int64_t(S.ref_bands()[b]);
+    if (data)
+        for (std::size_t k = 0; k < h->n_rows * S.ref_bands().size(); ++k) data[k] = S.ref_data()[k];
+}
+
+/// w (=|+=|-=) S * v (operation/mat_vec_mult.hpp:704-803)
+void mtlref_banded_spmv(void* p, const double* x, double* y, int assign)
+{
+    RefCsr* h = static_cast<RefCsr*>(p);
+    dvec vx(h->n_cols, const_cast<double*>(x)), vy(h->n_rows, y);
+    spmv_impl(band_copy(h), vx, vy, assign);
+}
 
 /// FP64 CG (solver 0) or BiCGSTAB (1) with itl::cyclic_iteration<double>
 /// (itl/iteration/cyclic_iteration.hpp:22-95) printing into a string: the

@@ -72,6 +72,36 @@ def main():
                                      ("bicgstab", "identity", 5, 1)]:
         err, text = R.solve_cyclic(b, solver, pc, max_iter=2000, rtol=1e-8, cycle=cycle, multi_print=bool(multi))
         out[f"lap32_{solver}_{pc}_cyclic{cycle}_{multi}"] = np.array(text)
+    # ELL and sparse_banded forms (ell_matrix / sparse_banded = compressed2D)
+    # and their products on the 8^3 convection-diffusion operator and on a
+    # rectangular banded matrix with bands that end inside it
+    st, sl, mi, da = R3.ell()
+    out["cd8_ell_stride"], out["cd8_ell_slots"] = np.array(st), np.array(sl)
+    out["cd8_ell_minor"], out["cd8_ell_data"] = mi, da
+    out["cd8_ell_y"] = R3.ell_spmv(xc)
+    bands, bd = R3.banded()
+    out["cd8_band_bands"], out["cd8_band_data"] = bands, bd
+    out["cd8_band_y"] = R3.banded_spmv(xc)
+    rb = np.random.default_rng(15)
+    offs = [-37, -5, -2, 0, 3, 19, 60]
+    nr, nc = 203, 231
+    rows, cols = [], []
+    for o in offs:
+        r = np.arange(max(0, -o), min(nr, nc - o))
+        rows.append(r)
+        cols.append(r + o)
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    Bm = P._from_coo(nr, rows, cols, rb.standard_normal(rows.size))
+    Bm = P.CSR(nr, nc, Bm.row_ptr, Bm.col, Bm.val)
+    RB = O.RefMatrix(Bm)
+    out["rb_rp"], out["rb_ci"], out["rb_val"] = Bm.row_ptr, Bm.col, Bm.val
+    out["rb_x"] = rb.standard_normal(nc)
+    out["rb_y0"] = rb.standard_normal(nr)
+    bands, bd = RB.banded()
+    out["rb_bands"], out["rb_data"] = bands, bd
+    for a in (0, 1, 2):
+        out[f"rb_band_y{a}"] = RB.banded_spmv(out["rb_x"], a, out["rb_y0"])
+        out[f"rb_ell_y{a}"] = RB.ell_spmv(out["rb_x"], a, out["rb_y0"])
     # mtl::dot and mtl::two_norm (four strided partial sums) on general values
     out["dot_x"] = xq[:1001]
     out["dot_y"] = np.random.default_rng(14).standard_normal(1001)
