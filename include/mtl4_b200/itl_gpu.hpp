@@ -590,6 +590,69 @@ inline int gmres(const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& 
     return iter.error_code();
 }
 
+/// The reference's other Krylov bodies (itl/krylov/*.hpp), host-driven on
+/// device vectors (FP64): bicg, cgs and bicgstab_2 with one preconditioner,
+/// tfqmr and qmr with left and right ones, bicgstab_ell and idr_s with both
+/// and their ell / s.
+namespace gpu {
+template <typename T, typename Left, typename Right, typename Iteration>
+inline int run2(int solver, const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& x,
+                const mtl::gpu::dense_vector<T>& b, const Left* L, const Right* R, Iteration& iter, int param = 0)
+{
+    mtlg_iter_params p = params_of(iter, param);
+    mtlg_iter_result r;
+    const int s = mtlg_solve(A.ctx().get(), solver, A.get(), L ? L->get() : nullptr, R ? R->get() : nullptr, x.get(),
+                             b.get(), &p, &r);
+    take_result(iter, r);
+    mtl::gpu::check(s, "krylov");
+    return iter.error_code();
+}
+}  // namespace gpu
+
+template <typename T, typename PC, typename Iteration>
+inline int bicg(const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& x, const mtl::gpu::dense_vector<T>& b,
+                const PC& M, Iteration& iter)
+{
+    return gpu::run2(MTLG_BICG, A, x, b, &M, static_cast<const PC*>(nullptr), iter);
+}
+template <typename T, typename PC, typename Iteration>
+inline int cgs(const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& x, const mtl::gpu::dense_vector<T>& b,
+               const PC& M, Iteration& iter)
+{
+    return gpu::run2(MTLG_CGS, A, x, b, &M, static_cast<const PC*>(nullptr), iter);
+}
+template <typename T, typename PC, typename Iteration>
+inline int bicgstab_2(const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& x,
+                      const mtl::gpu::dense_vector<T>& b, const PC& L, Iteration& iter)
+{
+    return gpu::run2(MTLG_BICGSTAB_2, A, x, b, &L, static_cast<const PC*>(nullptr), iter);
+}
+template <typename T, typename Left, typename Right, typename Iteration>
+inline int tfqmr(const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& x, const mtl::gpu::dense_vector<T>& b,
+                 const Left& L, const Right& R, Iteration& iter)
+{
+    return gpu::run2(MTLG_TFQMR, A, x, b, &L, &R, iter);
+}
+template <typename T, typename Left, typename Right, typename Iteration>
+inline int qmr(const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& x, const mtl::gpu::dense_vector<T>& b,
+               Left& L, const Right& R, Iteration& iter)
+{
+    return gpu::run2(MTLG_QMR, A, x, b, &L, &R, iter);
+}
+template <typename T, typename Left, typename Right, typename Iteration>
+inline int bicgstab_ell(const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& x,
+                        const mtl::gpu::dense_vector<T>& b, const Left& L, const Right& R, Iteration& iter,
+                        std::size_t l)
+{
+    return gpu::run2(MTLG_BICGSTAB_ELL, A, x, b, &L, &R, iter, int(l));
+}
+template <typename T, typename Left, typename Right, typename Iteration>
+inline int idr_s(const mtl::gpu::compressed2D<T>& A, mtl::gpu::dense_vector<T>& x, const mtl::gpu::dense_vector<T>& b,
+                 const Left& L, const Right& R, Iteration& iter, std::size_t s)
+{
+    return gpu::run2(MTLG_IDR_S, A, x, b, &L, &R, iter, int(s));
+}
+
 /// FP64 iterative refinement around an FP32 inner CG / BiCGSTAB (no
 /// reference counterpart): x, b FP64; P an FP32-stored preconditioner of A.
 template <typename PC>

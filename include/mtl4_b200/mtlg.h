@@ -64,7 +64,17 @@ enum {
 typedef enum { MTLG_F64 = 0, MTLG_F32 = 1 } mtlg_dtype;
 typedef enum { MTLG_ASSIGN = 0, MTLG_PLUS = 1, MTLG_MINUS = 2 } mtlg_assign;
 typedef enum { MTLG_PC_IDENTITY = 0, MTLG_PC_DIAGONAL = 1, MTLG_PC_ILU0 = 2, MTLG_PC_IC0 = 3 } mtlg_pc_kind;
-typedef enum { MTLG_CG = 0, MTLG_BICGSTAB = 1, MTLG_GMRES = 2 } mtlg_solver;
+typedef enum {
+    MTLG_CG = 0, MTLG_BICGSTAB = 1, MTLG_GMRES = 2,
+    /* host-driven bodies on device vectors (itl/krylov/*.hpp) */
+    MTLG_BICG = 3,          /* itl::bicg (bicg.hpp:28)        adjoint(A), adjoint_solve(L)  */
+    MTLG_CGS = 4,           /* itl::cgs (cgs.hpp:28)                                         */
+    MTLG_TFQMR = 5,         /* itl::tfqmr (tfqmr.hpp:30)      left L, right R                */
+    MTLG_QMR = 6,           /* itl::qmr (qmr.hpp:31)          left L, right R, trans(A)      */
+    MTLG_BICGSTAB_2 = 7,    /* itl::bicgstab_2 (bicgstab_2.hpp:29)                          */
+    MTLG_BICGSTAB_ELL = 8,  /* itl::bicgstab_ell (bicgstab_ell.hpp:29)  ell = params->restart */
+    MTLG_IDR_S = 9          /* itl::idr_s (idr_s.hpp:31)      s = params->restart           */
+} mtlg_solver;
 
 /* Termination state of one solve; mirrors itl::basic_iteration. */
 enum {
@@ -320,6 +330,16 @@ int mtlg_solve(mtlg_ctx* ctx, int solver, mtlg_csr* A, mtlg_pc* pc_left, mtlg_pc
  * `pc` (storage FP32, factorized in FP64). */
 int mtlg_refine_solve(mtlg_ctx* ctx, int solver, mtlg_csr* A, mtlg_pc* pc, mtlg_vec* x, const mtlg_vec* b,
                       const mtlg_refine_params* params, mtlg_iter_result* result);
+
+/* ---- matrix-free 2D Poisson operator ------------------------------------------ */
+/* mtl::mat::poisson2D_dirichlet(m, n) (matrix/poisson2D_dirichlet.hpp:24-80):
+ * the 5-point Laplacian on an m x n grid (unknown k = i n + j, Dirichlet
+ * boundary) applied without a matrix; results bitwise the reference's.
+ * mtlg_poisson2d_solve runs any mtlg_solver except GMRES on it, host-driven,
+ * without preconditioning (the reference's tutorial use), FP64 vectors. */
+int mtlg_poisson2d_spmv(mtlg_ctx* ctx, int m, int n, const mtlg_vec* x, mtlg_vec* y, int assign);
+int mtlg_poisson2d_solve(mtlg_ctx* ctx, int solver, int m, int n, mtlg_vec* x, const mtlg_vec* b,
+                         const mtlg_iter_params* params, mtlg_iter_result* result);
 
 /* ---- batched solves ------------------------------------------------------- */
 /* Many independent systems of uneven size solved together: every kernel of an

@@ -36,6 +36,7 @@ F64, F32 = 0, 1
 ASSIGN, PLUS, MINUS = 0, 1, 2
 PC_IDENTITY, PC_DIAGONAL, PC_ILU0, PC_IC0 = 0, 1, 2, 3
 CG, BICGSTAB, GMRES = 0, 1, 2
+BICG, CGS, TFQMR, QMR, BICGSTAB_2, BICGSTAB_ELL, IDR_S = 3, 4, 5, 6, 7, 8, 9
 ST_RUNNING, ST_CONVERGED, ST_MAXIT, ST_BREAKDOWN, ST_NO_DIRECTION, ST_STALLED = 0, 1, 2, 3, 4, 5
 
 
@@ -122,6 +123,8 @@ SIGNATURES = {
     "mtlg_batch_size": (C.c_int, [VP]),
     "mtlg_partition_systems": (C.c_int, [C.c_int64, VP, C.c_int, VP, VP]),
     "mtlg_trace_enable": (C.c_int, [C.c_int]),
+    "mtlg_poisson2d_spmv": (C.c_int, [VP, C.c_int, C.c_int, VP, VP, C.c_int]),
+    "mtlg_poisson2d_solve": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, VP, VP, VP, VP]),
     "mtlg_ell_create": (C.c_int, [VP, C.c_int64, C.c_int64, C.c_int64, C.c_int64, VP, VP, C.c_int, C.POINTER(VP)]),
     "mtlg_ell_destroy": (C.c_int, [VP]),
     "mtlg_ell_spmv": (C.c_int, [VP, VP, VP, VP, C.c_int]),

@@ -240,6 +240,7 @@ struct mtlg_csr {
     DBuf<SysDesc> desc;
     DBuf<SysState> st;
     DBuf<int> misc;                // running, err[3]
+    mtlg_csr* AT = nullptr;        // transpose (made for bicg / qmr on first need)
 };
 
 namespace mtlg {

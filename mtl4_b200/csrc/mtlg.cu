@@ -2,6 +2,7 @@
 // The declarations and the reference interface each entry point replaces are
 // in include/mtl4_b200/mtlg.h.
 #include "host_solve.cuh"
+#include "host_krylov.cuh"
 
 #include <map>
 #include <cmath>
@@ -235,6 +236,21 @@ int launch_spmv_rows(mtlg_ctx* c, mtlg_csr* A, const void* x, void* y, int asg)
 extern "C" int mtlg_pc_apply(mtlg_ctx* c, mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y);
 
 namespace mtlg {
+int pc_adjoint_raw(mtlg_ctx* c, mtlg_pc* P, int64_t n, const double* x, double* y)
+{
+    if (!P || P->kind == MTLG_PC_IDENTITY) {
+        if (x != y) MTLG_CUDA(cudaMemcpyAsync(y, x, size_t(n) * 8, cudaMemcpyDeviceToDevice, c->stream));
+        return MTLG_OK;
+    }
+    mtlg_vec xv, yv;
+    xv.ctx = yv.ctx = c;
+    xv.n = yv.n = n;
+    xv.dtype = yv.dtype = MTLG_F64;
+    xv.p = const_cast<double*>(x);
+    yv.p = y;
+    return mtlg_pc_adjoint_apply(c, P, &xv, &yv);
+}
+
 int pc_apply_raw(mtlg_ctx* c, mtlg_pc* P, int dtype, int64_t n, const void* x, void* y)
 {
     if (!P || P->kind == MTLG_PC_IDENTITY) {
@@ -572,6 +588,7 @@ int mtlg_csr_destroy(mtlg_csr* A)
 {
     if (!A) return MTLG_OK;
     cudaStreamSynchronize(A->ctx->stream);
+    if (A->AT) mtlg_csr_destroy(A->AT);
     purge_sets(A->ctx, A);
     delete A;
     return MTLG_OK;
@@ -811,6 +828,23 @@ static int vec_binary(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, int kin
     return MTLG_OK;
 }
 
+extern "C++" {
+namespace mtlg {
+// dot of raw FP64 device vectors in the summation kind rk (used by the
+// host-driven bodies)
+int dot_raw(mtlg_ctx* c, int64_t n, const double* x, const double* y, int rk, double* out)
+{
+    mtlg_vec xv, yv;
+    xv.ctx = yv.ctx = c;
+    xv.n = yv.n = n;
+    xv.dtype = yv.dtype = MTLG_F64;
+    xv.p = const_cast<double*>(x);
+    yv.p = const_cast<double*>(y);
+    return vec_binary(c, &xv, &yv, VOP_DOT, 0.0, out, rk);
+}
+}  // namespace mtlg
+}  // extern "C++"
+
 int mtlg_dot(mtlg_ctx* c, const mtlg_vec* x, const mtlg_vec* y, double* out)
 {
     MTLG_TRACE(2003, "dot");
@@ -1048,6 +1082,18 @@ int mtlg_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* L, mtlg_pc* R, mtl
         c->log_n = 0;   // GMRES runs its tests on the host: no residual log
         return mtlg_gmres_impl(c, A, L, R, x, b, p, res);
     }
+    if (solver >= MTLG_BICG && solver <= MTLG_IDR_S) {
+        c->log_n = 0;
+        if (x->dtype != MTLG_F64) {
+            set_error("the host-driven Krylov bodies take FP64 vectors");
+            return MTLG_ERR_NOT_SUPPORTED;
+        }
+        KOp op;
+        op.c = c;
+        op.A = A;
+        op.n = A->n_rows;
+        return krylov_run(c, solver, op, L, R, static_cast<double*>(x->p), static_cast<const double*>(b->p), p, res);
+    }
     const int f32 = x->dtype == MTLG_F32;
     if (L && L->kind == MTLG_PC_IDENTITY) L = nullptr;   // is_identity(P) short-cut (cg.hpp:80-81)
     SetKey key{A, L, solver, f32, 0, c->red_order};
@@ -1206,3 +1252,43 @@ int mtlg_refine_solve(mtlg_ctx* c, int solver, mtlg_csr* A, mtlg_pc* P, mtlg_vec
 #include "host_gmres.cuh"
 #include "host_batch.cuh"
 #include "formats.cuh"
+
+extern "C" {
+
+int mtlg_poisson2d_spmv(mtlg_ctx* c, int m, int n, const mtlg_vec* x, mtlg_vec* y, int assign)
+{
+    using namespace mtlg;
+    MTLG_TRACE(3080, "poisson2D_dirichlet::mult");
+    MTLG_CHECK_ARG(c && x && y && m >= 1 && n >= 1, "ctx/vectors/grid");
+    MTLG_CHECK_ARG(x->dtype == MTLG_F64 && y->dtype == MTLG_F64, "poisson2D takes FP64 vectors");
+    MTLG_CHECK_ARG(assign >= MTLG_ASSIGN && assign <= MTLG_MINUS, "assign");
+    if (x->n != int64_t(m) * n || y->n != int64_t(m) * n) {
+        set_error("poisson2D %dx%d needs vectors of %lld", m, n, (long long)m * n);
+        return MTLG_ERR_INCOMPATIBLE_SIZE;
+    }
+    const int asg = assign == MTLG_ASSIGN ? ASG_SET : (assign == MTLG_PLUS ? ASG_ADD : ASG_SUB);
+    return poisson2d_apply(c, m, n, static_cast<const double*>(x->p), static_cast<double*>(y->p), asg);
+}
+
+int mtlg_poisson2d_solve(mtlg_ctx* c, int solver, int m, int n, mtlg_vec* x, const mtlg_vec* b,
+                         const mtlg_iter_params* p, mtlg_iter_result* res)
+{
+    using namespace mtlg;
+    MTLG_TRACE(9112, "poisson2D_solve");
+    MTLG_CHECK_ARG(c && x && b && p && m >= 1 && n >= 1, "ctx/vectors/params");
+    MTLG_CHECK_ARG(x->dtype == MTLG_F64 && b->dtype == MTLG_F64, "FP64 vectors");
+    MTLG_CHECK_ARG(solver != MTLG_GMRES && solver >= MTLG_CG && solver <= MTLG_IDR_S, "solver");
+    if (x->n != int64_t(m) * n || b->n != int64_t(m) * n) {
+        set_error("poisson2D %dx%d needs vectors of %lld", m, n, (long long)m * n);
+        return MTLG_ERR_INCOMPATIBLE_SIZE;
+    }
+    KOp op;
+    op.c = c;
+    op.pm = m;
+    op.pn = n;
+    op.n = int64_t(m) * n;
+    return krylov_run(c, solver, op, nullptr, nullptr, static_cast<double*>(x->p), static_cast<const double*>(b->p),
+                      p, res);
+}
+
+}  // extern "C"

@@ -222,6 +222,9 @@ def adjoint_solve(P: pc._base, x: dense_vector, y: dense_vector | None = None) -
 
 
 def _solve(kind, A, x, b, L, R, it: basic_iteration, restart=0) -> int:
+    from .mtl import poisson2D_dirichlet
+    if isinstance(A, poisson2D_dirichlet):
+        return _solve_poisson(kind, A, x, b, it, restart)
     res = _lib.IterResult()
     params = it._params(restart)
     logged = getattr(it, "wants_log", False)
@@ -244,6 +247,17 @@ def _solve(kind, A, x, b, L, R, it: basic_iteration, restart=0) -> int:
     return it.error_code()
 
 
+def _solve_poisson(kind, A, x, b, it: basic_iteration, restart=0) -> int:
+    """Solves on the matrix-free poisson2D_dirichlet operator (host-driven,
+    no preconditioning)."""
+    res = _lib.IterResult()
+    params = it._params(restart)
+    st = A.ctx._L.mtlg_poisson2d_solve(A.ctx.h, kind, A.m, A.n, x.h, b.h, C.byref(params), C.byref(res))
+    it._take(res)
+    check(st, "poisson2D solve")
+    return it.error_code()
+
+
 def cg(A, x, b, P, it: basic_iteration) -> int:
     return _solve(_lib.CG, A, x, b, P, None, it)
 
@@ -254,6 +268,35 @@ def bicgstab(A, x, b, P, it: basic_iteration) -> int:
 
 def gmres(A, x, b, L, R, it: basic_iteration, restart: int) -> int:
     return _solve(_lib.GMRES, A, x, b, L, R, it, restart)
+
+
+# Host-driven bodies on device vectors (itl/krylov/*.hpp), FP64.
+def bicg(A, x, b, P, it: basic_iteration) -> int:
+    return _solve(_lib.BICG, A, x, b, P, None, it)
+
+
+def cgs(A, x, b, P, it: basic_iteration) -> int:
+    return _solve(_lib.CGS, A, x, b, P, None, it)
+
+
+def tfqmr(A, x, b, L, R, it: basic_iteration) -> int:
+    return _solve(_lib.TFQMR, A, x, b, L, R, it)
+
+
+def qmr(A, x, b, L, R, it: basic_iteration) -> int:
+    return _solve(_lib.QMR, A, x, b, L, R, it)
+
+
+def bicgstab_2(A, x, b, P, it: basic_iteration) -> int:
+    return _solve(_lib.BICGSTAB_2, A, x, b, P, None, it)
+
+
+def bicgstab_ell(A, x, b, L, R, it: basic_iteration, ell: int) -> int:
+    return _solve(_lib.BICGSTAB_ELL, A, x, b, L, R, it, ell)
+
+
+def idr_s(A, x, b, L, R, it: basic_iteration, s: int) -> int:
+    return _solve(_lib.IDR_S, A, x, b, L, R, it, s)
 
 
 def refine(solver: str, A: compressed2D, x: dense_vector, b: dense_vector, P, rtol: float = 1e-8,

@@ -334,10 +334,28 @@ class sparse_banded:
             pass
 
 
+class poisson2D_dirichlet:
+    """Matrix-free 2D Poisson operator on an m x n grid (the reference's
+    mtl::mat::poisson2D_dirichlet, matrix/poisson2D_dirichlet.hpp:24-80)."""
+
+    def __init__(self, m: int, n: int, ctx: context | None = None):
+        self.ctx = ctx or default_context()
+        self.m, self.n = int(m), int(n)
+        self.shape = (self.m * self.n, self.m * self.n)
+
+    def num_rows(self) -> int:
+        return self.m * self.n
+
+    def __mul__(self, v: "dense_vector") -> "_MatVec":
+        return _MatVec(self, v)
+
+
 def mult(A, x: dense_vector, y: dense_vector, assign: str = "="):
     """y = A x, y += A x or y -= A x (A: compressed2D, ell_matrix or
     sparse_banded)."""
-    if isinstance(A, ell_matrix):
+    if isinstance(A, poisson2D_dirichlet):
+        check(A.ctx._L.mtlg_poisson2d_spmv(A.ctx.h, A.m, A.n, x.h, y.h, _ASSIGN[assign]), "mult")
+    elif isinstance(A, ell_matrix):
         check(A.ctx._L.mtlg_ell_spmv(A.ctx.h, A.h, x.h, y.h, _ASSIGN[assign]), "mult")
     elif isinstance(A, sparse_banded):
         check(A.ctx._L.mtlg_banded_spmv(A.ctx.h, A.h, x.h, y.h, _ASSIGN[assign]), "mult")

@@ -22,7 +22,8 @@ REF_OMP_LIB = HERE / "_ref" / "libmtlref_omp.so"
 PORT_LIB = HERE / "_build" / "libmtloracle.so"
 
 PC_KIND = {"identity": 0, "diagonal": 1, "ilu_0": 2, "ic_0": 3}
-SOLVER = {"cg": 0, "bicgstab": 1, "gmres": 2}
+SOLVER = {"cg": 0, "bicgstab": 1, "gmres": 2, "bicg": 3, "cgs": 4, "tfqmr": 5, "qmr": 6, "bicgstab_2": 7,
+          "bicgstab_ell": 8, "idr_s": 9}
 
 
 class RefResult(C.Structure):
@@ -75,6 +76,10 @@ def ref_lib(omp: bool = False) -> C.CDLL:
         L.mtlref_refine_solve.argtypes = [VP, C.c_int, C.c_int, VP, VP, C.c_int, C.c_int, C.c_double, C.c_double,
                                           C.c_int, C.POINTER(RefResult)]
         L.mtlref_laplacian_setup.argtypes = [C.c_int, C.c_int, PI, VP, VP, VP]
+        L.mtlref_solve_krylov.argtypes = [VP, C.c_int, C.c_int, VP, VP, C.c_int, C.c_double, C.c_int,
+                                          C.POINTER(RefResult)]
+        L.mtlref_poisson2d_mult.argtypes = [C.c_int, C.c_int, VP, VP, C.c_int]
+        L.mtlref_poisson2d_cg.argtypes = [C.c_int, C.c_int, VP, VP, C.c_int, C.c_double, C.POINTER(RefResult)]
         L.mtlref_ell_export.argtypes = [VP, PI, PI, VP, VP]
         L.mtlref_ell_spmv.argtypes = [VP, VP, VP, C.c_int]
         L.mtlref_banded_export.argtypes = [VP, PI, VP, VP]
@@ -201,6 +206,15 @@ class RefMatrix:
                                       rtol, atol, restart, C.byref(r))
         return {"x": x, "iterations": r.iterations, "error": err, "resid": r.resid, "relresid": r.relresid,
                 "setup_s": r.setup_s, "solve_s": r.solve_s}
+
+    def solve_krylov(self, b, solver, pc="identity", max_iter=2000, rtol=1e-8, param=0):
+        """FP64 bicg / cgs / tfqmr / qmr / bicgstab_2 / bicgstab_ell / idr_s."""
+        r = RefResult()
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.A.n_rows)
+        err = self.L.mtlref_solve_krylov(self.h, SOLVER[solver], PC_KIND[pc], _p(b), _p(x), max_iter, rtol, param,
+                                         C.byref(r))
+        return {"x": x, "iterations": r.iterations, "error": err, "resid": r.resid, "relresid": r.relresid}
 
     def solve_cyclic(self, b, solver="cg", pc="identity", max_iter=2000, rtol=1e-8, cycle=100, multi_print=False):
         """FP64 solve with itl::cyclic_iteration printing into a string;
@@ -339,3 +353,17 @@ def port_banded_spmv(n_rows, n_cols, bands, data, x, assign=0, y=None):
     da = np.ascontiguousarray(data, np.float64)
     L.mtlo_banded_spmv(n_rows, n_cols, b.size, _p(b), _p(da), _p(np.ascontiguousarray(x, np.float64)), _p(y), assign)
     return y
+
+
+def ref_poisson2d_mult(m, n, x, assign=0, y=None):
+    y = np.zeros(m * n) if y is None else np.array(y, np.float64)
+    ref_lib().mtlref_poisson2d_mult(m, n, _p(np.ascontiguousarray(x, np.float64)), _p(y), assign)
+    return y
+
+
+def ref_poisson2d_cg(m, n, b, max_iter=2000, rtol=1e-8):
+    r = RefResult()
+    x = np.zeros(m * n)
+    err = ref_lib().mtlref_poisson2d_cg(m, n, _p(np.ascontiguousarray(b, np.float64)), _p(x), max_iter, rtol,
+                                        C.byref(r))
+    return {"x": x, "iterations": r.iterations, "error": err, "relresid": r.relresid}

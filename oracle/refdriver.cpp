@@ -19,6 +19,7 @@
 #include <boost/numeric/mtl/mtl.hpp>
 #include <boost/numeric/mtl/io/matrix_market.hpp>
 #include <boost/numeric/itl/itl.hpp>
+#include <boost/numeric/mtl/matrix/poisson2D_dirichlet.hpp>
 
 #include <chrono>
 #include <cstdio>
@@ -325,6 +326,24 @@ static int solve_typed(int solver, int kind, int pc_f32, const Mat& A, const Fac
 }
 
 template <typename PC>
+static int run_krylov(int solver, const dmat& A, dvec& x, const dvec& b, const PC& P, itl::basic_iteration<double>& iter,
+                      int param)
+{
+    itl::pc::identity<dmat> I(A);
+    PC& Pm = const_cast<PC&>(P);
+    switch (solver) {
+    case 3: return itl::bicg(A, x, b, P, iter);
+    case 4: return itl::cgs(A, x, b, P, iter);
+    case 5: return itl::tfqmr(A, x, b, P, I, iter);
+    case 6: return itl::qmr(A, x, b, Pm, I, iter);
+    case 7: return itl::bicgstab_2(A, x, b, P, iter);
+    case 8: return itl::bicgstab_ell(A, x, b, P, I, iter, std::size_t(param > 0 ? param : 2));
+    case 9: return itl::idr_s(A, x, b, P, I, iter, std::size_t(param > 0 ? param : 4));
+    default: return -1;
+    }
+}
+
+template <typename PC>
 static int run_cyclic(int solver, const dmat& A, dvec& x, const dvec& b, const PC& P,
                       itl::cyclic_iteration<double>& iter)
 {
@@ -396,6 +415,59 @@ void mtlref_banded_spmv(void* p, const double* x, double* y, int assign)
     RefCsr* h = static_cast<RefCsr*>(p);
     dvec vx(h->n_cols, const_cast<double*>(x)), vy(h->n_rows, y);
     spmv_impl(band_copy(h), vx, vy, assign);
+}
+
+/// FP64 bicg (3), cgs (4), tfqmr (5), qmr (6), bicgstab_2 (7),
+/// bicgstab_ell (8, ell = param), idr_s (9, s = param) with a left
+/// preconditioner of `kind` (right: identity), basic_iteration from b.
+int mtlref_solve_krylov(void* p, int solver, int kind, const double* b, double* x, int max_iter, double rtol, int param,
+                        mtlref_result* out)
+{
+    RefCsr* h = static_cast<RefCsr*>(p);
+    dvec vb(h->n_rows, const_cast<double*>(b)), vx(h->n_rows, x);
+    itl::basic_iteration<double> iter(vb, max_iter, rtol);
+    int err = -1;
+    try {
+        const dmat& A = *h->A;
+        if (kind == 0) { itl::pc::identity<dmat> P(A); err = run_krylov(solver, A, vx, vb, P, iter, param); }
+        else if (kind == 1) { itl::pc::diagonal<dmat> P(A); err = run_krylov(solver, A, vx, vb, P, iter, param); }
+        else if (kind == 2) { itl::pc::ilu_0<dmat> P(A); err = run_krylov(solver, A, vx, vb, P, iter, param); }
+        else if (kind == 3) { itl::pc::ic_0<dmat> P(A); err = run_krylov(solver, A, vx, vb, P, iter, param); }
+    } catch (const itl::unexpected_orthogonality&) {
+        err = -2;
+    }
+    if (out) {
+        out->iterations = iter.iterations(); out->error = err; out->resid = iter.resid();
+        out->relresid = iter.relresid(); out->setup_s = 0; out->solve_s = 0;
+        out->outer_iterations = 0; out->pad = 0;
+    }
+    return err;
+}
+
+/// poisson2D_dirichlet(m, n) times x (matrix/poisson2D_dirichlet.hpp), and a
+/// CG solve on it without preconditioning (the tutorial's use).
+void mtlref_poisson2d_mult(int m, int n, const double* x, double* y, int assign)
+{
+    mtl::mat::poisson2D_dirichlet A(m, n);
+    dvec vx(std::size_t(m) * n, const_cast<double*>(x)), vy(std::size_t(m) * n, y);
+    if (assign == 0) vy = A * vx;
+    else if (assign == 1) vy += A * vx;
+    else vy -= A * vx;
+}
+
+int mtlref_poisson2d_cg(int m, int n, const double* b, double* x, int max_iter, double rtol, mtlref_result* out)
+{
+    mtl::mat::poisson2D_dirichlet A(m, n);
+    dvec vb(std::size_t(m) * n, const_cast<double*>(b)), vx(std::size_t(m) * n, x);
+    itl::basic_iteration<double> iter(vb, max_iter, rtol);
+    itl::pc::identity<mtl::mat::poisson2D_dirichlet> P(A);
+    const int err = itl::cg(A, vx, vb, P, iter);
+    if (out) {
+        out->iterations = iter.iterations(); out->error = err; out->resid = iter.resid();
+        out->relresid = iter.relresid(); out->setup_s = 0; out->solve_s = 0;
+        out->outer_iterations = 0; out->pad = 0;
+    }
+    return err;
 }
 
 /// FP64 CG (solver 0) or BiCGSTAB (1) with itl::cyclic_iteration<double>

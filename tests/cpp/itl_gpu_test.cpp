@@ -91,6 +91,23 @@ int main()
         REQUIRE(t.find("finished! error code = 0") != std::string::npos, "cyclic summary");
     }
     {
+        // the other Krylov bodies with the reference's call shapes
+        itl::pc::ilu_0<matrix_type> P(A);
+        itl::pc::identity<matrix_type> I(A);
+        const char* names[] = {"cgs", "bicgstab_2", "tfqmr", "bicgstab_ell(2)", "idr_s(4)"};
+        for (int k = 0; k < 5; ++k) {
+            itl::basic_iteration<double> iter(b, 2000, 1.e-8);
+            x = 0.0;
+            if (k == 0) itl::cgs(A, x, b, P, iter);
+            else if (k == 1) itl::bicgstab_2(A, x, b, P, iter);
+            else if (k == 2) itl::tfqmr(A, x, b, I, I, iter);
+            else if (k == 3) itl::bicgstab_ell(A, x, b, P, I, iter, 2);
+            else itl::idr_s(A, x, b, I, I, iter, 4);
+            std::printf("%s: %d iterations, relres %.3e\n", names[k], iter.iterations(), relres(A, x, b));
+            REQUIRE(iter.error_code() == 0, names[k]);
+        }
+    }
+    {
         itl::pc::identity<matrix_type> L(A), R(A);
         itl::basic_iteration<double> iter(b, 5000, 1.e-8);
         x = 0.0;

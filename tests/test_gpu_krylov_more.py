@@ -1,0 +1,81 @@
+"""The reference's other Krylov bodies (itl/krylov/bicg, cgs, tfqmr, qmr,
+bicgstab_2, bicgstab_ell, idr_s) on device vectors, and the matrix-free
+poisson2D_dirichlet operator: against the reference build on the same
+inputs -- the iteration count within the +-2 bound where the method is
+deterministic, the same error code, and the solution meeting the tolerance
+the method reports.  IDR(s) draws its shadow space from another random
+generator than the reference, so its count is compared loosely."""
+import numpy as np
+import pytest
+
+from mtl4_b200 import problems as P
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CASES = [("bicg", "identity", 0), ("cgs", "identity", 0), ("cgs", "ilu_0", 0), ("tfqmr", "identity", 0),
+         ("tfqmr", "ilu_0", 0), ("qmr", "ilu_0", 0), ("bicgstab_2", "identity", 0), ("bicgstab_2", "ilu_0", 0),
+         ("bicgstab_ell", "identity", 3), ("bicgstab_ell", "ilu_0", 3), ("idr_s", "identity", 4)]
+
+
+def run(ctx, A, b, solver, pc, param, rctx=False):
+    from mtl4_b200 import itl, mtl
+    Ad = mtl.compressed2D.from_problem(A, ctx)
+    Pc = None if pc == "identity" else getattr(itl.pc, pc)(Ad)
+    x = mtl.dense_vector(A.n_rows, np.float64, ctx)
+    bd = mtl.dense_vector(b, np.float64, ctx)
+    it = itl.basic_iteration(bd, 2000, 1e-8)
+    f = getattr(itl, solver)
+    if solver in ("tfqmr", "qmr"):
+        f(Ad, x, bd, Pc, None, it)
+    elif solver in ("bicgstab_ell", "idr_s"):
+        f(Ad, x, bd, Pc, None, it, param)
+    else:
+        f(Ad, x, bd, Pc, it)
+    return x.numpy(), it
+
+
+@pytest.mark.parametrize("solver,pc,param", CASES)
+def test_krylov_bodies_against_the_reference(ctx, solver, pc, param):
+    A, b, _ = P.config2_solve(12)
+    ref = O.RefMatrix(A).solve_krylov(b, solver, pc, param=param)
+    ctx.set_tuning("reduction_order", 1)
+    try:
+        x, it = run(ctx, A, b, solver, pc, param)
+    finally:
+        ctx.set_tuning("reduction_order", 0)
+    assert it.error_code() == max(ref["error"], 0), (it.error_code(), ref)
+    if solver == "idr_s":
+        assert it.iterations() <= 2 * ref["iterations"] + 10, (it.iterations(), ref["iterations"])
+    else:
+        assert abs(it.iterations() - ref["iterations"]) <= 2, (it.iterations(), ref["iterations"])
+    if pc == "identity" and solver not in ("qmr",):
+        assert np.linalg.norm(A.matvec(x) - b) <= 1.5e-8 * np.linalg.norm(b)
+
+
+def test_poisson2d_matrix_free(ctx):
+    from mtl4_b200 import itl, mtl
+    m, n = 37, 23
+    Pm = mtl.poisson2D_dirichlet(m, n, ctx)
+    v = np.random.default_rng(3).standard_normal(m * n)
+    y = mtl.dense_vector(m * n, np.float64, ctx)
+    mtl.mult(Pm, mtl.dense_vector(v, np.float64, ctx), y)
+    assert np.array_equal(y.numpy(), O.ref_poisson2d_mult(m, n, v))
+    # the same operator as the assembled Laplacian (laplacian_setup(m, n))
+    Lap = P.laplacian_2d(m, n)
+    assert np.array_equal(y.numpy(), O.port_spmv(Lap, v))
+    y0 = np.random.default_rng(4).standard_normal(m * n)
+    y2 = mtl.dense_vector(y0, np.float64, ctx)
+    mtl.mult(Pm, mtl.dense_vector(v, np.float64, ctx), y2, "-=")
+    assert np.array_equal(y2.numpy(), O.ref_poisson2d_mult(m, n, v, 2, y0))
+    b = np.ones(m * n)
+    ref = O.ref_poisson2d_cg(m, n, b)
+    ctx.set_tuning("reduction_order", 1)
+    try:
+        x = mtl.dense_vector(m * n, np.float64, ctx)
+        it = itl.basic_iteration(mtl.dense_vector(b, np.float64, ctx), 2000, 1e-8)
+        itl.cg(Pm, x, mtl.dense_vector(b, np.float64, ctx), None, it)
+    finally:
+        ctx.set_tuning("reduction_order", 0)
+    assert it.error_code() == 0 and abs(it.iterations() - ref["iterations"]) <= 2
+    assert np.abs(x.numpy() - ref["x"]).max() <= 1e-6 * np.abs(ref["x"]).max()
