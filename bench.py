@@ -333,8 +333,9 @@ def run_kernel_case(args):
     from mtl4_b200 import itl, mtl
     from mtl4_b200 import problems as P
     ctx = mtl.context(0)
-    if args.kernel in ("spmv_powerlaw", "spmv_stencil"):
-        A = P.config2_spmv() if args.kernel == "spmv_powerlaw" else P.config2_solve(128)[0]
+    if args.kernel in ("spmv_powerlaw", "spmv_stencil", "spmv_lap2048"):
+        A = (P.config2_spmv() if args.kernel == "spmv_powerlaw" else P.config2_solve(128)[0]
+             if args.kernel == "spmv_stencil" else P.laplacian_2d(2048))
         Ad = mtl.compressed2D.from_problem(A, ctx)
         x = mtl.dense_vector(np.random.default_rng(0).standard_normal(A.n_rows), np.float64, ctx)
         y = mtl.dense_vector(A.n_rows, np.float64, ctx)
@@ -382,7 +383,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the config 3/4/5 samples")
     ap.add_argument("--serve-requests", type=int, default=200)
-    ap.add_argument("--kernel", choices=["spmv_powerlaw", "spmv_stencil", "sweep_ilu0", "solve_mixed"],
+    ap.add_argument("--kernel", choices=["spmv_powerlaw", "spmv_stencil", "spmv_lap2048", "sweep_ilu0", "solve_mixed"],
                     help="run one kernel on its bench case a few times and exit (for profilers)")
     ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()

@@ -180,8 +180,28 @@ inline void plan_tiles(const int64_t* rp, int n, int sys, std::vector<Tile>& out
     }
 }
 
-// Row-aligned warp tasks (see k_spmv_rows).
+inline void plan_warp_runs(const int64_t* rp, int n, std::vector<WarpTask>& out);
+
+// Row-aligned warp tasks (see k_spmv_rows), listed in the order the warps
+// take them: long-row tasks first (most entries first), then the runs.
 inline void plan_warp_tasks(const int64_t* rp, int n, std::vector<WarpTask>& out)
+{
+    std::vector<WarpTask> runs;
+    plan_warp_runs(rp, n, runs);
+    out.clear();
+    out.reserve(runs.size());
+    for (const WarpTask& t : runs)
+        if (t.row_end - t.row_begin == 1 && t.nnz_end - t.nnz_begin > kWarpNnz) out.push_back(t);
+    std::stable_sort(out.begin(), out.end(), [](const WarpTask& a, const WarpTask& b) {
+        return a.nnz_end - a.nnz_begin > b.nnz_end - b.nnz_begin;
+    });
+    for (const WarpTask& t : runs)
+        if (!(t.row_end - t.row_begin == 1 && t.nnz_end - t.nnz_begin > kWarpNnz)) out.push_back(t);
+}
+
+// Tasks in row order: a run of consecutive rows with at most kWarpNnz
+// entries (and rows), or one longer row.
+inline void plan_warp_runs(const int64_t* rp, int n, std::vector<WarpTask>& out)
 {
     int r = 0;
     while (r < n) {
@@ -231,6 +251,7 @@ struct mtlg_csr {
     int64_t tiles_by_kind[3] = {0, 0, 0};
     std::vector<WarpTask> wtasks;  // row-aligned warp tasks (irregular matrices)
     DBuf<WarpTask> d_wtasks;
+    DBuf<int> wctr;                // k_spmv_rows task counter and exit count (self-resetting)
     bool irregular = false;        // some row longer than kShortRow entries
     // single-system operation set (standalone SpMV / dot)
     DBuf<Tile> d_tiles;

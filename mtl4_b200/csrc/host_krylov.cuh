@@ -23,10 +23,11 @@ enum KVec : int {
     KV_SCAL,        // y = a y
     KV_DIV,         // y = x / a
     KV_XMY,         // y = x - z
-    KV_XPAYPBZ,     // y = x + a (z + b y)        (cgs: p = u + beta (q + beta p))
+    KV_XPAYPBZ,     // y = x + a (z + b y)        (cgs: p = u + beta (q + beta p); tfqmr's v)
     KV_XPAZ,        // y = x + a z
-    KV_XPAYPBZ2,    // y = x + a (y + b z)        (tfqmr: v = u1 + beta (u2 + beta v); bicgstab's p)
+    KV_XPAYPBZ2,    // y = x + a (y + b z)        (bicgstab: p = r + beta (p - omega v))
     KV_AXPBZ,       // y = y + (a x + b z)        (bicgstab: x += omega shat + alpha phat)
+    KV_AX,          // y = a x                    (y is not read)
 };
 
 __global__ void __launch_bounds__(kBlock) k_kvec(int op, long long n, double* __restrict__ y,
@@ -47,6 +48,7 @@ __global__ void __launch_bounds__(kBlock) k_kvec(int op, long long n, double* __
         case KV_XPAZ: y[i] = fma(a, z[i], x[i]); break;
         case KV_XPAYPBZ2: y[i] = fma(a, fma(b, z[i], y[i]), x[i]); break;
         case KV_AXPBZ: y[i] = y[i] + fma(a, x[i], b * z[i]); break;
+        case KV_AX: y[i] = a * x[i]; break;
         default: break;
         }
     }
@@ -279,7 +281,7 @@ inline int k_tfqmr(KOp& A, KWork& W, double* x, const double* b, mtlg_pc* L, mtl
         KTRY(kpc(W.c, R, n, y1, t));
         KTRY(A.apply(t, rt));
         KTRY(kpc(W.c, L, n, rt, u1));
-        KTRY(W.kv(KV_XPAYPBZ2, v, u1, u2, beta, beta));       // v = u1 + beta (u2 + beta v)
+        KTRY(W.kv(KV_XPAYPBZ, v, u1, u2, beta, beta));        // v = u1 + beta (u2 + beta v)
     }
     KTRY(kpc(W.c, R, n, x, t));
     return W.kv(KV_COPY, x, t);
@@ -343,8 +345,8 @@ inline int k_qmr(KOp& A, KWork& W, double* x, const double* b, mtlg_pc* L, mtlg_
         if (gamma == 0.0) return it.fail(6), MTLG_OK;
         eta = -eta * rho_1 * gamma * gamma / (beta * gamma_1 * gamma_1);
         if (it.first()) {
-            KTRY(W.kv(KV_AXPBY, d, p, nullptr, eta, 0.0));
-            KTRY(W.kv(KV_AXPBY, s, pt, nullptr, eta, 0.0));
+            KTRY(W.kv(KV_AX, d, p, nullptr, eta));
+            KTRY(W.kv(KV_AX, s, pt, nullptr, eta));
         } else {
             const double f = theta_1 * theta_1 * gamma * gamma;
             KTRY(W.kv(KV_AXPBY, d, p, nullptr, eta, f));
@@ -454,9 +456,10 @@ inline int k_bicgstab_ell(KOp& A, KWork& W, double* x, const double* b, mtlg_pc*
             for (int i = j + 1; i <= l; ++i) sum += tau[j][i] * gamma[i];
             gamma[j] = gamma_a[j] - sum;
         }
+        // gamma_aa[1..l) = strict_upper(tau[1..l)[1..l)) * gamma[2..l] + gamma[2..l]
         for (int j = 1; j < l; ++j) {
             double sum = 0.0;
-            for (int i = j + 1; i < l + 1; ++i) sum += tau[j][i] * gamma[i];   // strict_upper(tau) * gamma[2..]
+            for (int i = j + 1; i < l; ++i) sum += tau[j][i] * gamma[i + 1];
             gamma_aa[j] = sum + gamma[j + 1];
         }
         KTRY(W.kv(KV_AXPY, x, rh[0], nullptr, gamma[1]));

@@ -766,6 +766,7 @@ struct mtlg_pc {
                                     // refinement finishes with (made on first need)
     ChunkPlan plan[2];              // chunked sweeps with FP64 [0] / FP32 [1] vectors
     int plan_kernel[2] = {-1, -1};  // context's sweep_kernel / cluster setting the plan was made for
+    mtlg_pc* adjoint = nullptr;     // ILU(0): factors of (LU)^H, made on the first adjoint apply
     RowLists lt;                    // IC(0): transposed upper pattern (natural order)
     DBuf<int> lt_rp, lt_row, lt_src;
     bool has_factors() const { return kind == MTLG_PC_ILU0 || kind == MTLG_PC_IC0; }
@@ -1062,6 +1063,107 @@ inline int pc_build(mtlg_pc* P)
         set_error("factorization dependency wait expired");
         return MTLG_ERR_TIMEOUT;
     }
+    return MTLG_OK;
+}
+
+// FP64 copies of factor values stored as S (exact for FP32).
+__global__ void k_widen(int n, const void* __restrict__ v, int f32, double* __restrict__ out)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        out[k] = f32 ? double(static_cast<const float*>(v)[k]) : static_cast<const double*>(v)[k];
+}
+
+// Row lists of the transpose of a factor (from its flat layout): row j of
+// the result holds the entries (i, j) of T, each with src = src_off + its
+// flat index, columns ascending or descending.
+inline void transpose_rows(const TriDev& T, int n, int src_off, bool descending, RowLists& R)
+{
+    R.rp.assign(size_t(n) + 1, 0);
+    for (int k = 0; k < T.nnz; ++k) R.rp[size_t(T.h_ci[k]) + 1]++;
+    for (int i = 0; i < n; ++i) R.rp[size_t(i) + 1] += R.rp[size_t(i)];
+    R.col.assign(size_t(T.nnz), 0);
+    R.src.assign(size_t(T.nnz), 0);
+    R.mul.assign(size_t(T.nnz), -1);
+    std::vector<int> pos(R.rp.begin(), R.rp.end() - 1);
+    for (int p = 0; p < T.npad; ++p) {
+        const int i = T.h_row_of[p];
+        if (i < 0) continue;
+        for (int k = T.h_rp[p]; k < T.h_rp[p + 1]; ++k) {
+            const int o = pos[size_t(T.h_ci[k])]++;
+            R.col[size_t(o)] = i;
+            R.src[size_t(o)] = src_off + k;
+        }
+    }
+    parallel_for(n, [&](int j) {
+        const int a = R.rp[size_t(j)], e = R.rp[size_t(j) + 1];
+        if (e - a < 2) return;
+        std::vector<std::pair<int, int>> v;
+        v.reserve(size_t(e - a));
+        for (int o = a; o < e; ++o) v.push_back({R.col[size_t(o)], R.src[size_t(o)]});
+        if (descending) std::sort(v.begin(), v.end(), [](auto x, auto y) { return x.first > y.first; });
+        else std::sort(v.begin(), v.end());
+        for (int o = a; o < e; ++o) {
+            R.col[size_t(o)] = v[size_t(o - a)].first;
+            R.src[size_t(o)] = v[size_t(o - a)].second;
+        }
+    });
+}
+
+// ILU(0) adjoint apply, (LU)^H y = x: first U^H y0 = x (lower, the inverse
+// pivots as multipliers), then L^H y = y0 (upper, unit diagonal) -- the
+// reference's adjoint_lower_solver / adjoint_upper_solver on the transposed
+// views (itl/pc/ilu.hpp:104-115).  Those run column-oriented
+// (lower_trisolve.hpp:155-170, upper_trisolve.hpp:129-149): a row of U^H
+// takes its contributions in ascending column order, a row of L^H in
+// descending order (columns are processed from the last one down); the row
+// lists keep those orders, so the row-oriented sweeps add in the same
+// sequence.
+inline int pc_build_adjoint(mtlg_pc* P)
+{
+    mtlg_ctx* c = P->ctx;
+    const int n = P->n;
+    const TriDev& L = P->L;
+    const TriDev& U = P->U;
+    const int f32 = P->storage == MTLG_F32;
+    std::unique_ptr<mtlg_pc> Q(new mtlg_pc);
+    Q->ctx = c;
+    Q->A = P->A;
+    Q->kind = MTLG_PC_ILU0;
+    Q->storage = P->storage;
+    Q->n = n;
+    DBuf<double> v64;
+    MTLG_TRY(v64.alloc(c, size_t(std::max(1, L.nnz + U.nnz))));
+    if (L.nnz) k_widen<<<launch_grid(L.nnz), 256, 0, c->stream>>>(L.nnz, L.val.p, f32, v64.p);
+    if (U.nnz) k_widen<<<launch_grid(U.nnz), 256, 0, c->stream>>>(U.nnz, U.val.p, f32, v64.p + L.nnz);
+    c->launches += (L.nnz > 0) + (U.nnz > 0);
+    MTLG_CUDA(cudaGetLastError());
+    RowLists Lh, Uh;   // U^H (lower), L^H (upper)
+    transpose_rows(U, n, L.nnz, false, Lh);
+    transpose_rows(L, n, 0, true, Uh);
+    const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
+    MTLG_TRY(build_tri(c, Lh, n, true, Q->L, B, int(P->ssize())));
+    MTLG_TRY(build_tri(c, Uh, n, false, Q->U, B, int(P->ssize())));
+    MTLG_TRY(pc_setup_single_set(Q.get()));
+    MTLG_TRY(Q->inv_dia.alloc(c, size_t(std::max(n, 1))));
+    if (n) MTLG_CUDA(cudaMemcpyAsync(Q->inv_dia.p, P->inv_dia.p, size_t(n) * 8, cudaMemcpyDeviceToDevice, c->stream));
+    for (TriDev* T : {&Q->L, &Q->U}) {
+        const int unit = T == &Q->U;
+        MTLG_TRY(T->val.alloc(c, size_t(std::max(T->nnz, 1)) * Q->ssize()));
+        MTLG_TRY(T->dia.alloc(c, size_t(std::max(T->npad, 1)) * Q->ssize()));
+        if (T->nnz) {
+            k_fill_factor<<<launch_grid(T->nnz), 256, 0, c->stream>>>(T->nnz, T->src.p, T->mul.p, v64.p, Q->inv_dia.p,
+                                                                      T->val.p, f32);
+            c->launches++;
+        }
+        if (T->npad) {
+            k_fill_dia<<<launch_grid(T->npad), 256, 0, c->stream>>>(T->npad, T->row_of.p, Q->inv_dia.p, unit, T->dia.p, f32);
+            c->launches++;
+        }
+        MTLG_CUDA(cudaGetLastError());
+        MTLG_TRY(fill_chunk_values(Q.get(), *T, v64.p, Q->inv_dia.p, unit));
+    }
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    P->adjoint = Q.release();
     return MTLG_OK;
 }
 

@@ -566,41 +566,79 @@ struct WarpTask {
     int row_begin, row_end, nnz_begin, nnz_end;
 };
 
-// Run tasks: lanes load values and columns with coalesced loads and issue up
-// to 8 independent x gathers each; values and gathered x go to shared memory
-// and every lane then sums whole rows of up to kSeqRow entries from there,
+// Element copies global -> shared without register staging (cp.async of 4
+// or 8 bytes, cached in L1 as the only size-generic form allows).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_drain_warp()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+    __syncwarp();
+}
+
+// Run tasks: each lane loads 8 column indices (coalesced) and issues, without
+// register staging, the copies of the matching values and the 8 gathers of x
+// into the warp's shared buffers (cp.async), plus the task's row pointers;
+// every lane then sums whole rows of up to kSeqRow entries from there,
 // sequentially in storage order with row_step (so such a row's result is
-// bitwise the reference's row sum); longer rows are summed by the whole warp.  No CTA
-// barrier: warps proceed independently.  Long-row tasks: the warp strides
-// over the row (8 gathers in flight per lane) and reduces with a fixed tree.
+// bitwise the reference's row sum); longer rows are summed by the whole warp.
+// Long-row tasks: the warp strides over the row 256 entries at a time
+// through the same buffers and reduces with a fixed tree.
+// Scheduling: warps take tasks from a counter (one atomic per task) in the
+// order of the task list -- long-row tasks first, most entries first, then
+// the runs in row order -- so no warp is left holding several long rows at
+// the end; the next task's descriptor is loaded while the current one runs.
+// The last warp to finish resets the counter for the next launch.  No CTA
+// barrier: warps proceed independently.
 template <typename T, int ASG>
 __global__ void __launch_bounds__(kBlock, 3)
-k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restrict__ rp, const int* __restrict__ ci,
-            const T* __restrict__ va, const T* __restrict__ x, T* __restrict__ y)
+k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, int* __restrict__ ctr, const int* __restrict__ rp,
+            const int* __restrict__ ci, const T* __restrict__ va, const T* __restrict__ x, T* __restrict__ y)
 {
     __shared__ T s_a[kBlock / 32][kWarpNnz];
     __shared__ T s_x[kBlock / 32][kWarpNnz];
     __shared__ int s_rp[kBlock / 32][kWarpNnz + 1];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int gw = blockIdx.x * (blockDim.x >> 5) + wib, nwarps = gridDim.x * (blockDim.x >> 5);
     T* sa = s_a[wib];
     T* sx = s_x[wib];
     int* srp = s_rp[wib];
-    for (int t = gw; t < ntasks; t += nwarps) {
-        const WarpTask task = tasks[t];
+    auto grab = [&]() {
+        int v = 0;
+        if (lane == 0) v = atomicAdd(ctr, 1);
+        return __shfl_sync(0xffffffffu, v, 0);
+    };
+    int t = grab();
+    WarpTask nxt;
+    if (t < ntasks) nxt = tasks[t];
+    while (t < ntasks) {
+        const WarpTask task = nxt;
+        t = grab();
+        if (t < ntasks) nxt = tasks[t];
         const int k0 = task.nnz_begin, k1 = task.nnz_end;
         if (task.row_end - task.row_begin == 1 && k1 - k0 > kWarpNnz) {
             T acc = T(0);
             for (int kb = k0; kb < k1; kb += 32 * 8) {
-                T xv[8], av[8];
+                int cc[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
                     const int k = kb + lane + 32 * u;
-                    if (k < k1) { av[u] = va[k]; xv[u] = x[ci[k]]; }
+                    if (k < k1) {
+                        cc[u] = __ldg(ci + k);
+                        cp_async_elem<sizeof(T)>(sa + lane + 32 * u, va + k);
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < 8; ++u)
-                    if (kb + lane + 32 * u < k1) acc = mac(acc, av[u], xv[u]);
+                    if (kb + lane + 32 * u < k1) cp_async_elem<sizeof(T)>(sx + lane + 32 * u, x + cc[u]);
+                cp_async_drain_warp();
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (kb + lane + 32 * u < k1) acc = mac(acc, sa[lane + 32 * u], sx[lane + 32 * u]);
+                __syncwarp();   // the buffers are refilled by the next 256 entries
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
@@ -611,31 +649,41 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restric
             }
             continue;
         }
-        T xv[8], av[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int k = k0 + lane + 32 * u;
-            if (k < k1) { av[u] = va[k]; xv[u] = x[ci[k]]; }
-        }
         const int nr = task.row_end - task.row_begin;
-        for (int r = lane; r <= nr; r += 32) srp[r] = rp[task.row_begin + r] - k0;
+        int cc[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int k = k0 + lane + 32 * u;
-            if (k < k1) { sa[lane + 32 * u] = av[u]; sx[lane + 32 * u] = xv[u]; }
+            if (k < k1) {
+                cc[u] = __ldg(ci + k);
+                cp_async_elem<sizeof(T)>(sa + lane + 32 * u, va + k);
+            }
         }
-        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < 9; ++u) {
+            const int r = lane + 32 * u;
+            if (r <= nr) cp_async_elem<4>(srp + r, rp + task.row_begin + r);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (k0 + lane + 32 * u < k1) cp_async_elem<sizeof(T)>(sx + lane + 32 * u, x + cc[u]);
+        cp_async_drain_warp();
         // rows of up to kSeqRow entries: one lane each, summed sequentially
         // (bitwise the sequential row sum); longer rows: the whole warp,
         // lane-strided partial sums and a fixed shuffle tree, so no lane
         // walks a long row alone while the others wait
         for (int base = 0; base < nr; base += 32) {
             const int r = base + lane;
-            const bool seq = r < nr && srp[r + 1] - srp[r] <= kSeqRow;
+            int a = 0, e = 0;
+            if (r < nr) {
+                a = srp[r] - k0;
+                e = srp[r + 1] - k0;
+            }
+            const bool seq = r < nr && e - a <= kSeqRow;
             if (seq) {
                 T acc = T(0);
-                const int q = fused_tail(srp[r], srp[r + 1]);
-                for (int e = srp[r]; e < srp[r + 1]; ++e) acc = row_step(acc, sa[e], sx[e], e >= q);
+                const int q = fused_tail(a, e);
+                for (int j = a; j < e; ++j) acc = row_step(acc, sa[j], sx[j], j >= q);
                 const int row = task.row_begin + r;
                 const T yb = (ASG == ASG_SET) ? T(0) : y[row];
                 y[row] = assign_out<T, ASG>(yb, acc);
@@ -645,7 +693,8 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restric
                 const int rr = base + __ffs(lng) - 1;
                 lng &= lng - 1;
                 T acc = T(0);
-                for (int e = srp[rr] + lane; e < srp[rr + 1]; e += 32) acc = mac(acc, sa[e], sx[e]);
+                const int ra = srp[rr] - k0, re = srp[rr + 1] - k0;
+                for (int j = ra + lane; j < re; j += 32) acc = mac(acc, sa[j], sx[j]);
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
                 if (lane == 0) {
@@ -656,6 +705,15 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, const int* __restric
             }
         }
         __syncwarp();
+    }
+    // self-reset: the last warp out zeroes the task counter and itself
+    if (lane == 0) {
+        const int nw = gridDim.x * (blockDim.x >> 5);
+        if (atomicAdd(ctr + 1, 1) == nw - 1) {
+            ctr[0] = 0;
+            ctr[1] = 0;
+            __threadfence();
+        }
     }
 }
 

@@ -146,10 +146,15 @@ class pc:
     class _base:
         kind = _lib.PC_IDENTITY
 
-        def __init__(self, A: compressed2D, value=np.float64):
+        def __init__(self, A: compressed2D, value=np.float64, tune: bool = True):
             self.A = A
             self.ctx = A.ctx
             self.value = np.dtype(value)
+            if tune and self.kind in (_lib.PC_ILU0, _lib.PC_IC0) and self.ctx.autotune is not None:
+                from . import autotune, mtl
+                name = "ilu_0" if self.kind == _lib.PC_ILU0 else "ic_0"
+                mtl.tuned(A, ("pc", name, self.value.name),
+                          lambda ctx, Ad, cache: autotune.tune_pc(ctx, Ad, name, self.value, cache))
             h = C.c_void_p()
             st = _lib.F64 if self.value == np.float64 else _lib.F32
             check(self.ctx._L.mtlg_pc_create(self.ctx.h, A.h, self.kind, st, C.byref(h)), type(self).__name__)
@@ -221,10 +226,12 @@ def adjoint_solve(P: pc._base, x: dense_vector, y: dense_vector | None = None) -
     return y
 
 
-def _solve(kind, A, x, b, L, R, it: basic_iteration, restart=0) -> int:
+def _solve(kind, A, x, b, L, R, it: basic_iteration, restart=0, tune=True) -> int:
     from .mtl import poisson2D_dirichlet
     if isinstance(A, poisson2D_dirichlet):
         return _solve_poisson(kind, A, x, b, it, restart)
+    if tune and A.ctx.autotune is not None:
+        _tune_vec(A)
     res = _lib.IterResult()
     params = it._params(restart)
     logged = getattr(it, "wants_log", False)
@@ -243,8 +250,18 @@ def _solve(kind, A, x, b, L, R, it: basic_iteration, restart=0) -> int:
             it.error, it._resid = err, resid
     else:
         it._take(res)
-    check(st, ["cg", "bicgstab", "gmres"][kind])
+    check(st, _SOLVER_NAME.get(kind, "solve"))
     return it.error_code()
+
+
+_SOLVER_NAME = {_lib.CG: "cg", _lib.BICGSTAB: "bicgstab", _lib.GMRES: "gmres", _lib.BICG: "bicg", _lib.CGS: "cgs",
+                _lib.TFQMR: "tfqmr", _lib.QMR: "qmr", _lib.BICGSTAB_2: "bicgstab_2",
+                _lib.BICGSTAB_ELL: "bicgstab_ell", _lib.IDR_S: "idr_s"}
+
+
+def _tune_vec(A):
+    from . import autotune, mtl
+    mtl.tuned(A, "vec", lambda ctx, Ad, cache: autotune.tune_vec(ctx, Ad, np.float64, cache))
 
 
 def _solve_poisson(kind, A, x, b, it: basic_iteration, restart=0) -> int:
@@ -258,8 +275,8 @@ def _solve_poisson(kind, A, x, b, it: basic_iteration, restart=0) -> int:
     return it.error_code()
 
 
-def cg(A, x, b, P, it: basic_iteration) -> int:
-    return _solve(_lib.CG, A, x, b, P, None, it)
+def cg(A, x, b, P, it: basic_iteration, tune: bool = True) -> int:
+    return _solve(_lib.CG, A, x, b, P, None, it, tune=tune)
 
 
 def bicgstab(A, x, b, P, it: basic_iteration) -> int:
@@ -307,6 +324,8 @@ def refine(solver: str, A: compressed2D, x: dense_vector, b: dense_vector, P, rt
     ill-conditioned for FP32) or the inner solve breaks down, the system is
     finished by a plain FP64 solve (it.fp64_fallback is then True)."""
     kind = {"cg": _lib.CG, "bicgstab": _lib.BICGSTAB}[solver]
+    if A.ctx.autotune is not None:
+        _tune_vec(A)
     rp = _lib.RefineParams(int(max_outer), int(max_inner), 0, 0, float(rtol), float(inner_rtol))
     res = _lib.IterResult()
     st = A.ctx._L.mtlg_refine_solve(A.ctx.h, kind, A.h, P.h if P is not None else None, x.h, b.h, C.byref(rp),

@@ -28,6 +28,20 @@ class context:
         check(self._L.mtlg_ctx_create(device, hbm_budget, C.byref(h)), "ctx_create")
         self.h = h
         self.device = device
+        self.autotune = None   # autotune.Cache when launch shapes are tuned per operator class
+
+    def enable_autotune(self, cache=None):
+        """Tunes launch shapes per operator class from now on: preconditioner
+        set-ups take the chunked-sweep settings of their operator, solves the
+        vector-pass setting and mult the SpMV kernel (measured once per class,
+        then read from `cache`, an autotune.Cache or a path)."""
+        from . import autotune
+        if cache is None or isinstance(cache, (str, bytes)) or hasattr(cache, "__fspath__"):
+            cache = autotune.Cache(cache) if cache is not None else autotune.Cache()
+        self.autotune = cache
+
+    def disable_autotune(self):
+        self.autotune = None
 
     def synchronize(self):
         check(self._L.mtlg_ctx_synchronize(self.h), "synchronize")
@@ -112,6 +126,8 @@ class compressed2D:
         self.h = h
         self.shape = (n_rows, n_cols)
         self.nnz = int(rp[-1])
+        self.host_row_ptr = rp   # for the autotuner's operator key
+        self._tuned = {}
 
     @classmethod
     def from_problem(cls, A, ctx: context | None = None) -> "compressed2D":
@@ -129,6 +145,8 @@ class compressed2D:
         check(self.ctx._L.mtlg_csr_info(h, C.byref(nr), C.byref(nc), C.byref(nz)), "csr_info")
         self.shape = (nr.value, nc.value)
         self.nnz = nz.value
+        self.host_row_ptr = None
+        self._tuned = {}
         return self
 
     def num_rows(self) -> int:
@@ -350,9 +368,27 @@ class poisson2D_dirichlet:
         return _MatVec(self, v)
 
 
-def mult(A, x: dense_vector, y: dense_vector, assign: str = "="):
+def tuned(A, what: str, tune):
+    """Applies the autotuned settings `what` of device matrix A (measured on
+    first use per operator class; kept on A) when its context tunes."""
+    ctx = A.ctx
+    if ctx.autotune is None or not isinstance(A, compressed2D):
+        return
+    from . import autotune
+    key = what if isinstance(what, str) else tuple(what)
+    choice = A._tuned.get(key)
+    if choice is None:
+        choice = tune(ctx, A, ctx.autotune)[0]
+        A._tuned[key] = choice
+    autotune.apply_settings(ctx, choice)
+
+
+def mult(A, x: dense_vector, y: dense_vector, assign: str = "=", tune: bool = True):
     """y = A x, y += A x or y -= A x (A: compressed2D, ell_matrix or
     sparse_banded)."""
+    if tune and isinstance(A, compressed2D) and A.ctx.autotune is not None:
+        from . import autotune
+        tuned(A, "spmv", lambda ctx, Ad, cache: autotune.tune_spmv(ctx, Ad, cache))
     if isinstance(A, poisson2D_dirichlet):
         check(A.ctx._L.mtlg_poisson2d_spmv(A.ctx.h, A.m, A.n, x.h, y.h, _ASSIGN[assign]), "mult")
     elif isinstance(A, ell_matrix):

@@ -51,6 +51,7 @@ class batch:
         check(self.ctx._L.mtlg_batch_create(self.ctx.h, C.byref(h)), "batch_create")
         self.h = h
         self.sizes = []
+        self.systems = []   # (A, solver, pc) of each system, for tune=True
 
     def add(self, A, b, solver="cg", pc="ic_0", max_iter=2000, rtol=1e-8, atol=0.0) -> int:
         rp = np.ascontiguousarray(A.row_ptr, np.int64)
@@ -62,12 +63,29 @@ class batch:
         check(self.ctx._L.mtlg_batch_add(self.h, A.n_rows, A.nnz, _p(rp), _p(ci), _p(v), _p(bb), _SOLVER[solver],
                                          _PC[pc], C.byref(prm), C.byref(idx)), "batch_add")
         self.sizes.append(A.n_rows)
+        self.systems.append((A, solver, pc))
         return idx.value
 
     def solve(self, mixed: bool = False, rtol: float = 1e-8, inner_rtol: float = 1e-4, max_outer: int = 20,
-              max_inner: int = 2000):
+              max_inner: int = 2000, tune=False):
+        """Solves every system.  tune: True (or an autotune.Cache) first sets
+        the context's batched-pass knobs for this set of systems (measured on
+        a sample of them once per class, then cached)."""
+        if tune:
+            self.tune(mixed, cache=None if tune is True else tune)
         rp = _lib.RefineParams(int(max_outer), int(max_inner), 0, 0, float(rtol), float(inner_rtol))
         check(self.ctx._L.mtlg_batch_solve(self.h, _lib.F32 if mixed else _lib.F64, C.byref(rp)), "batch_solve")
+
+    def tune(self, mixed: bool = False, cache=None):
+        from . import autotune
+        if not self.systems:
+            return None
+        kinds = {}
+        for _, so, pc in self.systems:
+            kinds[(so, pc)] = kinds.get((so, pc), 0) + 1
+        solver, pc = max(kinds, key=kinds.get)
+        cache = cache or self.ctx.autotune or autotune.Cache()
+        return autotune.tune_batch(self.ctx, [A for A, _, _ in self.systems], solver, pc, mixed, cache=cache)[0]
 
     def result(self, i: int) -> Result:
         x = np.empty(self.sizes[i])
@@ -96,6 +114,22 @@ class server:
         check(self.ctx._L.mtlg_server_create(self.ctx.h, C.byref(o), C.byref(h)), "server_create")
         self.h = h
         self.n = {}
+        self.mixed = mixed
+
+    def tune(self, requests, cache=None):
+        """Sets the context's batched-pass knobs for requests like these
+        ((A, b, solver, pc) tuples; measured on a sample once per class, then
+        cached).  Call before the requests are submitted."""
+        from . import autotune
+        reqs = list(requests)
+        if not reqs:
+            return None
+        kinds = {}
+        for r in reqs:
+            kinds[(r[2], r[3])] = kinds.get((r[2], r[3]), 0) + 1
+        solver, pc = max(kinds, key=kinds.get)
+        cache = cache or self.ctx.autotune or autotune.Cache()
+        return autotune.tune_batch(self.ctx, [r[0] for r in reqs], solver, pc, self.mixed, cache=cache)[0]
 
     def submit(self, A, b, solver="cg", pc="ic_0", max_iter=2000) -> int:
         rp = np.ascontiguousarray(A.row_ptr, np.int64)

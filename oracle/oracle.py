@@ -67,6 +67,7 @@ def ref_lib(omp: bool = False) -> C.CDLL:
         L.mtlref_two_norm.argtypes = [C.c_int64, VP]
         L.mtlref_pc_apply.argtypes = [VP, C.c_int, C.c_int, VP, VP]
         L.mtlref_pc_apply_f32.argtypes = [VP, C.c_int, VP, VP]
+        L.mtlref_pc_adjoint_apply.argtypes = [VP, C.c_int, C.c_int, VP, VP]
         PI = C.POINTER(C.c_int64)
         L.mtlref_pc_factors.argtypes = [VP, C.c_int, PI, VP, VP, VP, PI, VP, VP, VP]
         L.mtlref_solve.argtypes = [VP, C.c_int, C.c_int, C.c_int, VP, VP, C.c_int, C.c_double, C.c_double, C.c_int,
@@ -178,6 +179,13 @@ class RefMatrix:
         else:
             y = np.zeros(self.A.n_rows)
             self.L.mtlref_pc_apply(self.h, PC_KIND[kind], int(storage_f32), _p(x), _p(y))
+        return y
+
+    def pc_adjoint_apply(self, kind, x, storage_f32=False):
+        y = np.zeros(self.A.n_rows)
+        if self.L.mtlref_pc_adjoint_apply(self.h, PC_KIND[kind], int(storage_f32),
+                                          _p(np.ascontiguousarray(x, np.float64)), _p(y)) != 0:
+            raise ValueError(f"no adjoint apply for {kind}")
         return y
 
     def factors(self, kind):

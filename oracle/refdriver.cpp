@@ -243,6 +243,19 @@ int mtlref_pc_apply(void* p, int kind, int pc_f32, const double* x, double* y)
     return 0;
 }
 
+/// y = adjoint_solve(P, x) of pc::ilu_0<M> / pc::ilu_0<M, float>
+/// (itl/pc/ilu.hpp:94-115): U^H then L^H through the transposed views.
+int mtlref_pc_adjoint_apply(void* p, int kind, int pc_f32, const double* x, double* y)
+{
+    RefCsr* h = static_cast<RefCsr*>(p);
+    const dmat& A = *h->A;
+    dvec vx(h->n_rows, const_cast<double*>(x)), vy(h->n_rows, y);
+    if (kind != 2) return -1;
+    if (pc_f32) { itl::pc::ilu_0<dmat, float> P(A); vy = adjoint_solve(P, vx); }
+    else { itl::pc::ilu_0<dmat> P(A); vy = adjoint_solve(P, vx); }
+    return 0;
+}
+
 /// FP32 vectors through a preconditioner factorized from the FP64 matrix
 /// and stored in FP32 (pc::ilu_0<M,float> / pc::ic_0<M,float>).
 int mtlref_pc_apply_f32(void* p, int kind, const float* x, float* y)

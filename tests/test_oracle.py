@@ -223,6 +223,24 @@ def test_port_gmres_restatement_converges():
 
 # ---------------------------------------------------------------- reference build
 @pytest.mark.ref
+def test_reference_ilu0_adjoint_solves_the_transposed_system(need_ref):
+    # adjoint_solve(P, x) of pc::ilu_0 (itl/pc/ilu.hpp:104-115): (L U)^T y = x
+    # with L unit lower and U stored with its inverted diagonal
+    import scipy.sparse as sp
+    A, _, _ = P.config2_solve(6)
+    R = need_ref.RefMatrix(A)
+    (Lrp, Lci, Lv), (Urp, Uci, Uv) = R.factors("ilu_0")
+    n = A.n_rows
+    Ld = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n)).toarray()
+    Ud = sp.csr_matrix((Uv, Uci, Urp), shape=(n, n)).toarray()
+    Ld = Ld - np.diag(np.diag(Ld)) + np.eye(n)
+    Ud = Ud - np.diag(np.diag(Ud)) + np.diag(1.0 / np.diag(Ud))
+    x = np.random.default_rng(0).standard_normal(n)
+    y = R.pc_adjoint_apply("ilu_0", x)
+    assert np.abs((Ld @ Ud).T @ y - x).max() <= 1e-13 * np.abs(x).max() * n
+
+
+@pytest.mark.ref
 def test_port_equals_reference_build(need_ref):
     A = P.convdiff_3d(10)
     R = need_ref.RefMatrix(A)
