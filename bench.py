@@ -543,6 +543,18 @@ def main():
     spmv_s = e0.elapsed_time(e1) * 1e-3 / reps
     spmv_bytes = 12 * Q.nnz + 4 * (Q.n_rows + 1) + 8 * Q.n_rows + 8 * Q.n_rows
     spmv_gbs = spmv_bytes / spmv_s / 1e9
+    # the memory floor of any SpMV on this matrix: values + columns streamed
+    # and one x gather per entry, no rows (uniformly random columns: every
+    # gather is its own 32-byte sector)
+    for _ in range(3):
+        mtl.gather_floor(Qd, xq)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        mtl.gather_floor(Qd, xq)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    floor_s = e0.elapsed_time(e1) * 1e-3 / reps
     del Qd, xq, yq
 
     extra = {}
@@ -574,7 +586,9 @@ def main():
                         "x_bitwise_equal_to_reference_build": oracle_bitwise},
         "mixed_over_fp64": value / v64,
         "spmv": {"matrix": f"power-law CSR {Q.n_rows} rows, {Q.nnz} nnz", "us": spmv_s * 1e6, "GBs": spmv_gbs,
-                 "frac_measured_peak": spmv_gbs / peak, "frac_8TBs_nominal": spmv_gbs / 8000.0},
+                 "frac_measured_peak": spmv_gbs / peak, "frac_8TBs_nominal": spmv_gbs / 8000.0,
+                 "gather_floor_us": floor_s * 1e6, "gather_floor_GBs": spmv_bytes / floor_s / 1e9,
+                 "frac_of_gather_floor": floor_s / spmv_s},
         "roofline": {"kernel": "k_sweep_chunk<float,float> (ILU(0) L and U sweeps, one apply)", "bound": "hbm",
                      "achieved": sweep_gbs, "peak": peak, "unit": "GB/s", "frac": sweep_gbs / peak,
                      "peak_kind": peak_kind, "traffic": TRAFFIC_PER_APPLY,

@@ -290,6 +290,11 @@ int mtlg_spmv_dot(mtlg_ctx* ctx, mtlg_csr* A, const mtlg_vec* p, mtlg_vec* q, do
  * stream capture. */
 int mtlg_spmv_dot_noalloc(int64_t n_rows, int64_t n_cols, const int32_t* row_ptr, const int32_t* col,
                           const double* val, const double* p, double* q, double* dot, void* stream);
+/* Roofline probe (no reference counterpart): one pass that streams A's FP64
+ * values and columns and gathers x[col] for every entry, without the row
+ * structure -- the memory-system floor of any y = A x on A, to time beside
+ * mtlg_spmv.  Partial sums land in a device scratch array of A. */
+int mtlg_spmv_gather_floor(mtlg_ctx* ctx, mtlg_csr* A, const mtlg_vec* x);
 int mtlg_dot(mtlg_ctx* ctx, const mtlg_vec* x, const mtlg_vec* y, double* out);
 int mtlg_two_norm(mtlg_ctx* ctx, const mtlg_vec* x, double* out);
 /* y += a x */

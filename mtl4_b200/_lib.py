@@ -103,6 +103,7 @@ SIGNATURES = {
     "mtlg_spmv": (C.c_int, [VP, VP, VP, VP, C.c_int]),
     "mtlg_spmv_dot": (C.c_int, [VP, VP, VP, VP, PDBL]),
     "mtlg_spmv_dot_noalloc": (C.c_int, [I64, I64, VP, VP, VP, VP, VP, VP, VP]),
+    "mtlg_spmv_gather_floor": (C.c_int, [VP, VP, VP]),
     "mtlg_dot": (C.c_int, [VP, VP, VP, PDBL]),
     "mtlg_two_norm": (C.c_int, [VP, VP, PDBL]),
     "mtlg_axpy": (C.c_int, [VP, C.c_double, VP, VP]),

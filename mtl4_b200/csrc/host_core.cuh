@@ -11,6 +11,49 @@
 #include <memory>
 #include <mutex>
 
+// Host-to-device copies of large host arrays through pinned staging blocks:
+// a pageable cudaMemcpyAsync copies at a few GB/s and holds the calling
+// thread; here the thread copies into a pinned block (a memcpy) and the DMA
+// engine drains it while the thread fills the next one.  A block is reused
+// once the copy recorded on its event has finished.
+struct PinnedStage {
+    static constexpr size_t kBlockBytes = size_t(8) << 20;
+    static constexpr int kBlocks = 8;
+    std::mutex init_mu;
+    bool ready = false, failed = false;
+    unsigned char* blk[kBlocks] = {};
+    cudaEvent_t ev[kBlocks] = {};
+    std::mutex mu[kBlocks];
+    std::atomic<unsigned> next{0};
+    bool init()
+    {
+        std::lock_guard<std::mutex> lk(init_mu);
+        if (ready || failed) return ready;
+        for (int i = 0; i < kBlocks; ++i) {
+            if (cudaHostAlloc(reinterpret_cast<void**>(&blk[i]), kBlockBytes, cudaHostAllocDefault) != cudaSuccess ||
+                cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                release();
+                failed = true;
+                return false;
+            }
+        }
+        ready = true;
+        return true;
+    }
+    void release()
+    {
+        for (int i = 0; i < kBlocks; ++i) {
+            if (ev[i]) cudaEventSynchronize(ev[i]), cudaEventDestroy(ev[i]);
+            if (blk[i]) cudaFreeHost(blk[i]);
+            ev[i] = nullptr;
+            blk[i] = nullptr;
+        }
+        ready = false;
+    }
+    ~PinnedStage() { release(); }
+};
+
 struct mtlg_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
@@ -41,6 +84,7 @@ struct mtlg_ctx {
     int log_n = 0;                        // tests of the last logged solve (CG / BiCGSTAB)
     int64_t admission_reserve_bytes = -1; // tuning: bytes kept out of admission (-1: max(1 GiB, 2%))
     int* d_scratch_err = nullptr;
+    PinnedStage stage;                    // staging blocks of large uploads
     int sweep_blocks() const
     {
         if (sweep_nblocks > 0) return std::min(sweep_nblocks, sm_count * sweep_max_bpsm);
@@ -120,6 +164,75 @@ inline void parallel_for(int n, F&& f, int threads = 0)
     for (auto& th : pool) th.join();
 }
 
+// Host vectors whose elements are left uninitialized on resize (the large
+// set-up arrays are written in full, in parallel, right after sizing: no
+// single-threaded zeroing pass first).
+template <typename T>
+struct uninit_alloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = uninit_alloc<U>;
+    };
+    uninit_alloc() = default;
+    template <typename U>
+    uninit_alloc(const uninit_alloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept { ::new (static_cast<void*>(p)) U; }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
+};
+template <typename T>
+using hvec = std::vector<T, uninit_alloc<T>>;
+
+// out[0] = 0, out[i + 1] = out[i] + len(i) for i < n, in parallel blocks
+// (block sums, their prefix, then each block's own prefix).
+template <typename Len>
+inline void parallel_prefix(int n, Len&& len, int* out)
+{
+    constexpr int kBlk = 1 << 16;
+    const int nb = (n + kBlk - 1) / kBlk;
+    std::vector<long long> bsum(size_t(nb) + 1, 0);
+    parallel_for(nb, [&](int b) {
+        long long t = 0;
+        for (int i = b * kBlk; i < std::min(n, (b + 1) * kBlk); ++i) t += len(i);
+        bsum[size_t(b) + 1] = t;
+    });
+    for (int b = 0; b < nb; ++b) bsum[size_t(b) + 1] += bsum[size_t(b)];
+    out[0] = 0;
+    parallel_for(nb, [&](int b) {
+        long long t = bsum[size_t(b)];
+        for (int i = b * kBlk; i < std::min(n, (b + 1) * kBlk); ++i) {
+            t += len(i);
+            out[i + 1] = int(t);
+        }
+    });
+}
+
+// Host -> device copy on the context's stream; arrays of 1 MiB and more go
+// through the pinned staging blocks (not while the stream is capturing a
+// graph: a captured copy would replay from a reused block).
+inline int upload_bytes(mtlg_ctx* c, void* dst, const void* src, size_t bytes)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(c->stream, &cs);
+    if (bytes < (size_t(1) << 20) || cs != cudaStreamCaptureStatusNone || !c->stage.init()) {
+        MTLG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+        return MTLG_OK;
+    }
+    PinnedStage& S = c->stage;
+    for (size_t off = 0; off < bytes; off += PinnedStage::kBlockBytes) {
+        const size_t piece = std::min(PinnedStage::kBlockBytes, bytes - off);
+        const int i = int(S.next++ % PinnedStage::kBlocks);
+        std::lock_guard<std::mutex> lk(S.mu[i]);
+        MTLG_CUDA(cudaEventSynchronize(S.ev[i]));
+        memcpy(S.blk[i], static_cast<const unsigned char*>(src) + off, piece);
+        MTLG_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, S.blk[i], piece, cudaMemcpyHostToDevice,
+                                  c->stream));
+        MTLG_CUDA(cudaEventRecord(S.ev[i], c->stream));
+    }
+    return MTLG_OK;
+}
+
 // Typed owning device buffer.
 template <typename T>
 struct DBuf {
@@ -143,7 +256,7 @@ struct DBuf {
     int upload(mtlg_ctx* c, const T* h, size_t count)
     {
         MTLG_TRY(alloc(c, count));
-        if (count) MTLG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+        if (count) MTLG_TRY(upload_bytes(c, p, h, count * sizeof(T)));
         return MTLG_OK;
     }
     void release()
@@ -252,6 +365,7 @@ struct mtlg_csr {
     std::vector<WarpTask> wtasks;  // row-aligned warp tasks (irregular matrices)
     DBuf<WarpTask> d_wtasks;
     DBuf<int> wctr;                // k_spmv_rows task counter and exit count (self-resetting)
+    DBuf<double> probe;            // k_gather_floor partial sums
     bool irregular = false;        // some row longer than kShortRow entries
     // single-system operation set (standalone SpMV / dot)
     DBuf<Tile> d_tiles;

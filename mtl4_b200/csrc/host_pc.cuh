@@ -17,9 +17,9 @@ struct RowLists {
 struct TriDev {
     int n = 0, npad = 0, nnz = 0, nlev = 0;
     bool lower = true;
-    std::vector<int> h_row_of;         // npad
-    std::vector<int> h_rp;             // npad + 1
-    std::vector<int> h_ci, h_src, h_mul;
+    hvec<int> h_row_of;                // npad
+    hvec<int> h_rp;                    // npad + 1
+    hvec<int> h_ci, h_src, h_mul;
     std::vector<int> lev_task_begin;   // nlev + 1, in units of tasks
     DBuf<int> row_of, rp, ci, src, mul;
     DBuf<unsigned char> val, dia;      // storage type S
@@ -78,7 +78,8 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     // rows of each chunk in (level, flat order): a counting sort by level per
     // chunk (rows visited ascending for L, descending for U, so rows of one
     // level keep the flat layout's order), and the largest wave
-    MTLG_TRACE(9153, "pc.chunk_order");
+    TracePhases ph;
+    ph.next(9153, "pc.chunk_order");
     std::vector<int> order(size_t(n), 0);
     std::vector<int> cbeg(nch + 1, 0);
     for (int p = 0; p < nch; ++p) {
@@ -122,7 +123,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     // kept as row ids (cext) or -(row + 2) (overflow codes) until every
     // chunk's position is known.  A chunk's arrays start 4-aligned in the
     // concatenation (its first segment opens 4-aligned).
-    MTLG_TRACE(9154, "pc.chunk_waves");
+    ph.next(9154, "pc.chunk_waves");
     struct ChunkLocal {
         std::vector<unsigned> wv;
         std::vector<int> crow, ccol, csrc, cmul, cext;
@@ -221,6 +222,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     });
     // concatenation: chunk bases, then the arrays with row ids turned into
     // positions (every earlier chunk's position is known now)
+    ph.next(9157, "pc.chunk_concat");
     std::vector<size_t> bw(nch), bp(nch), be(nch), bx(nch), bs(nch);
     size_t sw = 0, sp = 0, se = 0, sx = 0, ss = 0;
     std::vector<int> cpbeg(size_t(nch) + 1, 0);   // first position of each chunk (and the end)
@@ -240,8 +242,23 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         cseg[p + 1] = int(bs[p] + loc[size_t(p)].segs.size());
         cxr[p + 1] = int(bx[p] + loc[size_t(p)].cext.size());
     }
-    std::vector<unsigned> wv(sw, 0u);
-    std::vector<int> crow(sp, -1), ccol(se, -1), csrc(se, 0), cmul(se, -1), cext(sx, -1);
+    // capacities include the 16-byte tails added at the end (no
+    // reallocation); every element is written by the parallel copy below
+    // (chunk data, then the alignment gap up to the next chunk's base)
+    const size_t tw = size_t(round4(int(sw))) + 4, tp = size_t(round4(int(sp))) + 4;
+    const size_t te = size_t(round4(int(se))) + 4, tx = sx + 4;
+    hvec<unsigned> wv;
+    hvec<int> crow, ccol, csrc, cmul, cext;
+    wv.reserve(tw);
+    wv.resize(sw);
+    crow.reserve(tp);
+    crow.resize(sp);
+    for (hvec<int>* v : {&ccol, &csrc, &cmul}) {
+        v->reserve(te);
+        v->resize(se);
+    }
+    cext.reserve(tx);
+    cext.resize(sx);
     std::vector<SegRec> segs(ss);
     auto pos_of = [&](int row) {
         const int ch = row / B;
@@ -250,14 +267,21 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     };
     parallel_for(nch, [&](int p) {
         const ChunkLocal& L = loc[size_t(p)];
+        const bool last = p + 1 == nch;
         std::copy(L.wv.begin(), L.wv.end(), wv.begin() + bw[p]);
+        std::fill(wv.begin() + bw[p] + L.wv.size(), last ? wv.end() : wv.begin() + bw[p + 1], 0u);
         std::copy(L.crow.begin(), L.crow.end(), crow.begin() + bp[p]);
+        std::fill(crow.begin() + bp[p] + L.crow.size(), last ? crow.end() : crow.begin() + bp[p + 1], -1);
         for (size_t k = 0; k < L.ccol.size(); ++k) {
             const int v = L.ccol[k];
             ccol[be[p] + k] = v <= -2 ? -(pos_of(-v - 2) + 2) : v;
         }
         std::copy(L.csrc.begin(), L.csrc.end(), csrc.begin() + be[p]);
         std::copy(L.cmul.begin(), L.cmul.end(), cmul.begin() + be[p]);
+        const size_t ge = last ? ccol.size() : be[p + 1];
+        std::fill(ccol.begin() + be[p] + L.ccol.size(), ccol.begin() + ge, -1);
+        std::fill(csrc.begin() + be[p] + L.ccol.size(), csrc.begin() + ge, 0);
+        std::fill(cmul.begin() + be[p] + L.ccol.size(), cmul.begin() + ge, -1);
         for (size_t k = 0; k < L.cext.size(); ++k) cext[bx[p] + k] = L.cext[k] >= 0 ? pos_of(L.cext[k]) : -1;
         for (size_t k = 0; k < L.segs.size(); ++k) {
             SegRec g = L.segs[k];
@@ -268,12 +292,14 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         }
     });
     loc.clear();
-    MTLG_TRACE(9155, "pc.chunk_pushes");
+    ph.next(9155, "pc.chunk_pushes");
     // pushes: a row of chunk p - 1 fills the first slot of chunk p that reads
     // it (when the two chunks run in neighbouring CTAs of a cluster); the
     // receivers fetch the other slots
     // (chunk p writes only positions of chunk p - 1: chunks run in parallel)
-    std::vector<int> cpush(crow.size(), -1);
+    std::vector<int> cpush;
+    cpush.reserve(tp);
+    cpush.assign(crow.size(), -1);
     std::vector<char> pushed(cext.size(), 0);
     parallel_for(nch - 1, [&](int pm) {
         const int p = pm + 1;
@@ -308,6 +334,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
         cquad[q] = make_int2(vec && mask ? p : -1, mask);
     }
     });
+    ph.next(9158, "pc.chunk_tails");
     // tails: a staged copy rounds each array's segment up to 16 bytes
     wv.resize(round4(int(wv.size())) + 4, 0u);
     crow.resize(round4(int(crow.size())) + 4, -1);
@@ -327,7 +354,7 @@ inline int build_chunks(mtlg_ctx* c, const RowLists& F, const std::vector<int>& 
     T.threads = NT;
     T.seg_rows = SR;
     T.seg_ents = SE;
-    MTLG_TRACE(9156, "pc.chunk_upload");
+    ph.next(9156, "pc.chunk_upload");
     MTLG_TRY(T.cseg.upload(c, cseg.data(), cseg.size()));
     MTLG_TRY(T.cxr.upload(c, cxr.data(), cxr.size()));
     MTLG_TRY(T.cext.upload(c, cext.data(), cext.size()));
@@ -691,7 +718,8 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
         MTLG_TRACE(9150, "pc.levels");
         compute_levels(F, n, lower, lev, T.nlev);
     }
-    MTLG_TRACE(9151, "pc.flat_layout");
+    TracePhases ph;
+    ph.next(9151, "pc.flat_layout");
     std::vector<int> cnt(T.nlev + 1, 0);
     for (int i = 0; i < n; ++i) cnt[lev[i]]++;
     // padded level starts
@@ -703,19 +731,51 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
         T.lev_task_begin[l + 1] = T.lev_task_begin[l] + padded / kSweepRows;
     }
     T.npad = start[T.nlev];
-    T.h_row_of.assign(T.npad, -1);
-    std::vector<int> fill(start.begin(), start.end() - 1);
-    // rows ascending within a level (lower) / descending (upper)
-    if (lower) {
-        for (int i = 0; i < n; ++i) T.h_row_of[fill[lev[i]]++] = i;
+    T.h_row_of.resize(T.npad);
+    // rows ascending within a level (lower) / descending (upper): a counting
+    // sort by level; with few levels, blocks of rows scatter in parallel
+    // (per-block offsets per level keep the sequential order)
+    constexpr int kSortBlk = 1 << 16;
+    const int nsb = (n + kSortBlk - 1) / kSortBlk;
+    parallel_for(T.nlev, [&](int l) {
+        for (int k = start[l] + cnt[l]; k < start[l + 1]; ++k) T.h_row_of[k] = -1;   // level padding
+    });
+    if (nsb > 1 && size_t(nsb) * size_t(T.nlev) <= (size_t(1) << 22)) {
+        std::vector<int> bc(size_t(nsb) * T.nlev, 0);
+        // block b of the visiting order (ascending rows for L, descending for U)
+        auto row_at = [&](int v) { return lower ? v : n - 1 - v; };
+        parallel_for(nsb, [&](int b) {
+            int* c0 = bc.data() + size_t(b) * T.nlev;
+            for (int v = b * kSortBlk; v < std::min(n, (b + 1) * kSortBlk); ++v) c0[lev[row_at(v)]]++;
+        });
+        parallel_for(T.nlev, [&](int l) {
+            int o = start[l];
+            for (int b = 0; b < nsb; ++b) {
+                const int t = bc[size_t(b) * T.nlev + l];
+                bc[size_t(b) * T.nlev + l] = o;
+                o += t;
+            }
+        });
+        parallel_for(nsb, [&](int b) {
+            int* c0 = bc.data() + size_t(b) * T.nlev;
+            for (int v = b * kSortBlk; v < std::min(n, (b + 1) * kSortBlk); ++v) {
+                const int r = row_at(v);
+                T.h_row_of[c0[lev[r]]++] = r;
+            }
+        });
     } else {
-        for (int i = n - 1; i >= 0; --i) T.h_row_of[fill[lev[i]]++] = i;
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        if (lower) {
+            for (int i = 0; i < n; ++i) T.h_row_of[fill[lev[i]]++] = i;
+        } else {
+            for (int i = n - 1; i >= 0; --i) T.h_row_of[fill[lev[i]]++] = i;
+        }
     }
-    T.h_rp.assign(T.npad + 1, 0);
-    for (int k = 0; k < T.npad; ++k) {
+    T.h_rp.resize(size_t(T.npad) + 1);
+    parallel_prefix(T.npad, [&](int k) {
         const int r = T.h_row_of[k];
-        T.h_rp[k + 1] = T.h_rp[k] + (r >= 0 ? F.rp[r + 1] - F.rp[r] : 0);
-    }
+        return r >= 0 ? F.rp[r + 1] - F.rp[r] : 0;
+    }, T.h_rp.data());
     T.nnz = T.h_rp[T.npad];
     T.h_ci.resize(T.nnz);
     T.h_src.resize(T.nnz);
@@ -736,13 +796,14 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
     });
     std::vector<SweepTask> tasks(T.npad / kSweepRows);
     for (size_t t = 0; t < tasks.size(); ++t) tasks[t] = {0, int(t) * kSweepRows};
-    MTLG_TRACE(9152, "pc.flat_upload");
+    ph.next(9152, "pc.flat_upload");
     MTLG_TRY(T.row_of.upload(c, T.h_row_of.data(), T.h_row_of.size()));
     MTLG_TRY(T.rp.upload(c, T.h_rp.data(), T.h_rp.size()));
     MTLG_TRY(T.ci.upload(c, T.h_ci.data(), T.h_ci.size()));
     MTLG_TRY(T.src.upload(c, T.h_src.data(), T.h_src.size()));
     MTLG_TRY(T.mul.upload(c, T.h_mul.data(), T.h_mul.size()));
     MTLG_TRY(T.tasks.upload(c, tasks.data(), tasks.size()));
+    ph.end();
     return build_chunks(c, F, lev, n, lower, chunk_rows, ssz, T);
 }
 
@@ -923,15 +984,16 @@ inline int pc_build(mtlg_pc* P)
         // L = strict_lower(LU) (unit diagonal), U = upper(LU) with the
         // inverted diagonal first (ilu_0.hpp:79-81, ilu.hpp:84-91)
         // row counts, offsets, then the entries (rows in parallel)
-        for (int i = 0; i < n; ++i) {
-            int nl = 0, nu = 0;
-            for (int64_t e = rp[i]; e < rp[i + 1]; ++e) {
-                nl += ci[e] < i;
-                nu += ci[e] > i;
-            }
-            Lr.rp[i + 1] = Lr.rp[i] + nl;
-            Ur.rp[i + 1] = Ur.rp[i] + nu;
-        }
+        parallel_prefix(n, [&](int i) {
+            int nl = 0;
+            for (int64_t e = rp[i]; e < rp[i + 1] && ci[e] < i; ++e) ++nl;
+            return nl;
+        }, Lr.rp.data());
+        parallel_prefix(n, [&](int i) {
+            int nu = 0;
+            for (int64_t e = rp[i + 1] - 1; e >= rp[i] && ci[e] > i; --e) ++nu;
+            return nu;
+        }, Ur.rp.data());
         for (RowLists* R : {&Lr, &Ur}) {
             R->col.resize(size_t(R->rp[n]));
             R->src.resize(size_t(R->rp[n]));

@@ -717,6 +717,30 @@ k_spmv_rows(const WarpTask* __restrict__ tasks, int ntasks, int* __restrict__ ct
     }
 }
 
+// Gather floor of y = A x (a measurement kernel): every entry's value and
+// column are streamed and x[col] gathered, 8 entries in flight per thread,
+// with no row structure; one partial sum per thread.
+__global__ void __launch_bounds__(kBlock) k_gather_floor(long long nnz, const int* __restrict__ ci,
+                                                         const double* __restrict__ va, const double* __restrict__ x,
+                                                         double* __restrict__ out)
+{
+    double acc = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k0 < nnz; k0 += 8 * stride) {
+        int c[8];
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const long long k = k0 + u * stride;
+            c[u] = k < nnz ? __ldg(ci + k) : 0;
+            v[u] = k < nnz ? __ldg(va + k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc = fma(v[u], __ldg(x + c[u]), acc);
+    }
+    out[blockIdx.x * (long long)blockDim.x + threadIdx.x] = acc;
+}
+
 // Thread per row straight from global memory (rows of consecutive threads are
 // adjacent, so a warp's value and column loads stay in the sectors L1 just
 // fetched); gathers issued 8 at a time, summed in storage order.

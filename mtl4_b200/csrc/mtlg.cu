@@ -785,6 +785,20 @@ static int spmv_impl(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, i
     return MTLG_OK;
 }
 
+int mtlg_spmv_gather_floor(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x)
+{
+    MTLG_CHECK_ARG(c && A && x, "null handle");
+    MTLG_CHECK_ARG(x->dtype == MTLG_F64 && x->n == A->n_cols, "x: FP64, n_cols entries");
+    const int grid = c->sm_count * 8;
+    if (!A->probe.p) MTLG_TRY(A->probe.alloc(c, size_t(grid) * kBlock));
+    if (A->nnz == 0) return MTLG_OK;
+    k_gather_floor<<<grid, kBlock, 0, c->stream>>>(A->nnz, A->ci.p, A->v64.p, static_cast<const double*>(x->p),
+                                                   A->probe.p);
+    c->launches++;
+    MTLG_CUDA(cudaGetLastError());
+    return MTLG_OK;
+}
+
 int mtlg_spmv(mtlg_ctx* c, mtlg_csr* A, const mtlg_vec* x, mtlg_vec* y, int assign)
 {
     MTLG_TRACE(3049, "crs_cvec_mult");

@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <optional>
 #include <string>
 
 namespace mtlg {
@@ -81,6 +82,21 @@ class TraceScope {
     const char* name_;
     bool timed_;
     std::chrono::steady_clock::time_point t0_;
+};
+
+// Consecutive phases of one function: next() closes the running phase's
+// scope and opens the next one.
+class TracePhases {
+  public:
+    void next(int id, const char* name)
+    {
+        cur_.reset();
+        cur_.emplace(id, name);
+    }
+    void end() { cur_.reset(); }
+
+  private:
+    std::optional<TraceScope> cur_;
 };
 
 #define MTLG_TRACE_CAT2(a, b) a##b

@@ -399,6 +399,13 @@ def mult(A, x: dense_vector, y: dense_vector, assign: str = "=", tune: bool = Tr
         check(A.ctx._L.mtlg_spmv(A.ctx.h, A.h, x.h, y.h, _ASSIGN[assign]), "mult")
 
 
+def gather_floor(A: compressed2D, x: dense_vector):
+    """Roofline probe: stream A's values and columns and gather x[col] for
+    every entry, without the row structure (the memory floor of mult on A);
+    asynchronous, to be timed by the caller."""
+    check(A.ctx._L.mtlg_spmv_gather_floor(A.ctx.h, A.h, x.h), "gather_floor")
+
+
 def mult_dot(A: compressed2D, p: dense_vector, q: dense_vector) -> float:
     """(q = A p) || (alpha = dot(p, q)) in one pass (cg.hpp:103)."""
     out = C.c_double()
