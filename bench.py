@@ -353,6 +353,7 @@ def run_kernel_case(args):
         A, b, _ = P.config2_solve(128)
         Ad = mtl.compressed2D.from_problem(A, ctx)
         bd = mtl.dense_vector(b, np.float64, ctx)
+        ctx.set_tuning("loop_mode", args.loop_mode)   # 2: no graphs, so profilers see every launch
         for _ in range(args.reps):
             Pc = itl.pc.ilu_0(Ad, np.float32)
             x = mtl.dense_vector(A.n_rows, np.float64, ctx)
@@ -383,6 +384,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the config 3/4/5 samples")
     ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--loop-mode", type=int, default=0, help="--kernel solve_mixed: 0 graphs, 2 direct launches")
     ap.add_argument("--kernel", choices=["spmv_powerlaw", "spmv_stencil", "spmv_lap2048", "sweep_ilu0", "solve_mixed"],
                     help="run one kernel on its bench case a few times and exit (for profilers)")
     ap.add_argument("--reps", type=int, default=3)

@@ -149,7 +149,8 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * overrides the former when > 0), "sweep_sleep_ns" (poll back-off, default
  * 0), "loop_mode" (0: the Krylov loop runs as chunks of 8 iterations in
  * plain CUDA graphs, two in flight; 1: one graph with a WHILE conditional
- * node per solve), "spmv_kernel" (standalone SpMV: 0 chooses by row
+ * node per solve; 2: the loop bodies launched directly, no graph -- for
+ * profilers that do not see kernels inside graphs), "spmv_kernel" (standalone SpMV: 0 chooses by row
  * lengths, 1 shared-memory stream tiles, 2 row-aligned warp tasks, 3 one
  * thread per row from global memory), "sweep_kernel" (0: chunked sweeps,
  * one CTA per chunk of rows, default; 1: flat level-order sweeps),

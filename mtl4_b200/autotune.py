@@ -12,7 +12,7 @@ Knobs and what measures them:
   chunk_rows       rows per chunk of the chunked triangular sweeps; read when
                    a preconditioner is built, so each candidate rebuilds it
   sweep_cluster    CTAs per cluster of the chunked sweeps (0 automatic)
-                                                               (tune_pc)
+  sweep_sleep_ns   back-off of the sweeps' dependency polls    (tune_pc)
   vec_ctas_per_sm  CTAs per SM of the vector passes of the Krylov loops
                                                                (tune_vec)
   sweep_blocks, sweep_sleep_ns   grid and back-off of the flat sweep kernel
@@ -245,7 +245,7 @@ def tune_pc(ctx, Ad, kind: str, value=np.float32, cache: Cache | None = None, re
         P = built[cr]
         return _timed(lambda: itl.solve(P, x, y), reps, ctx)
 
-    start = {"chunk_rows": 0, "sweep_cluster": 0}
+    start = {k: 0 for k in space}   # every knob of the space at its default (0)
     choice, timings = coordinate_search(space, start, measure)
     built.clear()
     apply_settings(ctx, choice)

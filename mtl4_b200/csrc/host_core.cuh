@@ -85,6 +85,7 @@ struct mtlg_ctx {
     int64_t admission_reserve_bytes = -1; // tuning: bytes kept out of admission (-1: max(1 GiB, 2%))
     int* d_scratch_err = nullptr;
     PinnedStage stage;                    // staging blocks of large uploads
+    cudaMemPool_t pool = nullptr;         // stream-ordered device memory (nullptr: cudaMalloc / cudaFree)
     int sweep_blocks() const
     {
         if (sweep_nblocks > 0) return std::min(sweep_nblocks, sm_count * sweep_max_bpsm);
@@ -120,10 +121,13 @@ inline int dalloc(mtlg_ctx* c, void** p, size_t bytes)
         set_error("device budget exceeded: %zu + %zu > %zu bytes", c->in_use.load(), b, c->budget);
         return MTLG_ERR_OOM;
     }
-    cudaError_t e = cudaMalloc(p, b);
+    // the context's pool: allocations and frees are ordered on its stream and
+    // freed blocks stay in the pool for the next set-up (no device-wide
+    // synchronization per buffer, as cudaMalloc / cudaFree have)
+    cudaError_t e = c->pool ? cudaMallocFromPoolAsync(p, b, c->pool, c->stream) : cudaMalloc(p, b);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        set_error("cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
+        set_error("device allocation of %zu bytes: %s", b, cudaGetErrorString(e));
         *p = nullptr;
         return MTLG_ERR_OOM;
     }
@@ -134,7 +138,8 @@ inline void dfree(mtlg_ctx* c, void* p, size_t bytes)
 {
     if (!p) return;
     if (bytes == 0) bytes = 16;
-    cudaFree(p);
+    if (c->pool) cudaFreeAsync(p, c->stream);
+    else cudaFree(p);
     const size_t b = round_up(bytes + 16, 256);
     size_t cur = c->in_use.load();
     while (!c->in_use.compare_exchange_weak(cur, cur >= b ? cur - b : 0)) {

@@ -75,10 +75,16 @@ struct KWork {
     int64_t n;
     int grid;
     std::vector<std::unique_ptr<DBuf<double>>> bufs;
+    // a zeroed work vector (no pass ever reads leftover device memory)
     double* vec()
     {
         bufs.emplace_back(new DBuf<double>());
-        if (bufs.back()->alloc(c, static_cast<size_t>(std::max<int64_t>(n, 1))) != MTLG_OK) return nullptr;
+        const size_t len = static_cast<size_t>(std::max<int64_t>(n, 1));
+        if (bufs.back()->alloc(c, len) != MTLG_OK) return nullptr;
+        if (cudaMemsetAsync(bufs.back()->p, 0, len * sizeof(double), c->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
         return bufs.back()->p;
     }
     int kv(int op, double* y, const double* x = nullptr, const double* z = nullptr, double a = 0.0, double b = 0.0)
@@ -555,8 +561,8 @@ inline int k_idr_s(KOp& A, KWork& W, double* x, const double* b, KIter& it, int 
         KDOT(vr, v, r);
         KDOT(vv, v, v);
         omega = vr / vv;
-        KTRY(W.kv(KV_AXPBY, dX[k], r, nullptr, omega, 0.0));
-        KTRY(W.kv(KV_AXPBY, dR[k], v, nullptr, -omega, 0.0));
+        KTRY(W.kv(KV_AX, dX[k], r, nullptr, omega));
+        KTRY(W.kv(KV_AX, dR[k], v, nullptr, -omega));
         KTRY(W.kv(KV_AXPY, x, dX[k], nullptr, 1.0));
         KTRY(W.kv(KV_AXPY, r, dR[k], nullptr, 1.0));
         ++it.i;
@@ -584,7 +590,7 @@ inline int k_idr_s(KOp& A, KWork& W, double* x, const double* b, KIter& it, int 
             }
             // dX[oldest] = omega v - dX * c, every column of dX (the oldest one
             // included) read before the update
-            KTRY(W.kv(KV_AXPBY, y, dX[0], nullptr, -c[0], 0.0));
+            KTRY(W.kv(KV_AX, y, dX[0], nullptr, -c[0]));
             for (int i = 1; i < s; ++i) KTRY(W.kv(KV_AXPY, y, dX[i], nullptr, -c[i]));
             KTRY(W.kv(KV_AXPY, y, v, nullptr, omega));
             KTRY(W.kv(KV_COPY, dX[oldest], y));

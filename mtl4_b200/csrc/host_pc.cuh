@@ -38,6 +38,11 @@ struct TriDev {
     DBuf<unsigned> wv;
     DBuf<unsigned char> cval, cdia;    // storage type S
     DBuf<unsigned char> ypos[2];       // results by position for FP64 [0] / FP32 [1] vectors (all sentinel between sweeps)
+    // flat layout entries (h_rp, h_ci, h_src, h_mul; rp, ci, src, mul, val,
+    // dia on the device): built at set-up only when the factor has no
+    // chunked layout, else on first need (ensure_flat) from the kept row lists
+    bool flat_entries = false;
+    RowLists F;
 };
 
 constexpr int kChunkMaxEntries = 16;   // longer factor rows: flat sweeps only
@@ -709,7 +714,44 @@ inline int default_chunk_rows(const mtlg_ctx* c, int storage)
     return storage == MTLG_F32 ? 16384 : 8192;
 }
 
-inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& T, int chunk_rows, int ssz)
+// Flat layout entries of a factor whose flat row order is built: per
+// position its row's entries (columns, value sources, multipliers), on the
+// host and the device.
+inline int build_flat_entries(mtlg_ctx* c, const RowLists& F, TriDev& T)
+{
+    MTLG_TRACE(9159, "pc.flat_entries");
+    T.h_rp.resize(size_t(T.npad) + 1);
+    parallel_prefix(T.npad, [&](int k) {
+        const int r = T.h_row_of[k];
+        return r >= 0 ? F.rp[r + 1] - F.rp[r] : 0;
+    }, T.h_rp.data());
+    T.nnz = T.h_rp[T.npad];
+    T.h_ci.resize(T.nnz);
+    T.h_src.resize(T.nnz);
+    T.h_mul.resize(T.nnz);
+    constexpr int kRowsPerBlock = 16384;
+    parallel_for((T.npad + kRowsPerBlock - 1) / kRowsPerBlock, [&](int blk) {
+        const int k1 = std::min(T.npad, (blk + 1) * kRowsPerBlock);
+        for (int k = blk * kRowsPerBlock; k < k1; ++k) {
+            const int r = T.h_row_of[k];
+            if (r < 0) continue;
+            int o = T.h_rp[k];
+            for (int e = F.rp[r]; e < F.rp[r + 1]; ++e, ++o) {
+                T.h_ci[o] = F.col[e];
+                T.h_src[o] = F.src[e];
+                T.h_mul[o] = F.mul[e];
+            }
+        }
+    });
+    MTLG_TRY(T.rp.upload(c, T.h_rp.data(), T.h_rp.size()));
+    MTLG_TRY(T.ci.upload(c, T.h_ci.data(), T.h_ci.size()));
+    MTLG_TRY(T.src.upload(c, T.h_src.data(), T.h_src.size()));
+    MTLG_TRY(T.mul.upload(c, T.h_mul.data(), T.h_mul.size()));
+    T.flat_entries = true;
+    return MTLG_OK;
+}
+
+inline int build_tri(mtlg_ctx* c, RowLists&& F, int n, bool lower, TriDev& T, int chunk_rows, int ssz, bool defer_flat)
 {
     T.n = n;
     T.lower = lower;
@@ -771,40 +813,17 @@ inline int build_tri(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& 
             for (int i = n - 1; i >= 0; --i) T.h_row_of[fill[lev[i]]++] = i;
         }
     }
-    T.h_rp.resize(size_t(T.npad) + 1);
-    parallel_prefix(T.npad, [&](int k) {
-        const int r = T.h_row_of[k];
-        return r >= 0 ? F.rp[r + 1] - F.rp[r] : 0;
-    }, T.h_rp.data());
-    T.nnz = T.h_rp[T.npad];
-    T.h_ci.resize(T.nnz);
-    T.h_src.resize(T.nnz);
-    T.h_mul.resize(T.nnz);
-    constexpr int kRowsPerBlock = 16384;
-    parallel_for((T.npad + kRowsPerBlock - 1) / kRowsPerBlock, [&](int blk) {
-        const int k1 = std::min(T.npad, (blk + 1) * kRowsPerBlock);
-        for (int k = blk * kRowsPerBlock; k < k1; ++k) {
-            const int r = T.h_row_of[k];
-            if (r < 0) continue;
-            int o = T.h_rp[k];
-            for (int e = F.rp[r]; e < F.rp[r + 1]; ++e, ++o) {
-                T.h_ci[o] = F.col[e];
-                T.h_src[o] = F.src[e];
-                T.h_mul[o] = F.mul[e];
-            }
-        }
-    });
     std::vector<SweepTask> tasks(T.npad / kSweepRows);
     for (size_t t = 0; t < tasks.size(); ++t) tasks[t] = {0, int(t) * kSweepRows};
     ph.next(9152, "pc.flat_upload");
     MTLG_TRY(T.row_of.upload(c, T.h_row_of.data(), T.h_row_of.size()));
-    MTLG_TRY(T.rp.upload(c, T.h_rp.data(), T.h_rp.size()));
-    MTLG_TRY(T.ci.upload(c, T.h_ci.data(), T.h_ci.size()));
-    MTLG_TRY(T.src.upload(c, T.h_src.data(), T.h_src.size()));
-    MTLG_TRY(T.mul.upload(c, T.h_mul.data(), T.h_mul.size()));
     MTLG_TRY(T.tasks.upload(c, tasks.data(), tasks.size()));
+    T.nnz = F.rp[n];
     ph.end();
-    return build_chunks(c, F, lev, n, lower, chunk_rows, ssz, T);
+    MTLG_TRY(build_chunks(c, F, lev, n, lower, chunk_rows, ssz, T));
+    if (T.nch == 0 || !defer_flat) return build_flat_entries(c, F, T);
+    T.F = std::move(F);
+    return MTLG_OK;
 }
 
 }  // namespace mtlg
@@ -927,6 +946,86 @@ inline int fill_chunk_values(mtlg_pc* P, TriDev& T, const double* srcvals, const
     return MTLG_OK;
 }
 
+// Values of the flat layout: entries from `srcvals` (times the inverse
+// pivot named by mul), multipliers from the FP64 pivots (1 for a unit
+// diagonal).
+inline int fill_flat_values(mtlg_pc* P, TriDev& T, const double* srcvals, int unit)
+{
+    mtlg_ctx* c = P->ctx;
+    const int f32 = P->storage == MTLG_F32;
+    MTLG_TRY(T.val.alloc(c, size_t(std::max(T.nnz, 1)) * P->ssize()));
+    MTLG_TRY(T.dia.alloc(c, size_t(std::max(T.npad, 1)) * P->ssize()));
+    if (T.nnz) {
+        k_fill_factor<<<launch_grid(T.nnz), 256, 0, c->stream>>>(T.nnz, T.src.p, T.mul.p, srcvals, P->inv_dia.p,
+                                                                 T.val.p, f32);
+        c->launches++;
+    }
+    if (T.npad) {
+        k_fill_dia<<<launch_grid(T.npad), 256, 0, c->stream>>>(T.npad, T.row_of.p, P->inv_dia.p, unit, T.dia.p, f32);
+        c->launches++;
+    }
+    MTLG_CUDA(cudaGetLastError());
+    return MTLG_OK;
+}
+
+// inv[csrc[e]] = e for the chunk entries with a value source (padding: src
+// < 0; alignment gaps: column code -1).
+__global__ void k_chunk_inverse(int nent, const int* __restrict__ csrc, const int* __restrict__ ccol,
+                                int* __restrict__ inv)
+{
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nent; e += gridDim.x * blockDim.x)
+        if (csrc[e] >= 0 && ccol[e] != -1) inv[csrc[e]] = e;
+}
+// val[k] = cval[inv[src[k]]]: a flat entry's value, copied from the chunked
+// layout's entry of the same source (the same value, already in S).
+__global__ void k_flat_from_chunk(int nnz, const int* __restrict__ src, const int* __restrict__ inv,
+                                  const unsigned char* __restrict__ cval, unsigned char* __restrict__ val, int ssz)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x) {
+        const int e = src[k] >= 0 ? inv[src[k]] : -1;   // every entry has its chunk twin; -1 stays 0
+        if (ssz == 8) reinterpret_cast<double*>(val)[k] = e >= 0 ? reinterpret_cast<const double*>(cval)[e] : 0.0;
+        else reinterpret_cast<float*>(val)[k] = e >= 0 ? reinterpret_cast<const float*>(cval)[e] : 0.0f;
+    }
+}
+
+// The flat layout of a preconditioner whose factors were built with the
+// chunked layout only: entries from the kept row lists, values copied from
+// the chunked layout, multipliers from the pivots.  Needed by flat sweeps,
+// factor downloads and the ILU(0) adjoint.
+inline int ensure_flat(mtlg_pc* P)
+{
+    if (!P || !P->has_factors()) return MTLG_OK;
+    mtlg_ctx* c = P->ctx;
+    for (TriDev* T : {&P->L, &P->U}) {
+        if (T->flat_entries) continue;
+        MTLG_TRY(build_flat_entries(c, T->F, *T));
+        T->F = RowLists();
+        const int unit = (P->kind == MTLG_PC_ILU0 && T == &P->L);
+        MTLG_TRY(T->val.alloc(c, size_t(std::max(T->nnz, 1)) * P->ssize()));
+        MTLG_TRY(T->dia.alloc(c, size_t(std::max(T->npad, 1)) * P->ssize()));
+        if (T->nnz) {
+            DBuf<int> inv;
+            const int64_t asz = std::max<int64_t>(1, P->A->nnz);
+            MTLG_TRY(inv.alloc(c, size_t(asz)));
+            MTLG_CUDA(cudaMemsetAsync(inv.p, 0xFF, size_t(asz) * sizeof(int), c->stream));
+            k_chunk_inverse<<<launch_grid(T->cnent), 256, 0, c->stream>>>(T->cnent, T->csrc.p, T->ccol.p, inv.p);
+            k_flat_from_chunk<<<launch_grid(T->nnz), 256, 0, c->stream>>>(T->nnz, T->src.p, inv.p, T->cval.p,
+                                                                          T->val.p, int(P->ssize()));
+            c->launches += 2;
+            MTLG_CUDA(cudaGetLastError());
+            MTLG_CUDA(cudaStreamSynchronize(c->stream));   // inv is freed at scope end
+        }
+        if (T->npad) {
+            k_fill_dia<<<launch_grid(T->npad), 256, 0, c->stream>>>(T->npad, T->row_of.p, P->inv_dia.p, unit, T->dia.p,
+                                                                     P->storage == MTLG_F32);
+            c->launches++;
+            MTLG_CUDA(cudaGetLastError());
+        }
+    }
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    return MTLG_OK;
+}
+
 // Structure + device factorization.
 inline int pc_build(mtlg_pc* P)
 {
@@ -947,8 +1046,8 @@ inline int pc_build(mtlg_pc* P)
         RowLists E;
         E.rp.assign(n + 1, 0);
         const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
-        MTLG_TRY(build_tri(c, E, n, true, P->L, B, int(P->ssize())));
-        MTLG_TRY(build_tri(c, E, n, false, P->U, B, int(P->ssize())));
+        MTLG_TRY(build_tri(c, RowLists(E), n, true, P->L, B, int(P->ssize()), false));
+        MTLG_TRY(build_tri(c, RowLists(E), n, false, P->U, B, int(P->ssize()), false));
         MTLG_TRY(P->L.val.alloc(c, 16));
         MTLG_TRY(P->U.val.alloc(c, 16));
         MTLG_TRY(P->L.dia.alloc(c, size_t(P->L.npad) * P->ssize()));
@@ -1046,13 +1145,13 @@ inline int pc_build(mtlg_pc* P)
         std::thread tu([&]() {
             cudaSetDevice(c->device);   // the thread's uploads go to the context's device
             MTLG_TRACE(9103, "pc.schedule_U");
-            su = build_tri(c, Ur, n, false, P->U, B, int(P->ssize()));
+            su = build_tri(c, std::move(Ur), n, false, P->U, B, int(P->ssize()), true);
             if (su != MTLG_OK) eu = last_error();
         });
         int sl = MTLG_OK;
         {
             MTLG_TRACE(9105, "pc.schedule_L");
-            sl = build_tri(c, Lr, n, true, P->L, B, int(P->ssize()));
+            sl = build_tri(c, std::move(Lr), n, true, P->L, B, int(P->ssize()), true);
         }
         tu.join();
         if (sl != MTLG_OK) return sl;
@@ -1101,21 +1200,9 @@ inline int pc_build(mtlg_pc* P)
         }
     }
     MTLG_CUDA(cudaGetLastError());
-    const int f32 = P->storage == MTLG_F32;
     for (TriDev* T : {&P->L, &P->U}) {
-        MTLG_TRY(T->val.alloc(c, size_t(std::max(T->nnz, 1)) * P->ssize()));
-        MTLG_TRY(T->dia.alloc(c, size_t(std::max(T->npad, 1)) * P->ssize()));
-        if (T->nnz) {
-            k_fill_factor<<<launch_grid(T->nnz), 256, 0, c->stream>>>(T->nnz, T->src.p, T->mul.p, srcvals, P->inv_dia.p,
-                                                                      T->val.p, f32);
-            c->launches++;
-        }
         const int unit = (P->kind == MTLG_PC_ILU0 && T == &P->L);
-        if (T->npad) {
-            k_fill_dia<<<launch_grid(T->npad), 256, 0, c->stream>>>(T->npad, T->row_of.p, P->inv_dia.p, unit, T->dia.p, f32);
-            c->launches++;
-        }
-        MTLG_CUDA(cudaGetLastError());
+        if (T->flat_entries) MTLG_TRY(fill_flat_values(P, *T, srcvals, unit));
         MTLG_TRY(fill_chunk_values(P, *T, srcvals, P->inv_dia.p, unit));
     }
     int err = 0;
@@ -1182,6 +1269,7 @@ inline void transpose_rows(const TriDev& T, int n, int src_off, bool descending,
 // sequence.
 inline int pc_build_adjoint(mtlg_pc* P)
 {
+    MTLG_TRY(ensure_flat(P));
     mtlg_ctx* c = P->ctx;
     const int n = P->n;
     const TriDev& L = P->L;
@@ -1203,8 +1291,8 @@ inline int pc_build_adjoint(mtlg_pc* P)
     transpose_rows(U, n, L.nnz, false, Lh);
     transpose_rows(L, n, 0, true, Uh);
     const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
-    MTLG_TRY(build_tri(c, Lh, n, true, Q->L, B, int(P->ssize())));
-    MTLG_TRY(build_tri(c, Uh, n, false, Q->U, B, int(P->ssize())));
+    MTLG_TRY(build_tri(c, std::move(Lh), n, true, Q->L, B, int(P->ssize()), false));
+    MTLG_TRY(build_tri(c, std::move(Uh), n, false, Q->U, B, int(P->ssize()), false));
     MTLG_TRY(pc_setup_single_set(Q.get()));
     MTLG_TRY(Q->inv_dia.alloc(c, size_t(std::max(n, 1))));
     if (n) MTLG_CUDA(cudaMemcpyAsync(Q->inv_dia.p, P->inv_dia.p, size_t(n) * 8, cudaMemcpyDeviceToDevice, c->stream));

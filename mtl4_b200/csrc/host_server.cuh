@@ -116,6 +116,14 @@ inline int free_memory(mtlg_ctx* c, size_t held, size_t& free_bytes, size_t& res
 {
     size_t fr = 0, total = 0;
     MTLG_CUDA(cudaMemGetInfo(&fr, &total));
+    if (c->pool) {
+        // blocks the context's pool holds but no buffer uses are free too
+        uint64_t reserved = 0, used = 0;
+        if (cudaMemPoolGetAttribute(c->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+            cudaMemPoolGetAttribute(c->pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+            fr += size_t(reserved - used);
+        cudaGetLastError();
+    }
     if (c->admission_free_bytes > 0) {
         const size_t f = size_t(c->admission_free_bytes);
         free_bytes = f > held ? f - held : 0;
@@ -288,6 +296,18 @@ inline int srv_rebuild(mtlg_server* S, int e)
         for (int s = 0; s < ss.S; ++s)
             if (E.slot_req[s] >= 0) pcs[s] = S->reqs[E.slot_req[s]]->P;
         MTLG_TRY(plan_set_chunks(ss, pcs));
+        if (!ss.cplan.ok) {
+            // flat sweeps: every active preconditioner's flat entries, and
+            // its views refreshed in both descriptors
+            for (int s = 0; s < ss.S; ++s) {
+                if (!pcs[s]) continue;
+                mtlg_pc* P = const_cast<mtlg_pc*>(pcs[s]);
+                MTLG_TRY(ensure_flat(P));
+                MTLG_TRY(pc_views(P, ss.f32, ss.h_desc[s].L, ss.h_desc[s].U));
+                ss.h_desc64[s].L = ss.h_desc[s].L;
+                ss.h_desc64[s].U = ss.h_desc[s].U;
+            }
+        }
     }
     MTLG_CUDA(cudaMemcpyAsync(ss.desc.p, ss.h_desc.data(), sizeof(SysDesc) * ss.S, cudaMemcpyHostToDevice, c->stream));
     MTLG_CUDA(cudaMemcpyAsync(ss.desc64.p, ss.h_desc64.data(), sizeof(SysDesc) * ss.S, cudaMemcpyHostToDevice,
@@ -405,6 +425,8 @@ int mtlg_server_step(mtlg_server* S)
     MTLG_CHECK_ARG(S, "server");
     mtlg_ctx* c = S->ctx;
     S->stats.steps++;
+    TracePhases ph;
+    ph.next(9133, "server.harvest");
     // 1. harvest finished slots
     for (int e = 0; e < 2; ++e) {
         auto& E = S->eng[e];
@@ -427,6 +449,7 @@ int mtlg_server_step(mtlg_server* S)
                     rp.max_outer = 20;
                     rp.max_inner = R.max_iter;
                     rp.rtol = S->o.rtol;
+                    MTLG_TRACE(9137, "server.fp64_finish");
                     MTLG_TRY(fp64_finish(c, R.solver, R.A, R.P, R.x.p, R.bd.p, fp64_budget(rp, R.res.iterations),
                                          S->o.rtol, R.res));
                 }
@@ -452,6 +475,7 @@ int mtlg_server_step(mtlg_server* S)
         }
     }
     // 2. admit queued requests while slots and memory allow
+    ph.next(9134, "server.admit");
     while (!S->queue.empty()) {
         const int64_t id = S->queue.front();
         auto it = S->reqs.find(id);
@@ -496,7 +520,11 @@ int mtlg_server_step(mtlg_server* S)
     for (int e = 0; e < 2; ++e) {
         auto& E = S->eng[e];
         if (E.nactive == 0) continue;
-        if (E.dirty) MTLG_TRY(srv_rebuild(S, e));
+        if (E.dirty) {
+            ph.next(9135, "server.rebuild");
+            MTLG_TRY(srv_rebuild(S, e));
+        }
+        ph.next(9136, "server.launch");
         SolveSet& ss = E.ss;
         const SetView sv = ss.view(false, false);
         if (S->refine) {

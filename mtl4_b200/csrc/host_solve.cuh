@@ -98,6 +98,7 @@ inline size_t vsize(int f32) { return f32 ? 4 : 8; }
 // Builds the set: tiling, descriptors, workspace, merged sweep schedules.
 inline int build_set(mtlg_ctx* c, SolveSet& ss)
 {
+    MTLG_TRACE(9140, "set.build");
     ss.ctx = c;
     ss.S = int(ss.in.size());
     std::vector<Tile> tiles;
@@ -123,6 +124,16 @@ inline int build_set(mtlg_ctx* c, SolveSet& ss)
                 return MTLG_ERR_NOT_SUPPORTED;
             }
         }
+    }
+    if (ss.path == PATH_SWEEP) {
+        // the chunked-sweep plan first: without one the set sweeps in flat
+        // level order, which needs every preconditioner's flat entries before
+        // its views go into the descriptors
+        std::vector<const mtlg_pc*> pcs(ss.S);
+        for (int s = 0; s < ss.S; ++s) pcs[s] = ss.in[s].P;
+        MTLG_TRY(plan_set_chunks(ss, pcs));
+        if (!ss.cplan.ok)
+            for (int s = 0; s < ss.S; ++s) MTLG_TRY(ensure_flat(const_cast<mtlg_pc*>(ss.in[s].P)));
     }
     ss.n_tiles = int(tiles.size());
     MTLG_TRY(ss.tiles.upload(c, tiles.data(), std::max<size_t>(1, tiles.size())));
@@ -219,9 +230,6 @@ inline int build_set(mtlg_ctx* c, SolveSet& ss)
         ss.ntu = int(tu.size());
         MTLG_TRY(ss.tl.upload(c, tl.data(), std::max<size_t>(1, tl.size())));
         MTLG_TRY(ss.tu.upload(c, tu.data(), std::max<size_t>(1, tu.size())));
-        std::vector<const mtlg_pc*> pcs(ss.S);
-        for (int s = 0; s < ss.S; ++s) pcs[s] = ss.in[s].P;
-        MTLG_TRY(plan_set_chunks(ss, pcs));
     }
     return MTLG_OK;
 }
@@ -246,7 +254,7 @@ template <typename T>
 inline int launch_sweep(SolveSet& ss, cudaStream_t st, const SetView& sv, int which, int in, int out, int reset,
                         int skip, int ticket)
 {
-    if (ss.cplan.ok && ss.ctx->sweep_kernel == 0) {
+    if (ss.cplan.ok) {   // planned when the set was built (no plan under sweep_kernel 1)
         ChunkSweepOp op;
         memset(&op, 0, sizeof op);
         op.tasks = which == 0 ? ss.cplan.tl.p : ss.cplan.tu.p;
@@ -540,6 +548,7 @@ inline int run_loop_chunked(SolveSet& ss, int max_iter)
 {
     mtlg_ctx* c = ss.ctx;
     if (!ss.chunk_exec) {
+        MTLG_TRACE(9141, "set.capture");
         if (!ss.cap_stream) MTLG_CUDA(cudaStreamCreateWithFlags(&ss.cap_stream, cudaStreamNonBlocking));
         if (!ss.h_running) MTLG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ss.h_running), 2 * sizeof(int), 0));
         for (auto& e : ss.chunk_ev)
@@ -579,8 +588,9 @@ inline int run_loop_chunked(SolveSet& ss, int max_iter)
 
 // Runs the loop until no system is running.  Default: chunked plain graphs
 // (run_loop_chunked).  loop_mode 1: one graph with a WHILE conditional node,
-// one launch per solve.  If a graph cannot be built, the body is replayed
-// from the host in chunks.
+// one launch per solve.  If a graph cannot be built, or under loop_mode 2
+// (for profilers that do not see kernels inside graphs), the body is
+// launched directly from the host, 8 at a time.
 template <typename T>
 inline int run_loop(SolveSet& ss, int max_iter)
 {
@@ -589,8 +599,8 @@ inline int run_loop(SolveSet& ss, int max_iter)
     int hdr[3] = {0, 0, max_iter / ipb + 4};   // err flag, body runs, cap
     MTLG_CUDA(cudaMemcpyAsync(ss.misc.p + 1, hdr, sizeof hdr, cudaMemcpyHostToDevice, c->stream));
     if (c->loop_mode == 0) return run_loop_chunked<T>(ss, max_iter);
-    MTLG_TRY(build_graph<T>(ss));
-    if (ss.exec) {
+    if (c->loop_mode == 1) MTLG_TRY(build_graph<T>(ss));   // loop_mode 2: direct launches (profilers)
+    if (c->loop_mode == 1 && ss.exec) {
         MTLG_CUDA(cudaGraphLaunch(ss.exec, c->stream));
         int runs = 0;
         MTLG_CUDA(cudaMemcpyAsync(&runs, ss.misc.p + 2, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

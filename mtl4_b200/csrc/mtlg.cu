@@ -54,6 +54,7 @@ inline CtxExtra& extra(const mtlg_ctx* c)
 
 inline void purge_sets(const mtlg_ctx* c, const void* obj)
 {
+    MTLG_TRACE(9108, "sets.purge");
     CtxExtra& e = extra(c);
     for (auto it = e.sets.begin(); it != e.sets.end();) {
         if (it->first.A == obj || it->first.P == obj) it = e.sets.erase(it);
@@ -126,8 +127,6 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
     d.b = y->p;
     d.ws = P->tmp.p;
     d.ws_stride = 0;
-    MTLG_TRY(pc_views(P, sizeof(T) == 4 ? 1 : 0, d.L, d.U));
-    MTLG_CUDA(cudaMemcpyAsync(P->desc.p, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
     ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
     int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
     const int setting = c->sweep_kernel | (c->sweep_cluster << 4);
@@ -136,7 +135,12 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
         MTLG_TRY((plan_chunks<T, S>(c, f, pl)));
         made = setting;
     }
-    if (pl.ok) {
+    // flat sweeps (no chunked plan, or chosen by sweep_kernel) need the flat entries
+    const bool chunked = pl.ok;
+    if (!chunked) MTLG_TRY(ensure_flat(P));
+    MTLG_TRY(pc_views(P, sizeof(T) == 4 ? 1 : 0, d.L, d.U));
+    MTLG_CUDA(cudaMemcpyAsync(P->desc.p, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
+    if (chunked) {
         ChunkSweepOp op;
         memset(&op, 0, sizeof op);
         op.skip = SKIP_NONE;
@@ -402,6 +406,22 @@ int mtlg_ctx_create(int device, size_t hbm_budget, mtlg_ctx** out)
     c->sweep_grid = c->sm_count * c->sweep_max_bpsm;
     MTLG_TRY(init_kernel_shapes());
     MTLG_TRY(init_chunk_shapes());
+    {
+        // stream-ordered pool of this context's device buffers, kept between
+        // set-ups (release threshold: never); without one, cudaMalloc
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&c->pool, &props) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            cudaGetLastError();
+            c->pool = nullptr;
+        }
+    }
     *out = c.release();
     return MTLG_OK;
 }
@@ -422,6 +442,9 @@ int mtlg_ctx_destroy(mtlg_ctx* c)
         }
     }
     if (c->log_dev) cudaFree(c->log_dev);
+    cudaStreamSynchronize(c->stream);
+    // the pool goes with the context once every buffer of it is back
+    if (c->pool && c->in_use.load() == 0) cudaMemPoolDestroy(c->pool);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return MTLG_OK;
@@ -437,6 +460,9 @@ int mtlg_ctx_synchronize(mtlg_ctx* c)
 int mtlg_ctx_set_stream(mtlg_ctx* c, void* s)
 {
     MTLG_CHECK_ARG(c, "ctx");
+    // buffers are allocated and freed in the order of the context's stream:
+    // the old stream's work ends before the new stream takes over
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));
     c->stream = s ? static_cast<cudaStream_t>(s) : c->own_stream;
     return MTLG_OK;
 }
@@ -449,7 +475,7 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     const std::string k(key);
     if (k == "sweep_blocks_per_sm") c->sweep_bpsm = int(std::max<int64_t>(0, value));
     else if (k == "sweep_blocks") c->sweep_nblocks = int(std::max<int64_t>(0, std::min<int64_t>(value, 1 << 16)));
-    else if (k == "loop_mode") c->loop_mode = value ? 1 : 0;
+    else if (k == "loop_mode") c->loop_mode = int(std::max<int64_t>(0, std::min<int64_t>(value, 2)));
     else if (k == "spmv_kernel") c->spmv_kernel = int(std::max<int64_t>(0, std::min<int64_t>(value, 3)));
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
     else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
@@ -914,6 +940,7 @@ int mtlg_pc_create(mtlg_ctx* c, mtlg_csr* A, int kind, mtlg_dtype storage, mtlg_
 int mtlg_pc_destroy(mtlg_pc* P)
 {
     if (!P) return MTLG_OK;
+    MTLG_TRACE(9107, "pc.destroy");
     cudaStreamSynchronize(P->ctx->stream);
     if (P->fallback64) mtlg_pc_destroy(P->fallback64);
     if (P->adjoint) mtlg_pc_destroy(P->adjoint);
@@ -962,6 +989,7 @@ int mtlg_pc_factor(const mtlg_pc* P, int which, int64_t* nnz, int64_t* row_ptr, 
         set_error("preconditioner has no triangular factors");
         return MTLG_ERR_NOT_SUPPORTED;
     }
+    MTLG_TRY(ensure_flat(const_cast<mtlg_pc*>(P)));   // the download reads the flat layout
     const TriDev& T = which == 0 ? P->L : P->U;
     const bool has_diag = !(P->kind == MTLG_PC_ILU0 && which == 0);
     const bool diag_first = which == 1;  // U: diagonal first; IC's L: last

@@ -169,6 +169,29 @@ def test_chunked_equals_flat(ctx):
         assert np.array_equal(y0, y1)
 
 
+@pytest.mark.parametrize("solver,kind", [("cg", "ic_0"), ("bicgstab", "ilu_0")])
+def test_flat_solve_after_chunked_setup(ctx, solver, kind):
+    # a preconditioner set up with the chunked layout only gets its flat
+    # entries on first need: here a solve under sweep_kernel 1 (flat level
+    # order), which must give the chunked solve's iterations and x exactly
+    from mtl4_b200 import itl, mtl
+    A = P.vardiff_3d(20, sigma=1.0, seed=5, beta=(0.05, 0.02, 0.01))
+    b = np.random.default_rng(3).standard_normal(A.n_rows)
+    out = []
+    for flat in (0, 1):
+        with tuning(ctx, chunk_rows=1024, sweep_kernel=0):
+            Ad = dev(A, ctx)
+            Pc = getattr(itl.pc, kind)(Ad)
+        with tuning(ctx, sweep_kernel=flat):
+            x = mtl.dense_vector(A.n_rows, np.float64, ctx)
+            bd = vec(b, ctx)
+            it = itl.basic_iteration(bd, 1000, 1e-10)
+            getattr(itl, solver)(Ad, x, bd, Pc, it)
+            out.append((it.iterations(), x.numpy()))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 def test_chunked_repeated_applies_keep_invariants(ctx):
     # the sweeps reset their buffers to the sentinel row by row; a second and
     # third apply on the same preconditioner must give the same result
