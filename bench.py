@@ -46,9 +46,10 @@ METRIC = "solves/s at relres<=1e-8, mixed vs plain FP64 on B200; SpMV %HBM; p99 
 WORKLOAD = ("BiCGSTAB+ILU(0) on 128^3 7-point convection-diffusion (2,097,152 unknowns, 14,581,760 nnz, "
             "beta=(0.5,0.3,0.2), h=1/129), b=A*x_true seed 1, relres<=1e-8")
 PEAKS = ROOT / "MEASURED_PEAKS.json"
-# DRAM bytes (read + write) of one FP32 ILU(0) apply (L and U k_sweep_chunk
-# launches) from one ncu capture of this workload
-TRAFFIC_PER_APPLY = 210_680_000   # 105.1 MB (L) + 105.5 MB (U)
+# DRAM bytes (read + write) of one FP32 ILU(0) apply (the L and U sweep
+# launches) from one ncu capture of this workload, per sweep kernel
+TRAFFIC_PER_APPLY = {"chunked": 210_680_000,   # k_sweep_chunk: 105.1 MB (L) + 105.5 MB (U)
+                     "grid": None}
 FALLBACK_HBM = 6650.0
 
 
@@ -491,8 +492,9 @@ def main():
     err_vs_oracle = float(np.abs(x_mixed - x_oracle).max() / np.abs(x_oracle).max())
     err_vs_true = float(np.abs(x_mixed - x_true).max() / np.abs(x_true).max())
 
-    # dominant kernel: the chunked triangular sweeps of the FP32 ILU(0)
-    # apply (k_sweep_chunk, L then U), timed with events on the launching
+    # dominant kernel: the triangular sweeps of the FP32 ILU(0) apply (the
+    # grid sweep on this grid-stencil operator, else the chunked sweep; L
+    # then U), timed with events on the launching
     # stream; the applies are queued back to back (pc_apply_sync = 0), then
     # one synchronous apply reports any expired device wait
     P32 = held["P32"]
@@ -521,7 +523,14 @@ def main():
     # (level-ordered) row, right-hand side read, result written, and the
     # temporary written and re-armed once each
     nnz_off = len(Lv) + (len(Uv) - n)
-    bytes_apply = 8 * nnz_off + 2 * 12 * n + 4 * n * 4
+    if plan["kernel"] == "grid":
+        # grid layout (no indices): entry values and one multiplier per row,
+        # right-hand side read, result written, the other vector reset, per sweep
+        bytes_apply = 4 * nnz_off + 2 * 4 * n + 2 * 3 * 4 * n
+        sweep_kernel = "k_sweep_grid<float,float> (ILU(0) L and U sweeps, one apply)"
+    else:
+        bytes_apply = 8 * nnz_off + 2 * 12 * n + 4 * n * 4
+        sweep_kernel = "k_sweep_chunk<float,float> (ILU(0) L and U sweeps, one apply)"
     peak, peak_kind = hbm_peak()
     sweep_gbs = bytes_apply / apply_s / 1e9
     t_setup32 = time.perf_counter()
@@ -591,9 +600,9 @@ def main():
                  "frac_measured_peak": spmv_gbs / peak, "frac_8TBs_nominal": spmv_gbs / 8000.0,
                  "gather_floor_us": floor_s * 1e6, "gather_floor_GBs": spmv_bytes / floor_s / 1e9,
                  "frac_of_gather_floor": floor_s / spmv_s},
-        "roofline": {"kernel": "k_sweep_chunk<float,float> (ILU(0) L and U sweeps, one apply)", "bound": "hbm",
+        "roofline": {"kernel": sweep_kernel, "bound": "hbm",
                      "achieved": sweep_gbs, "peak": peak, "unit": "GB/s", "frac": sweep_gbs / peak,
-                     "peak_kind": peak_kind, "traffic": TRAFFIC_PER_APPLY,
+                     "peak_kind": peak_kind, "traffic": TRAFFIC_PER_APPLY.get(plan["kernel"]),
                      "algorithmic_bytes_per_apply": bytes_apply, "apply_us": apply_s * 1e6,
                      "levels": lev_L + lev_U, "ns_per_level": apply_s * 1e9 / (lev_L + lev_U),
                      "note": "dependency-latency bound: one level of the L or U chain per step",

@@ -154,6 +154,11 @@ int64_t mtlg_ctx_kernel_launches(mtlg_ctx* ctx);
  * lengths, 1 shared-memory stream tiles, 2 row-aligned warp tasks, 3 one
  * thread per row from global memory), "sweep_kernel" (0: chunked sweeps,
  * one CTA per chunk of rows, default; 1: flat level-order sweeps),
+ * "grid_sweep" (1, default: factors whose pattern is a 5- or 7-point grid
+ * stencil in natural order get, at set-up, a layout of x-lines per lane and
+ * are swept by the grid kernel when sweep_kernel is 0; 0: chunked or flat
+ * only), "grid_warps" (compute warps per grid-sweep CTA: 4 or 8; 0,
+ * default: 8 where the shared memory fits, else 4),
  * "chunk_rows" (rows per chunk of preconditioners created afterwards; 0:
  * 16384 for FP32 factors, 8192 for FP64), "sweep_cluster" (CTAs per
  * thread-block cluster of the chunked sweeps, whose neighbouring chunks
@@ -316,13 +321,15 @@ int mtlg_pc_adjoint_apply(mtlg_ctx* ctx, mtlg_pc* P, const mtlg_vec* x, mtlg_vec
 int mtlg_pc_factor(const mtlg_pc* P, int which, int64_t* nnz, int64_t* row_ptr, int32_t* col, double* val);
 /* Number of dependency levels of the L and U sweeps. */
 int mtlg_pc_levels(const mtlg_pc* P, int* levels_L, int* levels_U);
-/* Launch plan of the chunked sweeps for vectors of `dtype` under the
- * context's current tuning, as 8 integers: rows per chunk, chunks of L,
- * CTAs resident at once, shared memory per CTA (bytes), compute threads per
- * CTA (one receiver warp more), entries per row (register bucket), rows and
- * entries per staged segment.  All zero when the flat level-order sweeps
- * run instead.  Not part of the reference's interface (introspection for
- * tuning). */
+/* Launch plan of the sweeps for vectors of `dtype` under the context's
+ * current tuning, as 8 integers.  Chunked sweeps: rows per chunk, chunks of
+ * L, CTAs resident at once, shared memory per CTA (bytes), compute threads
+ * per CTA, entries per row (register bucket), rows and entries per staged
+ * segment.  Grid sweeps (grid-stencil factors): 0, 0, CTAs resident at
+ * once, shared memory per CTA, compute threads per CTA (two receiver warps
+ * more), entries per row, tiles of L, steps per warp unit.  All zero when
+ * the flat level-order sweeps run instead.  Not part of the reference's
+ * interface (introspection for tuning). */
 int mtlg_pc_sweep_plan(mtlg_ctx* ctx, mtlg_pc* P, int dtype, int32_t* out8);
 
 /* ---- solvers ---------------------------------------------------------------- */

@@ -90,6 +90,7 @@ struct __align__(16) SegRec {
 
 constexpr unsigned kWaveOverflow = 0x8000u;   // wave reads rows of earlier chunks beyond the receive slots
 constexpr int kSlotBase = 4;                  // receive slots start at shared cell chunk_rows + kSlotBase (16-byte aligned)
+constexpr int kGridStepPad = 8;               // grid layout: steps per unit padded to a multiple of this
 
 // Level-ordered triangular factor (device pointers).  Row k of the factor is
 // original row `row_of[k]` (-1 marks padding that aligns levels to warps);
@@ -137,6 +138,24 @@ struct TriFactor {
     const int* ccol;   // entries' columns
     const void* cval;  // entries' values (S)
     const void* cdia;  // multiplier per position (S)
+    // Grid layout (k_sweep_grid): the factor's pattern is a 5- or 7-point
+    // grid stencil.  Counting rows from the sweep's start (r' = r for L,
+    // n - 1 - r for U), r' = i + gnx * (j + gny * k) and row r' reads rows
+    // r' - 1 (x, when i > 0), r' - gnx (y, when j > 0) and r' - gnx*gny (z,
+    // when k > 0) and nothing else.  A warp unit u = k * gnjb + jb holds the
+    // x-lines j = 32 jb + lane of plane k; its step s is row i = s - lane of
+    // each lane (i = s without skew).  gdata: [unit][step][slot][lane], slot
+    // q < gns the entry of direction (gperm >> 2q) & 3 (0 x, 1 y, 2 z; +0
+    // where the row has no such neighbour), slot gns the multiplier.
+    int gnx, gny, gnz;  // gnx == 0: no grid layout
+    int gns;            // entries per row (directions present): 0, 2 or 3
+    int gperm;          // slot order of the directions (the reference's entry order)
+    int gdirs;          // directions present (bit d)
+    int gskew;          // 1: lane l runs row i at step i + l (rows depend on the lane below)
+    int gnsteps;        // steps per unit
+    int gnsp;           // steps per unit in the layout (a multiple of kGridStepPad)
+    int gnjb;           // units along y
+    const void* gdata;  // S
 };
 
 // One CTA's chunk in a group of chunks run by one thread-block cluster:

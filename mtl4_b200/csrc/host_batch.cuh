@@ -176,6 +176,7 @@ int mtlg_batch_solve(mtlg_batch* B, int precision, const mtlg_refine_params* ref
         MTLG_CUDA(cudaMemcpy(&flag, ss.misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost));
         if (flag) {
             for (auto& si : ss.in) pc_reset_sweep_state(si.P);
+            reset_set_sweep_buffers(ss);
             set_error("a device-side wait expired during the batched solve");
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);

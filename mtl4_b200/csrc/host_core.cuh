@@ -1,6 +1,7 @@
 // Host side: context, device memory accounting, CSR / vector handles, tiling.
 #pragma once
 #include "sweep.cuh"
+#include "gridsweep.cuh"
 #include "refdot.cuh"
 #include "trace.cuh"
 #include "mmio.cuh"
@@ -75,6 +76,8 @@ struct mtlg_ctx {
     int sweep_cluster = 0;      // tuning: CTAs per cluster of the chunked sweeps (0: automatic)
     int vec_ctas_per_sm = 2;    // tuning: CTAs per SM of the vector passes
     int sweep_kernel = 0;       // tuning: 0 chunked waves, 1 flat level order
+    int grid_sweep = 1;         // tuning: 1 grid-stencil factors of new preconditioners get the grid layout and sweep
+    int grid_warps = 0;         // tuning: compute warps per grid-sweep CTA (0: automatic, 4 or 8)
     int pc_apply_sync = 1;      // tuning: 1 each preconditioner apply checks its device waits (synchronizes), 0 queued
     int red_order = 0;          // tuning: FP64 dots and norms, 0 tile-parallel, 1 the reference's summation order
     int64_t admission_free_bytes = 0;     // tuning: stand-in for cudaMemGetInfo's free bytes (0: query)

@@ -43,6 +43,13 @@ struct TriDev {
     // chunked layout, else on first need (ensure_flat) from the kept row lists
     bool flat_entries = false;
     RowLists F;
+    // grid layout (k_sweep_grid; gnx == 0: the pattern is not a grid
+    // stencil): geometry as in TriFactor, per element the value source and
+    // pivot row (kept until the values are filled), the values (type S)
+    int gnx = 0, gny = 0, gnz = 0, gns = 0, gperm = 0, gdirs = 0, gskew = 0, gnsteps = 0, gnsp = 0, gnjb = 0;
+    long long gnent = 0;
+    DBuf<int> gsrc, gmul;
+    DBuf<unsigned char> gval;
 };
 
 constexpr int kChunkMaxEntries = 16;   // longer factor rows: flat sweeps only
@@ -411,9 +418,18 @@ struct ChunkSide {
 struct ChunkPlan {
     bool ok = false;
     ChunkSide side[2];           // L [0], U [1]
-    DBuf<GroupTask> tl, tu;
+    DBuf<GroupTask> tl, tu;      // grid sweeps: tiles {sys, first unit along y, first plane, jw}
     int ntl = 0, ntu = 0;
+    bool grid = false;           // k_sweep_grid: every factor of the set has a grid layout
+    int gnw = 0, gsmem = 0, gresident = 0;   // compute warps, dynamic shared memory, CTAs resident at once
+    int gsteps = 0;              // steps per unit (the largest factor's)
 };
+
+// Context settings a sweep plan depends on (a plan is remade when they change).
+inline int plan_setting(const mtlg_ctx* c)
+{
+    return c->sweep_kernel | (c->sweep_cluster << 4) | (c->grid_sweep << 9) | (c->grid_warps << 10);
+}
 
 // Kernel shape of a wave cap of NT rows and KM entries per row: up to four
 // compute warps, two rows per thread beyond 128 rows.
@@ -566,12 +582,134 @@ inline int chunk_groups(const std::vector<int>& nch, int cl, std::vector<GroupTa
 // and U, or nulls for an unused slot), in groups (chunk_groups) of the
 // side's cluster size.  Not ok (flat sweeps) when a side's shape is not built
 // or its shared memory does not fit.
+// Grid-sweep launch shapes: NW compute warps (4 or 8) and two receiver warps.
+template <typename T, typename S, int NW>
+struct GridShape {
+    static constexpr int THREADS = 32 * (NW + kGridRecvWarps);
+    static int init()
+    {
+        if (grid_smem_bytes<T, S>(NW) > kChunkSmemMax) return MTLG_OK;   // not built for this type pair
+        MTLG_CUDA(cudaFuncSetAttribute(k_sweep_grid<T, S, NW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       grid_smem_bytes<T, S>(NW)));
+        MTLG_CUDA(cudaFuncSetAttribute(k_sweep_grid<T, S, NW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       grid_smem_bytes<T, S>(NW)));
+        return MTLG_OK;
+    }
+    static int resident(mtlg_ctx* c)
+    {
+        int n = 0, m = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_grid<T, S, NW, false>, THREADS,
+                                                          size_t(grid_smem_bytes<T, S>(NW))) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_sweep_grid<T, S, NW, true>, THREADS,
+                                                          size_t(grid_smem_bytes<T, S>(NW))) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return std::min(n, m) * c->sm_count;
+    }
+    static int launch(mtlg_ctx* c, cudaStream_t st, const SetView& sv, const ChunkSweepOp& op, int resident)
+    {
+        const int grid = std::max(1, std::min(op.ntasks, resident));
+        if (op.which) k_sweep_grid<T, S, NW, true><<<grid, THREADS, grid_smem_bytes<T, S>(NW), st>>>(sv, op);
+        else k_sweep_grid<T, S, NW, false><<<grid, THREADS, grid_smem_bytes<T, S>(NW), st>>>(sv, op);
+        c->launches++;
+        MTLG_CUDA(cudaGetLastError());
+        return MTLG_OK;
+    }
+};
+
+inline int init_grid_shapes()
+{
+    MTLG_TRY((GridShape<double, double, 4>::init()));
+    MTLG_TRY((GridShape<double, double, 8>::init()));
+    MTLG_TRY((GridShape<double, float, 4>::init()));
+    MTLG_TRY((GridShape<double, float, 8>::init()));
+    MTLG_TRY((GridShape<float, float, 4>::init()));
+    MTLG_TRY((GridShape<float, float, 8>::init()));
+    MTLG_TRY((GridShape<float, double, 4>::init()));
+    MTLG_TRY((GridShape<float, double, 8>::init()));
+    return MTLG_OK;
+}
+
+template <typename T, typename S, typename Fn>
+inline void with_grid_shape(int nw, Fn&& fn)
+{
+    if (nw == 8) fn(GridShape<T, S, 8>());
+    else fn(GridShape<T, S, 4>());
+}
+
+// Grid-sweep plan of a set whose factors all have grid layouts: compute
+// warps (the context's grid_warps, else 8 where the shared memory fits,
+// else 4), and per side the tiles of every system, taken round-robin over
+// the systems (a system's tiles plane block by plane block, y-blocks
+// ascending inside: every tile a tile reads comes earlier).  Systems with z
+// neighbours tile NW planes of one y-block (jw = 1), the others NW y-blocks.
+template <typename T, typename S>
+inline int plan_grid(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, const TriDev*>>& f, ChunkPlan& pl)
+{
+    int nw = c->grid_warps > 0 ? c->grid_warps : 8;
+    if (grid_smem_bytes<T, S>(nw) > kChunkSmemMax) nw = 4;
+    if (grid_smem_bytes<T, S>(nw) > kChunkSmemMax) return MTLG_OK;
+    int res = 0;
+    with_grid_shape<T, S>(nw, [&](auto shape) { res = decltype(shape)::resident(c); });
+    if (res < 1) return MTLG_OK;
+    int steps = 0;
+    for (int w = 0; w < 2; ++w) {
+        std::vector<std::vector<GroupTask>> per(f.size());
+        size_t most = 0;
+        for (size_t s = 0; s < f.size(); ++s) {
+            if (!f[s].first) continue;
+            const TriDev& F = w == 0 ? *f[s].first : *f[s].second;
+            steps = std::max(steps, F.gnsteps);
+            const int jw = (F.gdirs & 4) ? 1 : nw, kw = nw / jw;
+            for (int k0 = 0; k0 < F.gnz; k0 += kw)
+                for (int j0 = 0; j0 < F.gnjb; j0 += jw) per[s].push_back(GroupTask{int(s), j0, k0, jw});
+            most = std::max(most, per[s].size());
+        }
+        std::vector<GroupTask> g;
+        for (size_t a = 0; a < most; ++a)
+            for (size_t s = 0; s < f.size(); ++s)
+                if (a < per[s].size()) g.push_back(per[s][a]);
+        if (w == 0) {
+            pl.ntl = int(g.size());
+            MTLG_TRY(pl.tl.upload(c, g.data(), std::max<size_t>(1, g.size())));
+        } else {
+            pl.ntu = int(g.size());
+            MTLG_TRY(pl.tu.upload(c, g.data(), std::max<size_t>(1, g.size())));
+        }
+    }
+    pl.grid = true;
+    pl.gnw = nw;
+    pl.gsmem = grid_smem_bytes<T, S>(nw);
+    pl.gresident = res;
+    pl.gsteps = steps;
+    pl.ok = true;
+    return MTLG_OK;
+}
+
 template <typename T, typename S>
 inline int plan_chunks(mtlg_ctx* c, const std::vector<std::pair<const TriDev*, const TriDev*>>& f, ChunkPlan& pl)
 {
     pl.ok = false;
+    pl.grid = false;
     pl.side[0] = pl.side[1] = ChunkSide();
     pl.ntl = pl.ntu = 0;
+    if (c->grid_sweep && c->sweep_kernel == 0) {
+        bool all = false;
+        for (const auto& lu : f) {
+            if (!lu.first) continue;
+            const bool g = lu.first->gnx > 0 && lu.first->gval.p && lu.second->gnx > 0 && lu.second->gval.p;
+            if (!g) {
+                all = false;
+                break;
+            }
+            all = true;
+        }
+        if (all) {
+            MTLG_TRY((plan_grid<T, S>(c, f, pl)));
+            if (pl.ok) return MTLG_OK;
+        }
+    }
     bool any = false;
     for (const auto& lu : f) {
         if (!lu.first) continue;
@@ -640,6 +778,11 @@ template <typename T, typename S>
 inline int launch_chunk_sweep(mtlg_ctx* c, cudaStream_t st, const SetView& sv, ChunkSweepOp op, const ChunkPlan& plan)
 {
     if (op.ntasks == 0) return MTLG_OK;
+    if (plan.grid) {
+        int rc = MTLG_OK;
+        with_grid_shape<T, S>(plan.gnw, [&](auto shape) { rc = decltype(shape)::launch(c, st, sv, op, plan.gresident); });
+        return rc;
+    }
     const ChunkSide& pl = plan.side[op.which];
     op.vec_bytes = pl.vec_bytes;
     op.rows_cap = pl.seg_rows;
@@ -680,6 +823,19 @@ inline TriFactor tri_view(const TriDev& T)
         f.ccol = T.ccol.p;
         f.cval = T.cval.p;
         f.cdia = T.cdia.p;
+    }
+    if (T.gnx > 0 && T.gval.p) {
+        f.gnx = T.gnx;
+        f.gny = T.gny;
+        f.gnz = T.gnz;
+        f.gns = T.gns;
+        f.gperm = T.gperm;
+        f.gdirs = T.gdirs;
+        f.gskew = T.gskew;
+        f.gnsteps = T.gnsteps;
+        f.gnsp = T.gnsp;
+        f.gnjb = T.gnjb;
+        f.gdata = T.gval.p;
     }
     return f;
 }
@@ -751,8 +907,196 @@ inline int build_flat_entries(mtlg_ctx* c, const RowLists& F, TriDev& T)
     return MTLG_OK;
 }
 
+// Grid geometry of a triangular factor's pattern (natural row order): the
+// distinct offsets between a row and the rows it reads must be {1, nx} (2D)
+// or {1, nx, nx*ny} (3D) with n = nx*ny(*nz), every row must read exactly
+// its in-grid neighbours (x when i > 0, y when j > 0, z when k > 0; rows
+// counted from the sweep's start: r' = r for L, n - 1 - r for U), and the
+// rows' entries must follow one order of the directions (the slot order of
+// the layout).  A factor without entries (Jacobi's trivial factors) is a
+// grid of independent rows, run unskewed in lines of 256.
+inline bool detect_grid(const RowLists& F, int n, bool lower, TriDev& T)
+{
+    T.gnx = 0;
+    if (n < 1) return false;
+    constexpr int kBlk = 1 << 16;
+    const int nb = (n + kBlk - 1) / kBlk;
+    std::vector<long long> bo(size_t(nb) * 4, 0);
+    std::vector<int> bn(nb, 0);
+    parallel_for(nb, [&](int b) {
+        long long* o = bo.data() + size_t(b) * 4;
+        int cnt = 0;
+        const int r1 = std::min(n, (b + 1) * kBlk);
+        for (int r = b * kBlk; r < r1 && cnt <= 3; ++r)
+            for (int e = F.rp[r]; e < F.rp[r + 1]; ++e) {
+                const long long off = lower ? (long long)r - F.col[e] : (long long)F.col[e] - r;
+                bool seen = false;
+                for (int x = 0; x < cnt; ++x) seen |= o[x] == off;
+                if (seen) continue;
+                if (cnt == 3) {
+                    cnt = 4;   // more than three offsets: not a grid stencil
+                    break;
+                }
+                o[cnt++] = off;
+            }
+        bn[b] = cnt;
+    });
+    std::vector<long long> offs;
+    for (int b = 0; b < nb; ++b) {
+        if (bn[b] > 3) return false;
+        for (int x = 0; x < bn[b]; ++x)
+            if (std::find(offs.begin(), offs.end(), bo[size_t(b) * 4 + x]) == offs.end())
+                offs.push_back(bo[size_t(b) * 4 + x]);
+    }
+    if (offs.size() > 3) return false;
+    std::sort(offs.begin(), offs.end());
+    int nx, ny, nz;
+    if (offs.empty()) {
+        T.gnx = std::min(n, 256);
+        T.gny = (n + T.gnx - 1) / T.gnx;
+        T.gnz = 1;
+        T.gns = T.gperm = T.gdirs = T.gskew = 0;
+        return true;
+    }
+    if (offs.size() == 1 || offs[0] != 1 || offs[1] < 2 || offs[1] > n) return false;
+    nx = int(offs[1]);
+    if (offs.size() == 2) {
+        if (n % nx) return false;
+        ny = n / nx;
+        nz = 1;
+    } else {
+        if (offs[2] % offs[1] || offs[2] / offs[1] < 2 || n % offs[2]) return false;
+        ny = int(offs[2] / offs[1]);
+        nz = int(n / offs[2]);
+    }
+    if (ny < 2 || (offs.size() == 3 && nz < 2)) return false;
+    const int ns = int(offs.size());
+    auto dir_of = [&](long long off) { return off == 1 ? 0 : off == nx ? 1 : 2; };
+    // slot order: the directions of an interior row's entries
+    const long long rint = 1 + (long long)nx * (1 + (long long)ny * (ns == 3 ? 1 : 0));
+    if (rint >= n) return false;
+    const int ri = lower ? int(rint) : int(n - 1 - rint);
+    if (F.rp[ri + 1] - F.rp[ri] != ns) return false;
+    int perm = 0, rank[3] = {-1, -1, -1};
+    for (int q = 0; q < ns; ++q) {
+        const int e = F.rp[ri] + q;
+        const int d = dir_of(lower ? (long long)ri - F.col[e] : (long long)F.col[e] - ri);
+        if (rank[d] >= 0) return false;
+        rank[d] = q;
+        perm |= d << (2 * q);
+    }
+    // the kernel runs the farthest-first and nearest-first orders
+    if (ns == 3 ? (perm != kGridFar3 && perm != kGridNear3) : (perm != kGridFar2 && perm != kGridNear2)) return false;
+    // every row reads exactly its in-grid neighbours, in slot order
+    std::vector<char> bad(nb, 0);
+    parallel_for(nb, [&](int b) {
+        const int r1 = std::min(n, (b + 1) * kBlk);
+        for (int r = b * kBlk; r < r1; ++r) {
+            const long long rp = lower ? r : (long long)n - 1 - r;
+            const long long i = rp % nx, j = (rp / nx) % ny, k = rp / ((long long)nx * ny);
+            const int want = (i > 0) + (j > 0) + (k > 0);
+            if (F.rp[r + 1] - F.rp[r] != want) {
+                bad[b] = 1;
+                return;
+            }
+            int last = -1;
+            for (int e = F.rp[r]; e < F.rp[r + 1]; ++e) {
+                const long long off = lower ? (long long)r - F.col[e] : (long long)F.col[e] - r;
+                if (off != 1 && off != nx && off != (long long)nx * ny) {
+                    bad[b] = 1;
+                    return;
+                }
+                const int d = dir_of(off);
+                const bool inside = d == 0 ? i > 0 : d == 1 ? j > 0 : k > 0;
+                if (!inside || rank[d] < 0 || rank[d] <= last) {
+                    bad[b] = 1;
+                    return;
+                }
+                last = rank[d];
+            }
+        }
+    });
+    for (char x : bad)
+        if (x) return false;
+    T.gnx = nx;
+    T.gny = ny;
+    T.gnz = nz;
+    T.gns = ns;
+    T.gperm = perm;
+    T.gdirs = ns == 3 ? 7 : 3;
+    T.gskew = 1;
+    return true;
+}
+
+// Grid layout of a factor whose pattern detect_grid accepted: per unit,
+// step, slot and lane the value source and pivot row of the element
+// (k_fill_grid fills the values after the factorization).
+inline int build_grid(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev& T)
+{
+    T.gnx = 0;
+    T.gnent = 0;
+    if (!c->grid_sweep) return MTLG_OK;
+    {
+        MTLG_TRACE(9160, "pc.grid_detect");
+        if (!detect_grid(F, n, lower, T)) {
+            T.gnx = 0;
+            return MTLG_OK;
+        }
+    }
+    MTLG_TRACE(9161, "pc.grid_layout");
+    T.gnjb = (T.gny + 31) / 32;
+    T.gnsteps = T.gskew ? T.gnx + std::min(T.gny, 32) - 1 : T.gnx;
+    T.gnsp = (T.gnsteps + kGridStepPad - 1) / kGridStepPad * kGridStepPad;
+    const int se = (T.gns + 1) * 32;
+    const long long units = (long long)T.gnjb * T.gnz;
+    const long long nent = units * T.gnsp * se;
+    if (nent > (long long)INT32_MAX) {
+        T.gnx = 0;
+        return MTLG_OK;
+    }
+    hvec<int> gsrc(static_cast<size_t>(nent)), gmul(static_cast<size_t>(nent));
+    const int nx = T.gnx, ny = T.gny, ns = T.gns, perm = T.gperm, skew = T.gskew, nsteps = T.gnsteps;
+    const long long nxy = (long long)nx * ny;
+    parallel_for(int(units), [&](int u) {
+        const int ju = u % T.gnjb, k = u / T.gnjb;
+        long long e = (long long)u * T.gnsp * se;
+        for (int s = 0; s < T.gnsp; ++s)
+            for (int q = 0; q <= ns; ++q)
+                for (int l = 0; l < 32; ++l, ++e) {
+                    const int i = skew ? s - l : s, j = 32 * ju + l;
+                    const long long rp = i + (long long)nx * (j + (long long)ny * k);
+                    if (s >= nsteps || i < 0 || i >= nx || j >= ny || rp >= n) {
+                        gsrc[e] = -1;
+                        gmul[e] = -1;
+                        continue;
+                    }
+                    const int r = lower ? int(rp) : int(n - 1 - rp);
+                    if (q == ns) {
+                        gsrc[e] = -2;
+                        gmul[e] = r;
+                        continue;
+                    }
+                    const int d = (perm >> (2 * q)) & 3;
+                    const long long off = d == 0 ? 1 : d == 1 ? nx : nxy;
+                    const long long col = lower ? r - off : r + off;
+                    gsrc[e] = -1;
+                    gmul[e] = -1;
+                    for (int f = F.rp[r]; f < F.rp[r + 1]; ++f)
+                        if (F.col[f] == col) {
+                            gsrc[e] = F.src[f];
+                            gmul[e] = F.mul[f];
+                        }
+                }
+    });
+    MTLG_TRY(T.gsrc.upload(c, gsrc.data(), gsrc.size()));
+    MTLG_TRY(T.gmul.upload(c, gmul.data(), gmul.size()));
+    T.gnent = nent;
+    return MTLG_OK;
+}
+
 inline int build_tri(mtlg_ctx* c, RowLists&& F, int n, bool lower, TriDev& T, int chunk_rows, int ssz, bool defer_flat)
 {
+    MTLG_TRY(build_grid(c, F, n, lower, T));
     T.n = n;
     T.lower = lower;
     std::vector<int> lev;
@@ -946,6 +1290,24 @@ inline int fill_chunk_values(mtlg_pc* P, TriDev& T, const double* srcvals, const
     return MTLG_OK;
 }
 
+// Values of the grid layout (same sources and roundings as the chunked
+// layout's); the per-element sources are released afterwards.
+inline int fill_grid_values(mtlg_pc* P, TriDev& T, const double* srcvals, const double* inv_dia, int unit)
+{
+    mtlg_ctx* c = P->ctx;
+    if (T.gnx == 0 || T.gnent == 0) return MTLG_OK;
+    const int f32 = P->storage == MTLG_F32;
+    MTLG_TRY(T.gval.alloc(c, size_t(T.gnent) * P->ssize()));
+    k_fill_grid<<<launch_grid(T.gnent), 256, 0, c->stream>>>(T.gnent, T.gsrc.p, T.gmul.p, srcvals, inv_dia, unit,
+                                                           T.gval.p, f32);
+    c->launches++;
+    MTLG_CUDA(cudaGetLastError());
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));   // the sources are released next
+    T.gsrc.release();
+    T.gmul.release();
+    return MTLG_OK;
+}
+
 // Values of the flat layout: entries from `srcvals` (times the inverse
 // pivot named by mul), multipliers from the FP64 pivots (1 for a unit
 // diagonal).
@@ -1063,7 +1425,10 @@ inline int pc_build(mtlg_pc* P)
             c->launches += 3;
             MTLG_CUDA(cudaGetLastError());
         }
-        for (TriDev* T : {&P->L, &P->U}) MTLG_TRY(fill_chunk_values(P, *T, P->inv_dia.p, P->inv_dia.p, T == &P->U));
+        for (TriDev* T : {&P->L, &P->U}) {
+            MTLG_TRY(fill_chunk_values(P, *T, P->inv_dia.p, P->inv_dia.p, T == &P->U));
+            MTLG_TRY(fill_grid_values(P, *T, P->inv_dia.p, P->inv_dia.p, T == &P->U));
+        }
         return pc_setup_single_set(P);
     }
     if (!P->has_factors()) return pc_setup_single_set(P);
@@ -1204,6 +1569,7 @@ inline int pc_build(mtlg_pc* P)
         const int unit = (P->kind == MTLG_PC_ILU0 && T == &P->L);
         if (T->flat_entries) MTLG_TRY(fill_flat_values(P, *T, srcvals, unit));
         MTLG_TRY(fill_chunk_values(P, *T, srcvals, P->inv_dia.p, unit));
+        MTLG_TRY(fill_grid_values(P, *T, srcvals, P->inv_dia.p, unit));
     }
     int err = 0;
     MTLG_CUDA(cudaMemcpyAsync(&err, P->misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1311,6 +1677,7 @@ inline int pc_build_adjoint(mtlg_pc* P)
         }
         MTLG_CUDA(cudaGetLastError());
         MTLG_TRY(fill_chunk_values(Q.get(), *T, v64.p, Q->inv_dia.p, unit));
+        MTLG_TRY(fill_grid_values(Q.get(), *T, v64.p, Q->inv_dia.p, unit));
     }
     MTLG_CUDA(cudaStreamSynchronize(c->stream));
     P->adjoint = Q.release();

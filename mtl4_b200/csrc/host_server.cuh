@@ -472,6 +472,7 @@ int mtlg_server_step(mtlg_server* S)
             int z = 0;
             MTLG_CUDA(cudaMemcpy(ss.misc.p + 1, &z, sizeof z, cudaMemcpyHostToDevice));
             MTLG_CUDA(cudaMemset(ss.tickets.p, 0, 8 * sizeof(int)));
+            MTLG_TRY(reset_set_sweep_buffers(ss));
         }
     }
     // 2. admit queued requests while slots and memory allow

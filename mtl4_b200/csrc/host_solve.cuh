@@ -91,6 +91,21 @@ struct SolveSet {
     }
 };
 
+// After an expired device wait: the L sweeps' output (V_Z0) back to all
+// sentinel, as the flat and grid sweeps expect before a sweep (the L sweep
+// itself resets the U sweeps' outputs row by row).
+inline int reset_set_sweep_buffers(SolveSet& ss)
+{
+    if (ss.path != PATH_SWEEP) return MTLG_OK;
+    const size_t vb = ss.f32 ? 4 : 8;
+    for (int s = 0; s < ss.S && s < int(ss.h_desc.size()); ++s)
+        if (ss.h_desc[s].ws && ss.h_desc[s].ws_stride > 0)
+            MTLG_TRY(fill_sentinel(ss.ctx,
+                                   static_cast<unsigned char*>(ss.h_desc[s].ws) + size_t(V_Z0) * size_t(ss.h_desc[s].ws_stride) * vb,
+                                   size_t(ss.h_desc[s].ws_stride) * vb));
+    return MTLG_OK;
+}
+
 inline int plan_set_chunks(SolveSet& ss, const std::vector<const mtlg_pc*>& pcs);
 
 inline size_t vsize(int f32) { return f32 ? 4 : 8; }

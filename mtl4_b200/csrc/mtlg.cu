@@ -129,7 +129,7 @@ int pc_sweeps(mtlg_pc* P, const mtlg_vec* x, mtlg_vec* y)
     d.ws_stride = 0;
     ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
     int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
-    const int setting = c->sweep_kernel | (c->sweep_cluster << 4);
+    const int setting = plan_setting(c);
     if (made != setting) {
         std::vector<std::pair<const TriDev*, const TriDev*>> f(1, {&P->L, &P->U});
         MTLG_TRY((plan_chunks<T, S>(c, f, pl)));
@@ -406,6 +406,7 @@ int mtlg_ctx_create(int device, size_t hbm_budget, mtlg_ctx** out)
     c->sweep_grid = c->sm_count * c->sweep_max_bpsm;
     MTLG_TRY(init_kernel_shapes());
     MTLG_TRY(init_chunk_shapes());
+    MTLG_TRY(init_grid_shapes());
     {
         // stream-ordered pool of this context's device buffers, kept between
         // set-ups (release threshold: never); without one, cudaMalloc
@@ -479,6 +480,14 @@ int mtlg_ctx_set_tuning(mtlg_ctx* c, const char* key, int64_t value)
     else if (k == "spmv_kernel") c->spmv_kernel = int(std::max<int64_t>(0, std::min<int64_t>(value, 3)));
     else if (k == "sweep_sleep_ns") c->sweep_sleep_ns = int(std::max<int64_t>(0, std::min<int64_t>(value, 100000)));
     else if (k == "sweep_kernel") c->sweep_kernel = value ? 1 : 0;
+    else if (k == "grid_sweep") c->grid_sweep = value ? 1 : 0;
+    else if (k == "grid_warps") {
+        if (value != 0 && value != 4 && value != 8) {
+            set_error("grid_warps must be 0, 4 or 8");
+            return MTLG_ERR_INVALID_ARG;
+        }
+        c->grid_warps = int(value);
+    }
     else if (k == "pc_apply_sync") c->pc_apply_sync = value ? 1 : 0;
     else if (k == "reduction_order") c->red_order = value ? 1 : 0;
     else if (k == "spin_limit") c->spin_limit = std::max<int64_t>(0, value);
@@ -512,6 +521,8 @@ int mtlg_ctx_get_tuning(mtlg_ctx* c, const char* key, int64_t* value)
     else if (k == "sweep_sleep_ns") *value = c->sweep_sleep_ns;
     else if (k == "sm_count") *value = c->sm_count;
     else if (k == "sweep_kernel") *value = c->sweep_kernel;
+    else if (k == "grid_sweep") *value = c->grid_sweep;
+    else if (k == "grid_warps") *value = c->grid_warps;
     else if (k == "pc_apply_sync") *value = c->pc_apply_sync;
     else if (k == "reduction_order") *value = c->red_order;
     else if (k == "spin_limit") *value = c->spin_limit > 0 ? c->spin_limit : kSpinLimit;
@@ -1037,7 +1048,7 @@ static int sweep_plan_of(mtlg_ctx* c, mtlg_pc* P, int32_t* out)
 {
     ChunkPlan& pl = P->plan[sizeof(T) == 4 ? 1 : 0];
     int& made = P->plan_kernel[sizeof(T) == 4 ? 1 : 0];
-    const int setting = c->sweep_kernel | (c->sweep_cluster << 4);
+    const int setting = plan_setting(c);
     if (made != setting) {
         std::vector<std::pair<const TriDev*, const TriDev*>> f(1, {&P->L, &P->U});
         MTLG_TRY((plan_chunks<T, S>(c, f, pl)));
@@ -1045,6 +1056,15 @@ static int sweep_plan_of(mtlg_ctx* c, mtlg_pc* P, int32_t* out)
     }
     for (int i = 0; i < 8; ++i) out[i] = 0;
     if (!pl.ok) return MTLG_OK;
+    if (pl.grid) {
+        out[2] = pl.gresident;
+        out[3] = pl.gsmem;
+        out[4] = 32 * pl.gnw;
+        out[5] = P->L.gns;
+        out[6] = pl.ntl;
+        out[7] = pl.gsteps;
+        return MTLG_OK;
+    }
     const ChunkSide& sl = pl.side[0];
     out[0] = sl.rows;
     out[1] = P->L.nch;
@@ -1110,6 +1130,7 @@ static int timed_result(mtlg_ctx* c, SolveSet& ss, cudaEvent_t e0, cudaEvent_t e
         MTLG_CUDA(cudaMemcpy(ss.misc.p + 1, &z, sizeof z, cudaMemcpyHostToDevice));
         MTLG_CUDA(cudaMemset(ss.tickets.p, 0, 8 * sizeof(int)));
         for (auto& si : ss.in) MTLG_TRY(pc_reset_sweep_state(si.P));
+        MTLG_TRY(reset_set_sweep_buffers(ss));
         set_error("a device-side wait expired during the solve");
         return MTLG_ERR_TIMEOUT;
     }

@@ -166,13 +166,19 @@ class pc:
             return a.value, b.value
 
         def sweep_plan(self, dtype=np.float64) -> dict:
-            """Launch plan of the chunked sweeps for vectors of `dtype` under
-            the context's tuning (all zero: flat level-order sweeps)."""
+            """Launch plan of the sweeps for vectors of `dtype` under the
+            context's tuning: "kernel" is "grid" (grid-stencil factors: tiles,
+            steps per warp unit), "chunked" (chunk rows and count, staging) or
+            "flat" (level order, all other fields zero)."""
             out = (C.c_int * 8)()
             dt = _lib.F32 if np.dtype(dtype) == np.float32 else _lib.F64
             check(self.ctx._L.mtlg_pc_sweep_plan(self.ctx.h, self.h, dt, out), "sweep_plan")
+            v = list(out)
+            if v[1] == 0 and v[2] > 0:
+                keys = ("chunk_rows", "chunks", "resident", "smem", "threads", "entries", "tiles", "steps")
+                return dict(zip(keys, v), kernel="grid")
             keys = ("chunk_rows", "chunks", "resident", "smem", "threads", "entries", "seg_rows", "seg_ents")
-            return dict(zip(keys, list(out)))
+            return dict(zip(keys, v), kernel="chunked" if v[1] > 0 else "flat")
 
         def factor(self, which: str):
             """Stored factor ('L' or 'U') as (row_ptr, col, val) host arrays."""

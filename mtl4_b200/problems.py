@@ -131,20 +131,23 @@ def _face_diffusion(shape, kappa: np.ndarray, beta=None, h: float = 1.0) -> CSR:
     return _from_coo(N, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals))
 
 
-def vardiff_3d(m: int, sigma: float = 1.0, seed: int = 3, beta=None) -> CSR:
-    """SPD 7-point diffusion on an m^3 grid with log-normal cell coefficients
-    (kappa ~ exp(N(0, sigma^2)), seeded), face value = arithmetic mean of the
-    two cells, Dirichlet.  With beta, adds centred convection (nonsymmetric)."""
+def vardiff_3d(m, sigma: float = 1.0, seed: int = 3, beta=None) -> CSR:
+    """SPD 7-point diffusion on an m^3 grid (or an (nx, ny, nz) grid, x
+    fastest) with log-normal cell coefficients (kappa ~ exp(N(0, sigma^2)),
+    seeded), face value = arithmetic mean of the two cells, Dirichlet.  With
+    beta, adds centred convection (nonsymmetric)."""
+    shape = tuple(m) if isinstance(m, (tuple, list)) else (m, m, m)
     rng = np.random.default_rng(seed)
-    kappa = np.exp(sigma * rng.standard_normal(m ** 3))
-    return _face_diffusion((m, m, m), kappa, beta)
+    kappa = np.exp(sigma * rng.standard_normal(int(np.prod(shape))))
+    return _face_diffusion(shape, kappa, beta)
 
 
-def vardiff_2d(m: int, sigma: float = 1.0, seed: int = 3, beta=None) -> CSR:
-    """2D 5-point counterpart of :func:`vardiff_3d` on an m x m grid."""
+def vardiff_2d(m, sigma: float = 1.0, seed: int = 3, beta=None) -> CSR:
+    """2D 5-point counterpart of :func:`vardiff_3d` on an m x m (or (nx, ny)) grid."""
+    shape = tuple(m) if isinstance(m, (tuple, list)) else (m, m)
     rng = np.random.default_rng(seed)
-    kappa = np.exp(sigma * rng.standard_normal(m * m))
-    return _face_diffusion((m, m), kappa, beta)
+    kappa = np.exp(sigma * rng.standard_normal(int(np.prod(shape))))
+    return _face_diffusion(shape, kappa, beta)
 
 
 # Continuous Pareto (density ~ x^-alpha, alpha = 2.1) floored and clipped to

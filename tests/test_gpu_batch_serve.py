@@ -83,10 +83,11 @@ def test_served_mix_in_clusters(ctx):
     # small chunks and 4-CTA clusters: every request spans several chunks,
     # cluster groups hold CTAs without a chunk, and slots (slot 0 among
     # them) fall free while the others still run
-    old = {k: ctx.get_tuning(k) for k in ("chunk_rows", "sweep_cluster")}
+    old = {k: ctx.get_tuning(k) for k in ("chunk_rows", "sweep_cluster", "grid_sweep")}
     try:
         ctx.set_tuning("chunk_rows", 512)
         ctx.set_tuning("sweep_cluster", 4)
+        ctx.set_tuning("grid_sweep", 0)   # the chunked kernel, also for grid-stencil requests
         served_alone_equals_in_mix(ctx, True)
     finally:
         for k, v in old.items():

@@ -4,7 +4,8 @@ the oracle bit for bit at chunk sizes that put most dependencies in other
 chunks (32 rows), in the same chunk (whole matrix), and in between; waves
 larger than a CTA are split; the chunked and the flat level-order kernels give
 identical results; batched solves over many-chunk factors equal standalone
-solves."""
+solves.  Grid-stencil matrices run here with the grid layout switched off
+(grid_sweep 0), so the chunked kernel is the one under test."""
 import contextlib
 
 import numpy as np
@@ -87,7 +88,7 @@ def test_chunked_apply_matches_oracle(ctx, name, chunk_rows):
     from mtl4_b200 import itl
     A = PROBLEMS[name]()
     x = np.random.default_rng(5).standard_normal(A.n_rows)
-    with tuning(ctx, chunk_rows=chunk_rows, sweep_kernel=0):
+    with tuning(ctx, grid_sweep=0, chunk_rows=chunk_rows, sweep_kernel=0):
         Ad = dev(A, ctx)
         for kind in ("ilu_0", "ic_0"):
             for mode in ("f64", "f64s32", "f32"):
@@ -111,7 +112,7 @@ def test_cluster_pushes_match_oracle(ctx, cluster):
     A = P.vardiff_3d(24, sigma=1.0, seed=5, beta=(0.05, 0.02, 0.01))
     x = np.random.default_rng(12).standard_normal(A.n_rows)
     for chunk_rows in (96, 576, 2304):
-        with tuning(ctx, chunk_rows=chunk_rows, sweep_kernel=0, sweep_cluster=cluster):
+        with tuning(ctx, grid_sweep=0, chunk_rows=chunk_rows, sweep_kernel=0, sweep_cluster=cluster):
             Ad = dev(A, ctx)
             for kind, dt in (("ilu_0", np.float64), ("ic_0", np.float32)):
                 Pc = getattr(itl.pc, kind)(Ad, dt)
@@ -127,7 +128,7 @@ def test_batch_cluster_groups_match_standalone(ctx, cluster):
     from mtl4_b200 import itl, mtl, serve
     probs = [P.vardiff_3d(m, sigma=0.5, seed=m, beta=(0.05, 0.02, 0.01)) for m in (7, 9, 12, 15)]
     rhs = [P.random_rhs(A.n_rows, 4) for A in probs]
-    with tuning(ctx, chunk_rows=256, sweep_kernel=0, sweep_cluster=cluster):
+    with tuning(ctx, grid_sweep=0, chunk_rows=256, sweep_kernel=0, sweep_cluster=cluster):
         B = serve.batch(ctx)
         for A, b in zip(probs, rhs):
             B.add(A, b, "bicgstab", "ilu_0", max_iter=2000, rtol=1e-8)
@@ -148,7 +149,7 @@ def test_wave_split_beyond_cta(ctx):
     from mtl4_b200 import itl
     A = paired_blocks(9001)
     x = np.random.default_rng(3).standard_normal(A.n_rows)
-    with tuning(ctx, chunk_rows=8192, sweep_kernel=0):
+    with tuning(ctx, grid_sweep=0, chunk_rows=8192, sweep_kernel=0):
         Pc = itl.pc.ilu_0(dev(A, ctx))
         y = itl.solve(Pc, vec(x, ctx)).numpy()
     assert np.array_equal(y, O.port_pc_apply(A, "ilu_0", x))
@@ -158,13 +159,13 @@ def test_chunked_equals_flat(ctx):
     from mtl4_b200 import itl
     A = P.vardiff_3d(24, sigma=1.0, seed=3, beta=(0.05, 0.02, 0.01))
     x = np.random.default_rng(9).standard_normal(A.n_rows)
-    with tuning(ctx, chunk_rows=1024, sweep_kernel=0):
+    with tuning(ctx, grid_sweep=0, chunk_rows=1024, sweep_kernel=0):
         Ad = dev(A, ctx)
         pcs = [itl.pc.ilu_0(Ad), itl.pc.ic_0(Ad, np.float32)]
     for Pc in pcs:
-        with tuning(ctx, sweep_kernel=0):
+        with tuning(ctx, grid_sweep=0, sweep_kernel=0):
             y0 = itl.solve(Pc, vec(x, ctx)).numpy()
-        with tuning(ctx, sweep_kernel=1):
+        with tuning(ctx, grid_sweep=0, sweep_kernel=1):
             y1 = itl.solve(Pc, vec(x, ctx)).numpy()
         assert np.array_equal(y0, y1)
 
@@ -179,10 +180,10 @@ def test_flat_solve_after_chunked_setup(ctx, solver, kind):
     b = np.random.default_rng(3).standard_normal(A.n_rows)
     out = []
     for flat in (0, 1):
-        with tuning(ctx, chunk_rows=1024, sweep_kernel=0):
+        with tuning(ctx, grid_sweep=0, chunk_rows=1024, sweep_kernel=0):
             Ad = dev(A, ctx)
             Pc = getattr(itl.pc, kind)(Ad)
-        with tuning(ctx, sweep_kernel=flat):
+        with tuning(ctx, grid_sweep=0, sweep_kernel=flat):
             x = mtl.dense_vector(A.n_rows, np.float64, ctx)
             bd = vec(b, ctx)
             it = itl.basic_iteration(bd, 1000, 1e-10)
@@ -198,7 +199,7 @@ def test_chunked_repeated_applies_keep_invariants(ctx):
     from mtl4_b200 import itl
     A = P.vardiff_2d(64, sigma=1.0, seed=2)
     x = np.random.default_rng(4).standard_normal(A.n_rows)
-    with tuning(ctx, chunk_rows=256, sweep_kernel=0):
+    with tuning(ctx, grid_sweep=0, chunk_rows=256, sweep_kernel=0):
         Pc = itl.pc.ic_0(dev(A, ctx))
         ys = [itl.solve(Pc, vec(x, ctx)).numpy() for _ in range(3)]
     assert all(np.array_equal(ys[0], y) for y in ys[1:])
@@ -210,7 +211,7 @@ def test_batch_many_chunks_matches_standalone(ctx, solver, kind):
     from mtl4_b200 import itl, mtl, serve
     probs = [P.vardiff_3d(m, sigma=0.5, seed=m, beta=(0.05, 0.02, 0.01)) for m in (10, 14, 17)]
     rhs = [P.random_rhs(A.n_rows, 3) for A in probs]
-    with tuning(ctx, chunk_rows=128, sweep_kernel=0):
+    with tuning(ctx, grid_sweep=0, chunk_rows=128, sweep_kernel=0):
         B = serve.batch(ctx)
         for A, b in zip(probs, rhs):
             B.add(A, b, solver, kind, max_iter=2000, rtol=1e-8)
@@ -239,11 +240,11 @@ def test_expired_dependency_waits_report_timeout_and_recover(ctx, cluster):
     A = P.convdiff_3d(40)
     v = np.random.default_rng(5).standard_normal(A.n_rows).astype(np.float32)
     want = O.port_pc_apply(A, "ilu_0", v)
-    with tuning(ctx, chunk_rows=1600, sweep_cluster=cluster):
+    with tuning(ctx, grid_sweep=0, chunk_rows=1600, sweep_cluster=cluster):
         Pc = itl.pc.ilu_0(dev(A, ctx), np.float32)
         assert Pc.sweep_plan(np.float32)["chunks"] >= 16
         assert np.array_equal(itl.solve(Pc, vec(v, ctx, np.float32)).numpy(), want)
-        with tuning(ctx, spin_limit=1):
+        with tuning(ctx, grid_sweep=0, spin_limit=1):
             with pytest.raises(_lib.device_timeout):
                 itl.solve(Pc, vec(v, ctx, np.float32))
         for _ in range(2):
@@ -266,11 +267,11 @@ def test_expired_waits_in_a_solve_report_timeout_and_recover(ctx):
         itl.bicgstab(Ad, x, vec(b, ctx), Pc, it)
         return x.numpy(), it
 
-    with tuning(ctx, chunk_rows=1024):
+    with tuning(ctx, grid_sweep=0, chunk_rows=1024):
         Pa = itl.pc.ilu_0(Ad, np.float64)
         Pb = itl.pc.ilu_0(Ad, np.float64)
         x0, it0 = solve(Pa)
-        with tuning(ctx, spin_limit=1):
+        with tuning(ctx, grid_sweep=0, spin_limit=1):
             with pytest.raises(_lib.device_timeout):
                 solve(Pb)
         Pc = itl.pc.ilu_0(Ad, np.float64)
