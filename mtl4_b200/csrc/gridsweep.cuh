@@ -438,6 +438,61 @@ __global__ void __launch_bounds__(32 * (NW + kGridRecvWarps)) k_sweep_grid(SetVi
     }
 }
 
+// Grid layout values straight from the matrix's CSR (no per-element index
+// arrays): element (unit, step, slot, lane) is row r's entry of the slot's
+// direction, found in A's row, with the sources and pivot rows of the
+// preconditioner's factor row lists -- ILU(0): the entry (r, c) of the
+// factorized values, no pivot; IC(0): L's (r, c) is a_cr times the inverse
+// pivot of c, U's (r, c) is a_rc times the inverse pivot of r -- and the
+// multiplier slot the inverse pivot of r (1 for a unit diagonal); padding +0.
+// The same values and roundings as k_fill_grid and the chunked layout's fill.
+struct GridFillGeom {
+    int n, nx, ny, nz, ns, perm, skew, nsteps, nsp, njb;
+};
+constexpr int kGridFillILU = 0, kGridFillIC = 1;
+__global__ void k_fill_grid_csr(long long nent, GridFillGeom g, int lower, int kind, int unit,
+                                const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ src,
+                                const double* __restrict__ inv_dia, void* val, int f32)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nent;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int lane = int(e & 31);
+        long long rest = e >> 5;
+        const int q = int(rest % (g.ns + 1));
+        rest /= (g.ns + 1);
+        const int s = int(rest % g.nsp);
+        const long long u = rest / g.nsp;
+        const int ju = int(u % g.njb), k = int(u / g.njb);
+        const int i = g.skew ? s - lane : s, j = 32 * ju + lane;
+        const long long rpr = i + (long long)g.nx * (j + (long long)g.ny * k);
+        double v = 0.0;
+        if (s < g.nsteps && i >= 0 && i < g.nx && j < g.ny && rpr < g.n) {
+            const int r = lower ? int(rpr) : int(g.n - 1 - rpr);
+            if (q == g.ns) {
+                v = unit ? 1.0 : inv_dia[r];
+            } else {
+                const int d = (g.perm >> (2 * q)) & 3;
+                const bool present = d == 0 ? i > 0 : d == 1 ? j > 0 : k > 0;
+                if (present) {
+                    const long long off = d == 0 ? 1 : d == 1 ? g.nx : (long long)g.nx * g.ny;
+                    const int c = int(lower ? r - off : r + off);
+                    const bool tr = kind == kGridFillIC && lower;   // IC(0)'s L holds the transposed upper entries
+                    const int row = tr ? c : r, col = tr ? r : c;
+                    int pos = -1;
+                    for (int f = rp[row]; f < rp[row + 1]; ++f)
+                        if (ci[f] == col) pos = f;
+                    if (pos >= 0) {
+                        v = src[pos];
+                        if (kind == kGridFillIC) v = v * inv_dia[lower ? c : r];
+                    }
+                }
+            }
+        }
+        if (f32) static_cast<float*>(val)[e] = float(v);
+        else static_cast<double*>(val)[e] = v;
+    }
+}
+
 // Grid layout values: per element a value source (>= 0, times the inverse
 // pivot named by gmul when >= 0), -2 for a row's multiplier (the inverse
 // pivot of row gmul, 1 for a unit diagonal), -1 for padding (+0).

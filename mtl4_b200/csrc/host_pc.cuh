@@ -48,6 +48,7 @@ struct TriDev {
     // pivot row (kept until the values are filled), the values (type S)
     int gnx = 0, gny = 0, gnz = 0, gns = 0, gperm = 0, gdirs = 0, gskew = 0, gnsteps = 0, gnsp = 0, gnjb = 0;
     long long gnent = 0;
+    bool grid_indices = true;   // false: values filled straight from the matrix's CSR (no gsrc / gmul)
     DBuf<int> gsrc, gmul;
     DBuf<unsigned char> gval;
 };
@@ -1054,6 +1055,8 @@ inline int build_grid(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev&
         T.gnx = 0;
         return MTLG_OK;
     }
+    T.gnent = nent;
+    if (!T.grid_indices) return MTLG_OK;
     hvec<int> gsrc(static_cast<size_t>(nent)), gmul(static_cast<size_t>(nent));
     const int nx = T.gnx, ny = T.gny, ns = T.gns, perm = T.gperm, skew = T.gskew, nsteps = T.gnsteps;
     const long long nxy = (long long)nx * ny;
@@ -1090,7 +1093,6 @@ inline int build_grid(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev&
     });
     MTLG_TRY(T.gsrc.upload(c, gsrc.data(), gsrc.size()));
     MTLG_TRY(T.gmul.upload(c, gmul.data(), gmul.size()));
-    T.gnent = nent;
     return MTLG_OK;
 }
 
@@ -1298,6 +1300,16 @@ inline int fill_grid_values(mtlg_pc* P, TriDev& T, const double* srcvals, const 
     if (T.gnx == 0 || T.gnent == 0) return MTLG_OK;
     const int f32 = P->storage == MTLG_F32;
     MTLG_TRY(T.gval.alloc(c, size_t(T.gnent) * P->ssize()));
+    if (!T.grid_indices) {
+        const GridFillGeom g = {T.n, T.gnx, T.gny, T.gnz, T.gns, T.gperm, T.gskew, T.gnsteps, T.gnsp, T.gnjb};
+        const int kind = P->kind == MTLG_PC_IC0 ? kGridFillIC : kGridFillILU;
+        k_fill_grid_csr<<<launch_grid(T.gnent), 256, 0, c->stream>>>(T.gnent, g, T.lower ? 1 : 0, kind, unit,
+                                                                   P->A->rp.p, P->A->ci.p, srcvals, inv_dia,
+                                                                   T.gval.p, f32);
+        c->launches++;
+        MTLG_CUDA(cudaGetLastError());
+        return MTLG_OK;
+    }
     k_fill_grid<<<launch_grid(T.gnent), 256, 0, c->stream>>>(T.gnent, T.gsrc.p, T.gmul.p, srcvals, inv_dia, unit,
                                                            T.gval.p, f32);
     c->launches++;
@@ -1408,6 +1420,7 @@ inline int pc_build(mtlg_pc* P)
         RowLists E;
         E.rp.assign(n + 1, 0);
         const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
+        P->L.grid_indices = P->U.grid_indices = false;
         MTLG_TRY(build_tri(c, RowLists(E), n, true, P->L, B, int(P->ssize()), false));
         MTLG_TRY(build_tri(c, RowLists(E), n, false, P->U, B, int(P->ssize()), false));
         MTLG_TRY(P->L.val.alloc(c, 16));
@@ -1502,6 +1515,7 @@ inline int pc_build(mtlg_pc* P)
     }
     }
     const int B = c->sweep_kernel == 0 ? default_chunk_rows(c, P->storage) : 0;
+    P->L.grid_indices = P->U.grid_indices = false;   // grid values straight from the CSR
     {
         // the two factors' schedules are independent: U on a second host thread
         MTLG_TRACE(9102, "pc.schedule");
