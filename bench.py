@@ -49,7 +49,7 @@ PEAKS = ROOT / "MEASURED_PEAKS.json"
 # DRAM bytes (read + write) of one FP32 ILU(0) apply (the L and U sweep
 # launches) from one ncu capture of this workload, per sweep kernel
 TRAFFIC_PER_APPLY = {"chunked": 210_680_000,   # k_sweep_chunk: 105.1 MB (L) + 105.5 MB (U)
-                     "grid": None}
+                     "grid": 104_306_000}      # k_sweep_grid: 52.28 MB (L) + 52.03 MB (U)
 FALLBACK_HBM = 6650.0
 
 

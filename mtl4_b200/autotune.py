@@ -12,6 +12,8 @@ Knobs and what measures them:
   chunk_rows       rows per chunk of the chunked triangular sweeps; read when
                    a preconditioner is built, so each candidate rebuilds it
   sweep_cluster    CTAs per cluster of the chunked sweeps (0 automatic)
+  grid_warps       compute warps per CTA of the grid sweeps (grid-stencil
+                   factors; 0 automatic)                       (tune_pc)
   sweep_sleep_ns   back-off of the sweeps' dependency polls    (tune_pc)
   vec_ctas_per_sm  CTAs per SM of the vector passes of the Krylov loops
                                                                (tune_vec)
@@ -44,6 +46,7 @@ SPMV_KERNELS = (0, 1, 2, 3)
 VEC_CTAS = (1, 2, 4, 8)
 SWEEP_CLUSTERS = (0, 1, 2, 4, 8, 16)
 CHUNK_ROWS = (0, 4096, 8192, 16384, 32768)
+GRID_WARPS = (0, 4, 8)
 
 
 def row_histogram(row_ptr: np.ndarray) -> list[int]:
@@ -221,7 +224,9 @@ def tune_pc(ctx, Ad, kind: str, value=np.float32, cache: Cache | None = None, re
             gpu: str | None = None, space: dict | None = None):
     """Chooses chunk_rows and sweep_cluster for preconditioner `kind`
     ("ilu_0" or "ic_0", stored in `value`) of device matrix Ad by timing its
-    apply; each chunk_rows candidate builds the preconditioner anew."""
+    apply; each chunk_rows candidate builds the preconditioner anew.  A
+    preconditioner swept by the grid kernel (grid-stencil factors) tunes
+    grid_warps instead."""
     from . import itl, mtl
     cache = cache or Cache()
     dt = np.dtype(value)
@@ -229,12 +234,16 @@ def tune_pc(ctx, Ad, kind: str, value=np.float32, cache: Cache | None = None, re
     hit = _cached(cache, key, ctx)
     if hit is not None:
         return hit, True
-    space = space or {"chunk_rows": CHUNK_ROWS, "sweep_cluster": SWEEP_CLUSTERS}
     n = Ad.shape[0]
     x = mtl.dense_vector(np.ones(n, dt), dt, ctx)
     y = mtl.dense_vector(n, dt, ctx)
     built = {}
     cls = getattr(itl.pc, kind)
+    if space is None:
+        probe = cls(Ad, dt, tune=False)
+        grid = probe.sweep_plan(dt).get("kernel") == "grid"
+        del probe
+        space = {"grid_warps": GRID_WARPS} if grid else {"chunk_rows": CHUNK_ROWS, "sweep_cluster": SWEEP_CLUSTERS}
 
     def measure(c):
         apply_settings(ctx, c)
@@ -300,6 +309,7 @@ def tune_batch(ctx, systems, solver: str = "cg", pc: str = "ic_0", mixed: bool =
     if space is None:
         space = {"vec_ctas_per_sm": VEC_CTAS}
         if pc in ("ilu_0", "ic_0"):
+            space["grid_warps"] = GRID_WARPS
             space["sweep_cluster"] = SWEEP_CLUSTERS
             space["chunk_rows"] = CHUNK_ROWS
     start = {k: 0 for k in space}

@@ -493,6 +493,33 @@ __global__ void k_fill_grid_csr(long long nent, GridFillGeom g, int lower, int k
     }
 }
 
+// Flat-layout values copied from the grid layout (a factor built with the
+// grid layout only, when a flat sweep, a factor download or the ILU(0)
+// adjoint needs its flat layout): flat position p is row row_of[p], its
+// entry k (column ci[k]) the grid element of that row and direction.
+__global__ void k_flat_from_grid(int npos, const int* __restrict__ row_of, const int* __restrict__ rp,
+                                 const int* __restrict__ ci, GridFillGeom g, int lower,
+                                 const unsigned char* __restrict__ gval, unsigned char* __restrict__ val, int ssz)
+{
+    int rank[3] = {-1, -1, -1};
+    for (int q = 0; q < g.ns; ++q) rank[(g.perm >> (2 * q)) & 3] = q;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npos; p += gridDim.x * blockDim.x) {
+        const int r = row_of[p];
+        if (r < 0) continue;
+        const long long rpr = lower ? r : (long long)g.n - 1 - r;
+        const int i = int(rpr % g.nx), j = int((rpr / g.nx) % g.ny), k = int(rpr / ((long long)g.nx * g.ny));
+        const long long u = (long long)k * g.njb + j / 32;
+        const int lane = j & 31, s = g.skew ? i + lane : i;
+        for (int e = rp[p]; e < rp[p + 1]; ++e) {
+            const long long off = lower ? (long long)r - ci[e] : (long long)ci[e] - r;
+            const int d = off == 1 ? 0 : off == g.nx ? 1 : 2;
+            const long long src = ((u * g.nsp + s) * (g.ns + 1) + rank[d]) * 32 + lane;
+            if (ssz == 8) reinterpret_cast<double*>(val)[e] = reinterpret_cast<const double*>(gval)[src];
+            else reinterpret_cast<float*>(val)[e] = reinterpret_cast<const float*>(gval)[src];
+        }
+    }
+}
+
 // Grid layout values: per element a value source (>= 0, times the inverse
 // pivot named by gmul when >= 0), -2 for a row's multiplier (the inverse
 // pivot of row gmul, 1 for a unit diagonal), -1 for padding (+0).

@@ -1099,6 +1099,10 @@ inline int build_grid(mtlg_ctx* c, const RowLists& F, int n, bool lower, TriDev&
 inline int build_tri(mtlg_ctx* c, RowLists&& F, int n, bool lower, TriDev& T, int chunk_rows, int ssz, bool defer_flat)
 {
     MTLG_TRY(build_grid(c, F, n, lower, T));
+    // a factor swept on its grid layout (values filled from the CSR) needs no
+    // chunked layout; its flat entries come on first need (ensure_flat)
+    const bool grid_only = T.gnx > 0 && !T.grid_indices;
+    if (grid_only) chunk_rows = 0;
     T.n = n;
     T.lower = lower;
     std::vector<int> lev;
@@ -1167,7 +1171,7 @@ inline int build_tri(mtlg_ctx* c, RowLists&& F, int n, bool lower, TriDev& T, in
     T.nnz = F.rp[n];
     ph.end();
     MTLG_TRY(build_chunks(c, F, lev, n, lower, chunk_rows, ssz, T));
-    if (T.nch == 0 || !defer_flat) return build_flat_entries(c, F, T);
+    if ((T.nch == 0 && !grid_only) || !defer_flat) return build_flat_entries(c, F, T);
     T.F = std::move(F);
     return MTLG_OK;
 }
@@ -1377,7 +1381,15 @@ inline int ensure_flat(mtlg_pc* P)
         const int unit = (P->kind == MTLG_PC_ILU0 && T == &P->L);
         MTLG_TRY(T->val.alloc(c, size_t(std::max(T->nnz, 1)) * P->ssize()));
         MTLG_TRY(T->dia.alloc(c, size_t(std::max(T->npad, 1)) * P->ssize()));
-        if (T->nnz) {
+        if (T->nnz && T->nch == 0 && T->gnx > 0 && T->gval.p) {
+            // values from the grid layout
+            const GridFillGeom g = {T->n, T->gnx, T->gny, T->gnz, T->gns, T->gperm, T->gskew, T->gnsteps, T->gnsp, T->gnjb};
+            k_flat_from_grid<<<launch_grid(T->npad), 256, 0, c->stream>>>(T->npad, T->row_of.p, T->rp.p, T->ci.p, g,
+                                                                          T->lower ? 1 : 0, T->gval.p, T->val.p,
+                                                                          int(P->ssize()));
+            c->launches++;
+            MTLG_CUDA(cudaGetLastError());
+        } else if (T->nnz) {
             DBuf<int> inv;
             const int64_t asz = std::max<int64_t>(1, P->A->nnz);
             MTLG_TRY(inv.alloc(c, size_t(asz)));

@@ -98,10 +98,13 @@ def test_autotune_wired_into_pc_solve_mult_and_batch(tmp_path):
     try:
         A = P.vardiff_2d(96, seed=3)
         Ad = mtl.compressed2D.from_problem(A, ctx)
-        Pc = itl.pc.ic_0(Ad, np.float32)          # tunes chunk_rows / sweep_cluster
+        Pc = itl.pc.ic_0(Ad, np.float32)          # tunes grid_warps (a grid stencil), else chunk_rows / sweep_cluster
         assert ("pc", "ic_0", "float32") in Ad._tuned
         ch = Ad._tuned[("pc", "ic_0", "float32")]
-        assert ch["chunk_rows"] in autotune.CHUNK_ROWS and ch["sweep_cluster"] in autotune.SWEEP_CLUSTERS
+        if "grid_warps" in ch:
+            assert ch["grid_warps"] in autotune.GRID_WARPS and Pc.sweep_plan(np.float32)["kernel"] == "grid"
+        else:
+            assert ch["chunk_rows"] in autotune.CHUNK_ROWS and ch["sweep_cluster"] in autotune.SWEEP_CLUSTERS
         # the tuned preconditioner is still the reference's apply
         r = np.random.default_rng(1).standard_normal(A.n_rows).astype(np.float32)
         assert np.array_equal(itl.solve(Pc, mtl.dense_vector(r, np.float32, ctx)).numpy(),

@@ -77,9 +77,8 @@ def test_grid_apply_matches_oracle(ctx, name, warps):
             for mode, vt, st in MODES:
                 Pc = getattr(itl.pc, kind)(Ad, st)
                 plan = Pc.sweep_plan(vt)
-                # eight warps where their shared memory fits (FP32 vectors and factors), else four
-                fits = warps == 4 or (vt == np.float32 and st == np.float32)
-                assert plan["kernel"] == "grid" and plan["threads"] == 32 * (warps if fits else 4), (name, plan)
+                # the context's warp count where its shared memory fits, else four
+                assert plan["kernel"] == "grid" and plan["threads"] in (128, 32 * warps), (name, plan)
                 want = oracle_apply(A, kind, x, vt, st)
                 if want is None:
                     with tuning(ctx, grid_sweep=0):
@@ -193,3 +192,22 @@ def test_grid_expired_waits_in_a_solve_recover(ctx):
     x2, it2 = solve(Pa)
     assert it0.is_converged() and it1.iterations() == it0.iterations() and np.array_equal(x1, x0)
     assert it2.iterations() == it0.iterations() and np.array_equal(x2, x0)
+
+
+@pytest.mark.parametrize("kind", ["ilu_0", "ic_0"])
+def test_flat_sweep_after_grid_setup(ctx, kind):
+    # a preconditioner set up with the grid layout only gets its flat layout
+    # on first need (values copied from the grid layout): a flat-sweep apply
+    # (sweep_kernel 1) and the factor download are the oracle's bit for bit
+    from mtl4_b200 import itl
+    A = P.vardiff_3d((40, 36, 9), sigma=0.7, seed=9, beta=(0.2, 0.1, 0.05))
+    Ad = dev(A, ctx)
+    x = np.random.default_rng(7).standard_normal(A.n_rows)
+    for st in (np.float64, np.float32):
+        Pc = getattr(itl.pc, kind)(Ad, st)
+        assert Pc.sweep_plan(np.float64)["kernel"] == "grid"
+        with tuning(ctx, sweep_kernel=1):
+            y = itl.solve(Pc, vec(x, ctx)).numpy()
+        assert np.array_equal(y, O.port_pc_apply(A, kind, x, storage_f32=(st == np.float32)))
+        y2 = itl.solve(Pc, vec(x, ctx)).numpy()   # back on the grid sweep
+        assert np.array_equal(y2, y)
