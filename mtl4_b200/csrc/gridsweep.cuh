@@ -44,18 +44,27 @@ static_assert(kGridRecvWarps * kGridBatch <= kGridRing, "receiver batches in fli
 static_assert(kGridStepPad % kGridG == 0, "layout padding must hold whole staged blocks");
 static_assert(kGridRhs >= 3 * kGridG, "the right-hand-side ring holds the current block and two ahead");
 
-// Staged S elements per compute warp (kGridNB blocks of up to four slots).
-template <typename S>
+// Row operations of the grid kernel: a triangular sweep, or the FP64 pivots
+// of an ILU(0) or IC(0) factorization (the same dependencies: a row's pivot
+// needs its three earlier neighbours' pivots).
+constexpr int kGridSweep = 0, kGridILU0 = 1, kGridIC0 = 2;
+// Slots per step (capacity): a sweep's entries and multiplier fit four; an
+// ILU(0) pivot reads its L entries, the neighbours' entries in its column and
+// its diagonal (up to seven).
+__host__ __device__ constexpr int grid_cap(int opk) { return opk == kGridILU0 ? 8 : 4; }
+
+// Staged S elements per compute warp (kGridNB blocks of up to grid_cap slots).
+template <typename S, int OPK = kGridSweep>
 __host__ __device__ constexpr int grid_stage_elems()
 {
-    return kGridNB * kGridG * 4 * 32;
+    return kGridNB * kGridG * grid_cap(OPK) * 32;
 }
 
 // Dynamic shared memory of a k_sweep_grid CTA of nw compute warps.
-template <typename T, typename S>
+template <typename T, typename S, int OPK = kGridSweep>
 __host__ __device__ inline int grid_smem_bytes(int nw)
 {
-    return nw * (grid_stage_elems<S>() * int(sizeof(S)) + (kGridRhs + kGridRing) * 32 * int(sizeof(T)) +
+    return nw * (grid_stage_elems<S, OPK>() * int(sizeof(S)) + (kGridRhs + kGridRing) * 32 * int(sizeof(T)) +
                  kGridRing * int(sizeof(T)));
 }
 
@@ -170,13 +179,13 @@ struct GridWarp {
 // a row at every step run without per-step validity tests.  NS entries per
 // row, FAR: the farthest neighbour's entry first (z, y, x; else x, y, z),
 // REV: rows counted from the end (U sweeps).
-template <typename T, typename S, int NS, bool FAR, bool REV>
+template <typename T, typename S, int NS, bool FAR, bool REV, int OPK = kGridSweep>
 __device__ __forceinline__ void grid_warp_run(const GridWarp<T, S>& g, unsigned& phase)
 {
     typedef typename std::conditional<(sizeof(S) > sizeof(T)), S, T>::type W;   // promoted type
     constexpr int G = kGridG;
-    constexpr int SES = (NS + 1) * 32;   // S elements per step
-    constexpr int BE = G * 4 * 32;       // S elements per staged block (capacity)
+    constexpr int SES = (OPK == kGridILU0 ? 2 * NS + 1 : NS + 1) * 32;   // S elements per step
+    constexpr int BE = G * grid_cap(OPK) * 32;                          // S elements per staged block (capacity)
     constexpr bool SKEW = NS > 0;        // rows depend on the lane below: lane l runs row i at step i + l
     const int lane = g.lane;
     const int nblk = (g.nsteps + G - 1) / G;
@@ -188,7 +197,7 @@ __device__ __forceinline__ void grid_warp_run(const GridWarp<T, S>& g, unsigned&
         }
     // right-hand sides of block m into their ring cells (one cp.async group)
     auto fetch = [&](int m) {
-        if (m < nblk) {
+        if (OPK == kGridSweep && m < nblk) {
             const int i0 = SKEW ? m * G - lane : m * G;
             const long long r0 = g.rbase + i0;
             const T* p = g.vin + (REV ? (long long)g.n - 1 - r0 : r0);
@@ -235,8 +244,36 @@ __device__ __forceinline__ void grid_warp_run(const GridWarp<T, S>& g, unsigned&
                     wl = lane == 0 ? T(0) : wy;
                 }
                 const S* e = bk + u * SES;
-                T acc = rc[u << 5];
-                if (NS == 3) {
+                T acc = OPK == kGridSweep ? rc[u << 5] : T(e[(SES / 32 - 1) * 32]);   // a pivot starts from a_ii
+                if constexpr (OPK == kGridILU0) {
+                    // k_ilu0_factor on a grid stencil: per earlier neighbour k
+                    // (ascending column) l = a_ik / u_kk (rounded), u_ii -= l a_ki
+                    // (fused); L's entries and the other U entries do not change
+                    if (NS == 3) {
+                        acc = __fma_rn(-__dmul_rn(e[0], wz), e[96], acc);
+                        acc = __fma_rn(-__dmul_rn(e[32], wl), e[128], acc);
+                        acc = __fma_rn(-__dmul_rn(e[64], wx), e[160], acc);
+                    } else if (NS == 2) {
+                        acc = __fma_rn(-__dmul_rn(e[0], wl), e[64], acc);
+                        acc = __fma_rn(-__dmul_rn(e[32], wx), e[96], acc);
+                    }
+                } else if constexpr (OPK == kGridIC0) {
+                    // k_ic0_factor: d = a_ki / sqrt(u_kk) (rounded), u_ii -= d d
+                    // (rounded product), per earlier neighbour k ascending
+                    if (NS == 3) {
+                        T d = __dmul_rn(e[0], wz);
+                        acc = __dsub_rn(acc, __dmul_rn(d, d));
+                        d = __dmul_rn(e[32], wl);
+                        acc = __dsub_rn(acc, __dmul_rn(d, d));
+                        d = __dmul_rn(e[64], wx);
+                        acc = __dsub_rn(acc, __dmul_rn(d, d));
+                    } else if (NS == 2) {
+                        T d = __dmul_rn(e[0], wl);
+                        acc = __dsub_rn(acc, __dmul_rn(d, d));
+                        d = __dmul_rn(e[32], wx);
+                        acc = __dsub_rn(acc, __dmul_rn(d, d));
+                    }
+                } else if constexpr (NS == 3) {
                     if (FAR) {
                         acc = sweep_step<T, S>(acc, e[0], wz);
                         acc = sweep_step<T, S>(acc, e[32], wl);
@@ -255,7 +292,10 @@ __device__ __forceinline__ void grid_warp_run(const GridWarp<T, S>& g, unsigned&
                         acc = sweep_step<T, S>(acc, e[32], wl);
                     }
                 }
-                T out = unsentinel(T(W(acc) * W(e[NS * 32])));
+                T out;
+                if constexpr (OPK == kGridILU0) out = unsentinel(T(__ddiv_rn(1.0, double(acc))));
+                else if constexpr (OPK == kGridIC0) out = unsentinel(T(__ddiv_rn(1.0, __dsqrt_rn(double(acc)))));
+                else out = unsentinel(T(W(acc) * W(e[NS * 32])));
                 if (EDGE) out = valid ? out : T(0);   // +0 outside the lane's line: an absent neighbour
                 st_relaxed_gpu_if(REV ? po - u : po + u, out, valid);
                 if (pr && valid) *(REV ? pr - u : pr + u) = sentinel_value<T>();
@@ -285,11 +325,11 @@ __device__ __forceinline__ void grid_warp_run(const GridWarp<T, S>& g, unsigned&
 // {sys, first unit along y, first plane, units along y per tile (jw)}; a
 // tile's warp q runs unit (first + q % jw, plane + q / jw).  Systems with z
 // neighbours are tiled with jw = 1 (the warps are consecutive planes).
-template <typename T, typename S, int NW, bool REV>
+template <typename T, typename S, int NW, bool REV, int OPK = kGridSweep>
 __global__ void __launch_bounds__(32 * (NW + kGridRecvWarps)) k_sweep_grid(SetView sv, ChunkSweepOp op)
 {
     constexpr int NTH = 32 * (NW + kGridRecvWarps);
-    constexpr int SE = grid_stage_elems<S>();
+    constexpr int SE = grid_stage_elems<S, OPK>();
     if (blockDim.x != unsigned(NTH) || op.which != int(REV)) {   // launch shape mismatch: report, never wait
         if (threadIdx.x == 0) atomicExch(sv.err, 1);
         return;
@@ -337,7 +377,8 @@ __global__ void __launch_bounds__(32 * (NW + kGridRecvWarps)) k_sweep_grid(SetVi
                 if (ju < njb && k < nz) {
                     const int j = 32 * ju + lane;
                     GridWarp<T, S> g;
-                    g.src = static_cast<const S*>(F.gdata) + (size_t(k) * njb + ju) * size_t(F.gnsp) * size_t(ns + 1) * 32;
+                    const int slots = OPK == kGridILU0 ? 2 * ns + 1 : ns + 1;
+                    g.src = static_cast<const S*>(F.gdata) + (size_t(k) * njb + ju) * size_t(F.gnsp) * size_t(slots) * 32;
                     g.stg = stage + size_t(q) * SE;
                     g.fb = full + q * kGridNB;
                     g.vin = vptr<T>(d, op.in);
@@ -361,7 +402,11 @@ __global__ void __launch_bounds__(32 * (NW + kGridRecvWarps)) k_sweep_grid(SetVi
                     g.y_out = (dirs & 2) && qj + 1 < jw && ju + 1 < njb;
                     g.err = sv.err;
                     g.spin = sv.spin;
-                    if (ns == 3) {
+                    if constexpr (OPK != kGridSweep) {
+                        // pivots: L's geometry, farthest neighbour first
+                        if (ns == 3) grid_warp_run<T, S, 3, true, false, OPK>(g, phase);
+                        else grid_warp_run<T, S, 2, true, false, OPK>(g, phase);
+                    } else if (ns == 3) {
                         if (perm == kGridFar3) grid_warp_run<T, S, 3, true, REV>(g, phase);
                         else grid_warp_run<T, S, 3, false, REV>(g, phase);
                     } else if (ns == 2) {
@@ -446,11 +491,13 @@ __global__ void __launch_bounds__(32 * (NW + kGridRecvWarps)) k_sweep_grid(SetVi
 // pivot of c, U's (r, c) is a_rc times the inverse pivot of r -- and the
 // multiplier slot the inverse pivot of r (1 for a unit diagonal); padding +0.
 // The same values and roundings as k_fill_grid and the chunked layout's fill.
+// lmul: ILU(0) factorized on the grid (A's values in `src`): L's entries are
+// a_rc times the inverse pivot of c, as k_ilu0_factor forms them.
 struct GridFillGeom {
     int n, nx, ny, nz, ns, perm, skew, nsteps, nsp, njb;
 };
 constexpr int kGridFillILU = 0, kGridFillIC = 1;
-__global__ void k_fill_grid_csr(long long nent, GridFillGeom g, int lower, int kind, int unit,
+__global__ void k_fill_grid_csr(long long nent, GridFillGeom g, int lower, int kind, int unit, int lmul,
                                 const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ src,
                                 const double* __restrict__ inv_dia, void* val, int f32)
 {
@@ -484,12 +531,54 @@ __global__ void k_fill_grid_csr(long long nent, GridFillGeom g, int lower, int k
                     if (pos >= 0) {
                         v = src[pos];
                         if (kind == kGridFillIC) v = v * inv_dia[lower ? c : r];
+                        else if (lmul && lower) v = v * inv_dia[c];   // ILU(0)'s l_rc = a_rc / u_cc, as the factorization rounds it
                     }
                 }
             }
         }
         if (f32) static_cast<float*>(val)[e] = float(v);
         else static_cast<double*>(val)[e] = v;
+    }
+}
+
+// Layout of a grid factorization (L's geometry, farthest neighbour first):
+// per step and lane the row's entries toward its earlier neighbours a_ik
+// (ILU(0) only), those neighbours' entries in the row's column a_ki, then
+// a_ii; +0 where the row has no such neighbour.  FP64 values of A.
+__global__ void k_fill_grid_factor(long long nent, GridFillGeom g, int kind, const int* __restrict__ rp,
+                                   const int* __restrict__ ci, const double* __restrict__ a, double* __restrict__ out)
+{
+    const int slots = kind == kGridILU0 ? 2 * g.ns + 1 : g.ns + 1;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nent;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int lane = int(e & 31);
+        long long rest = e >> 5;
+        const int q = int(rest % slots);
+        rest /= slots;
+        const int s = int(rest % g.nsp);
+        const long long u = rest / g.nsp;
+        const int ju = int(u % g.njb), k = int(u / g.njb);
+        const int i = g.skew ? s - lane : s, j = 32 * ju + lane;
+        const long long r = i + (long long)g.nx * (j + (long long)g.ny * k);
+        double v = 0.0;
+        if (s < g.nsteps && i >= 0 && i < g.nx && j < g.ny && r < g.n) {
+            int row = int(r), col = int(r);   // q == slots - 1: the diagonal
+            bool present = true;
+            if (q < slots - 1) {
+                const int qd = q < g.ns ? q : q - g.ns;
+                const int d = (g.perm >> (2 * qd)) & 3;
+                present = d == 0 ? i > 0 : d == 1 ? j > 0 : k > 0;
+                const long long off = d == 0 ? 1 : d == 1 ? g.nx : (long long)g.nx * g.ny;
+                const int nb = int(r - off);
+                const bool toward = kind == kGridILU0 && q < g.ns;   // a_ik (row r, column nb); else a_ki
+                row = toward ? int(r) : nb;
+                col = toward ? nb : int(r);
+            }
+            if (present)
+                for (int f = rp[row]; f < rp[row + 1]; ++f)
+                    if (ci[f] == col) v = a[f];
+        }
+        out[e] = v;
     }
 }
 

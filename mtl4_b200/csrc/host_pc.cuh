@@ -619,8 +619,35 @@ struct GridShape {
     }
 };
 
+// Grid factorizations: FP64, ILU(0) pivots with two compute warps (its
+// steps carry seven values), IC(0) pivots with four.
+constexpr int kGridFactorWarpsILU = 2, kGridFactorWarpsIC = 4;
+template <int OPK, int NW>
+struct GridFactorShape {
+    static constexpr int THREADS = 32 * (NW + kGridRecvWarps);
+    static int smem() { return grid_smem_bytes<double, double, OPK>(NW); }
+    static int init()
+    {
+        MTLG_CUDA(cudaFuncSetAttribute(k_sweep_grid<double, double, NW, false, OPK>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem()));
+        return MTLG_OK;
+    }
+    static int resident(mtlg_ctx* c)
+    {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_grid<double, double, NW, false, OPK>, THREADS,
+                                                          size_t(smem())) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return n * c->sm_count;
+    }
+};
+
 inline int init_grid_shapes()
 {
+    MTLG_TRY((GridFactorShape<kGridILU0, kGridFactorWarpsILU>::init()));
+    MTLG_TRY((GridFactorShape<kGridIC0, kGridFactorWarpsIC>::init()));
     MTLG_TRY((GridShape<double, double, 4>::init()));
     MTLG_TRY((GridShape<double, double, 8>::init()));
     MTLG_TRY((GridShape<double, float, 4>::init()));
@@ -1197,6 +1224,7 @@ struct mtlg_pc {
     ChunkPlan plan[2];              // chunked sweeps with FP64 [0] / FP32 [1] vectors
     int plan_kernel[2] = {-1, -1};  // context's sweep_kernel / cluster setting the plan was made for
     mtlg_pc* adjoint = nullptr;     // ILU(0): factors of (LU)^H, made on the first adjoint apply
+    bool grid_factored = false;     // pivots computed by the grid kernel (ILU(0): A's values, no factorized copy)
     RowLists lt;                    // IC(0): transposed upper pattern (natural order)
     DBuf<int> lt_rp, lt_row, lt_src;
     bool has_factors() const { return kind == MTLG_PC_ILU0 || kind == MTLG_PC_IC0; }
@@ -1308,8 +1336,8 @@ inline int fill_grid_values(mtlg_pc* P, TriDev& T, const double* srcvals, const 
         const GridFillGeom g = {T.n, T.gnx, T.gny, T.gnz, T.gns, T.gperm, T.gskew, T.gnsteps, T.gnsp, T.gnjb};
         const int kind = P->kind == MTLG_PC_IC0 ? kGridFillIC : kGridFillILU;
         k_fill_grid_csr<<<launch_grid(T.gnent), 256, 0, c->stream>>>(T.gnent, g, T.lower ? 1 : 0, kind, unit,
-                                                                   P->A->rp.p, P->A->ci.p, srcvals, inv_dia,
-                                                                   T.gval.p, f32);
+                                                                   P->grid_factored ? 1 : 0, P->A->rp.p, P->A->ci.p,
+                                                                   srcvals, inv_dia, T.gval.p, f32);
         c->launches++;
         MTLG_CUDA(cudaGetLastError());
         return MTLG_OK;
@@ -1409,6 +1437,92 @@ inline int ensure_flat(mtlg_pc* P)
         }
     }
     MTLG_CUDA(cudaStreamSynchronize(c->stream));
+    return MTLG_OK;
+}
+
+// FP64 pivots of an ILU(0) / IC(0) preconditioner whose L factor has the
+// grid layout (farthest neighbour first), on the grid kernel: the factor
+// layout (A's values per row and neighbour) is filled on the device, the
+// pivots land in P->inv_dia (all sentinel before).  ILU(0) needs sides of
+// at least 3 (with 2 a neighbour's entry falls in the row's pattern and
+// off-diagonal entries change too).  Sets `done` when it ran.
+inline int grid_factorize(mtlg_pc* P, bool& done)
+{
+    done = false;
+    mtlg_ctx* c = P->ctx;
+    const TriDev& L = P->L;
+    if (L.gnx == 0 || L.gns < 2 || !L.gskew) return MTLG_OK;
+    if (L.gperm != (L.gns == 3 ? kGridFar3 : kGridFar2)) return MTLG_OK;
+    const int kind = P->kind == MTLG_PC_IC0 ? kGridIC0 : kGridILU0;
+    if (kind == kGridILU0 && (L.gnx < 3 || (L.gns == 3 && L.gny < 3) || (L.gns == 2 && L.gny < 2))) return MTLG_OK;
+    const int nw = kind == kGridILU0 ? kGridFactorWarpsILU : kGridFactorWarpsIC;
+    const int res = kind == kGridILU0 ? GridFactorShape<kGridILU0, kGridFactorWarpsILU>::resident(c)
+                                      : GridFactorShape<kGridIC0, kGridFactorWarpsIC>::resident(c);
+    if (res < 1) return MTLG_OK;
+    MTLG_TRACE(9162, "pc.grid_factor");
+    const int slots = kind == kGridILU0 ? 2 * L.gns + 1 : L.gns + 1;
+    const long long nent = (long long)L.gnjb * L.gnz * L.gnsp * slots * 32;
+    DBuf<double> lay;
+    MTLG_TRY(lay.alloc(c, size_t(nent)));
+    const GridFillGeom gg = {L.n, L.gnx, L.gny, L.gnz, L.gns, L.gperm, L.gskew, L.gnsteps, L.gnsp, L.gnjb};
+    k_fill_grid_factor<<<launch_grid(nent), 256, 0, c->stream>>>(nent, gg, kind, P->A->rp.p, P->A->ci.p, P->A->v64.p,
+                                                                 lay.p);
+    c->launches++;
+    // one system: inv_dia is the output vector, L's view carries the factor layout
+    SysDesc d;
+    memset(&d, 0, sizeof d);
+    d.n = P->n;
+    d.x = P->inv_dia.p;
+    d.L = tri_view(L);
+    d.L.gnx = L.gnx;
+    d.L.gny = L.gny;
+    d.L.gnz = L.gnz;
+    d.L.gns = L.gns;
+    d.L.gperm = L.gperm;
+    d.L.gdirs = L.gdirs;
+    d.L.gskew = L.gskew;
+    d.L.gnsteps = L.gnsteps;
+    d.L.gnsp = L.gnsp;
+    d.L.gnjb = L.gnjb;
+    d.L.gdata = lay.p;
+    MTLG_CUDA(cudaMemcpyAsync(P->desc.p, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
+    std::vector<GroupTask> tiles;
+    const int jw = L.gns == 3 ? 1 : nw, kw = nw / jw;
+    for (int k0 = 0; k0 < L.gnz; k0 += kw)
+        for (int j0 = 0; j0 < L.gnjb; j0 += jw) tiles.push_back(GroupTask{0, j0, k0, jw});
+    DBuf<GroupTask> tl;
+    MTLG_TRY(tl.upload(c, tiles.data(), tiles.size()));
+    SetView sv;
+    memset(&sv, 0, sizeof sv);
+    sv.n_sys = 1;
+    sv.desc = P->desc.p;
+    sv.st = P->st.p;
+    sv.running = P->misc.p;
+    sv.err = P->misc.p + 1;
+    sv.spin = c->spin_limit;
+    ChunkSweepOp op;
+    memset(&op, 0, sizeof op);
+    op.tasks = tl.p;
+    op.ntasks = int(tiles.size());
+    op.ticket = P->tickets.p + 6;
+    op.which = 0;
+    op.in = SLOT_NONE;
+    op.out = SLOT_X;
+    op.reset = SLOT_NONE;
+    op.skip = SKIP_NONE;
+    op.sleep_ns = c->sweep_sleep_ns;
+    const int grid = std::max(1, std::min(op.ntasks, res));
+    if (kind == kGridILU0) {
+        using Sh = GridFactorShape<kGridILU0, kGridFactorWarpsILU>;
+        k_sweep_grid<double, double, kGridFactorWarpsILU, false, kGridILU0><<<grid, Sh::THREADS, Sh::smem(), c->stream>>>(sv, op);
+    } else {
+        using Sh = GridFactorShape<kGridIC0, kGridFactorWarpsIC>;
+        k_sweep_grid<double, double, kGridFactorWarpsIC, false, kGridIC0><<<grid, Sh::THREADS, Sh::smem(), c->stream>>>(sv, op);
+    }
+    c->launches++;
+    MTLG_CUDA(cudaGetLastError());
+    MTLG_CUDA(cudaStreamSynchronize(c->stream));   // the layout and task list are released next
+    done = true;
     return MTLG_OK;
 }
 
@@ -1571,7 +1685,12 @@ inline int pc_build(mtlg_pc* P)
     op.dpos = A->dpos.p;
     op.err = P->misc.p + 1;
     op.spin = c->spin_limit;
-    if (P->kind == MTLG_PC_ILU0) {
+    bool gdone = false;
+    if (c->grid_sweep) MTLG_TRY(grid_factorize(P, gdone));
+    P->grid_factored = gdone;
+    if (gdone) {
+        // pivots done on the grid kernel; factor values come from A's values
+    } else if (P->kind == MTLG_PC_ILU0) {
         MTLG_TRY(lu.alloc(c, size_t(std::max<int64_t>(1, A->nnz))));
         MTLG_CUDA(cudaMemcpyAsync(lu.p, A->v64.p, size_t(A->nnz) * 8, cudaMemcpyDeviceToDevice, c->stream));
         op.lu = lu.p;

@@ -211,3 +211,24 @@ def test_flat_sweep_after_grid_setup(ctx, kind):
         assert np.array_equal(y, O.port_pc_apply(A, kind, x, storage_f32=(st == np.float32)))
         y2 = itl.solve(Pc, vec(x, ctx)).numpy()   # back on the grid sweep
         assert np.array_equal(y2, y)
+
+
+@pytest.mark.parametrize("kind", ["ilu_0", "ic_0"])
+def test_grid_factorization_equals_level_factorization(ctx, kind):
+    # the pivots computed on the grid kernel (grid-stencil patterns) are the
+    # level-scheduled factorization's bit for bit: the downloaded factors
+    # match, for 2D and 3D grids, and for sides of 2 (ILU(0) keeps the
+    # level-scheduled kernel there)
+    from mtl4_b200 import itl
+    for A in (P.vardiff_3d((17, 12, 5), sigma=1.0, seed=3, beta=(0.3, 0.2, 0.1)),
+              P.vardiff_2d((45, 21), sigma=1.0, seed=4),
+              P.vardiff_3d((9, 2, 6), sigma=0.5, seed=5)):
+        Ad = dev(A, ctx)
+        got = {}
+        for grid in (1, 0):
+            with tuning(ctx, grid_sweep=grid):
+                Pc = getattr(itl.pc, kind)(Ad)
+                got[grid] = [Pc.factor(w) for w in ("L", "U")]
+        for (a, b) in zip(got[1], got[0]):
+            for u, v in zip(a, b):
+                assert np.array_equal(u, v)
