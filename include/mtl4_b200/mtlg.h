@@ -331,6 +331,17 @@ int mtlg_pc_levels(const mtlg_pc* P, int* levels_L, int* levels_U);
  * the flat level-order sweeps run instead.  Not part of the reference's
  * interface (introspection for tuning). */
 int mtlg_pc_sweep_plan(mtlg_ctx* ctx, mtlg_pc* P, int dtype, int32_t* out8);
+/* Grid structure of a sparse pattern as the triangular sweeps see it: the
+ * strictly lower (lower != 0) or strictly upper entries of the n x n CSR
+ * pattern (row_ptr, col) are tested for a 5- or 7-point grid stencil in
+ * natural order (the preconditioners whose factors pass get the grid sweep
+ * and grid factorization).  out8: nx, ny, nz, entries per row, entry order
+ * (1 farthest neighbour first, 2 nearest first, 0 none), 1 when rows depend
+ * on their neighbours, 0, 0; all zero when the pattern is not a grid
+ * stencil (a pattern without entries reports a grid of independent rows).
+ * Host-only, no device work.  Not part of the reference's interface
+ * (introspection). */
+int mtlg_grid_structure(int64_t n, const int64_t* row_ptr, const int32_t* col, int lower, int32_t* out8);
 
 /* ---- solvers ---------------------------------------------------------------- */
 /* x is in/out (initial guess on entry).  pc_right may be NULL (identity); CG

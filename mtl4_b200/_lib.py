@@ -114,6 +114,7 @@ SIGNATURES = {
     "mtlg_pc_factor": (C.c_int, [VP, C.c_int, PI64, VP, VP, VP]),
     "mtlg_pc_levels": (C.c_int, [VP, PINT, PINT]),
     "mtlg_pc_sweep_plan": (C.c_int, [VP, VP, C.c_int, PINT]),
+    "mtlg_grid_structure": (C.c_int, [I64, VP, VP, C.c_int, PINT]),
     "mtlg_solve": (C.c_int, [VP, C.c_int, VP, VP, VP, VP, VP, C.POINTER(IterParams), C.POINTER(IterResult)]),
     "mtlg_refine_solve": (C.c_int, [VP, C.c_int, VP, VP, VP, VP, C.POINTER(RefineParams), C.POINTER(IterResult)]),
     "mtlg_batch_create": (C.c_int, [VP, C.POINTER(VP)]),

@@ -1091,6 +1091,31 @@ int mtlg_pc_sweep_plan(mtlg_ctx* c, mtlg_pc* P, int dtype, int32_t* out8)
     return sweep_plan_of<double, double>(c, P, out8);
 }
 
+int mtlg_grid_structure(int64_t n, const int64_t* row_ptr, const int32_t* col, int lower, int32_t* out8)
+{
+    MTLG_CHECK_ARG(out8 && n >= 0 && (n == 0 || (row_ptr && col)), "null array");
+    for (int i = 0; i < 8; ++i) out8[i] = 0;
+    MTLG_CHECK_ARG(n <= INT32_MAX && (n == 0 || row_ptr[n] <= INT32_MAX), "sizes beyond int32");
+    // the strictly lower (upper) entries of each row, in storage order, as
+    // the preconditioners' factor row lists hold them
+    RowLists F;
+    F.rp.assign(size_t(n) + 1, 0);
+    for (int64_t r = 0; r < n; ++r) {
+        for (int64_t e = row_ptr[r]; e < row_ptr[r + 1]; ++e)
+            if (lower ? col[e] < r : col[e] > r) F.col.push_back(col[e]);
+        F.rp[size_t(r) + 1] = int(F.col.size());
+    }
+    TriDev T;
+    if (!detect_grid(F, int(n), lower != 0, T) || T.gnx == 0) return MTLG_OK;
+    out8[0] = T.gnx;
+    out8[1] = T.gny;
+    out8[2] = T.gnz;
+    out8[3] = T.gns;
+    out8[4] = T.gns == 0 ? 0 : (T.gperm == (T.gns == 3 ? kGridFar3 : kGridFar2) ? 1 : 2);
+    out8[5] = T.gskew;
+    return MTLG_OK;
+}
+
 // ------------------------------------------------------------------ solves
 static int check_solve_args(int solver, mtlg_csr* A, mtlg_vec* x, const mtlg_vec* b, const mtlg_pc* P)
 {
