@@ -29,6 +29,11 @@
 // reads comes earlier, and a tile runs to its end on a running CTA, so the
 // waits end; every wait is still bounded (the context's spin_limit polls),
 // after which the kernel records a timeout and drains with zeros.
+// The same kernel computes the FP64 pivots of an ILU(0) or IC(0)
+// factorization of a grid-stencil pattern (OPK kGridILU0 / kGridIC0): a
+// row's pivot needs its earlier neighbours' pivots exactly as an L sweep's
+// row needs their results (boost/numeric/itl/pc/ilu_0.hpp:45-82,
+// ic_0.hpp:124-186, with k_ilu0_factor's and k_ic0_factor's roundings).
 #pragma once
 #include "sweep.cuh"
 
