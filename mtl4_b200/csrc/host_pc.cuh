@@ -1443,9 +1443,10 @@ inline int ensure_flat(mtlg_pc* P)
 // FP64 pivots of an ILU(0) / IC(0) preconditioner whose L factor has the
 // grid layout (farthest neighbour first), on the grid kernel: the factor
 // layout (A's values per row and neighbour) is filled on the device, the
-// pivots land in P->inv_dia (all sentinel before).  ILU(0) needs sides of
-// at least 3 (with 2 a neighbour's entry falls in the row's pattern and
-// off-diagonal entries change too).  Sets `done` when it ran.
+// pivots land in P->inv_dia (all sentinel before).  ILU(0) grids with a
+// side of 2 stay on the level-scheduled kernel (the rule holds there as
+// well, but this kernel is exercised on sides of 3 and more).  Sets `done`
+// when it ran.
 inline int grid_factorize(mtlg_pc* P, bool& done)
 {
     done = false;
